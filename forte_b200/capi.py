@@ -1,0 +1,112 @@
+"""ctypes binding of the engine's C ABI (include/fcib.h).
+
+This is the binding a host program would add to call the engine; it loads the in-tree
+libfcib200.so and raises when the library or a CUDA device is missing (there is no CPU
+fallback).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libfcib200.so")
+_LIB = None
+
+FCIB_OK = 0
+FCIB_ERR_ARG = -1
+FCIB_ERR_STATE = -2
+FCIB_ERR_CUDA = -3
+FCIB_ERR_UNSUPPORTED = -4
+FCIB_ERR_NOT_CONVERGED = -5
+FCIB_ERR_NUMERIC = -6
+
+PREC_FP64 = 0
+PREC_MIXED = 1
+PREC_MIXED_TF32 = 2
+PRECOND_DIAG = 0
+PRECOND_MLP = 1
+
+
+class FcibOptions(C.Structure):
+    _fields_ = [
+        ("maxiter", C.c_int),
+        ("e_convergence", C.c_double),
+        ("r_convergence", C.c_double),
+        ("guess_per_root", C.c_int),
+        ("dets_per_guess", C.c_int),
+        ("collapse_per_root", C.c_int),
+        ("subspace_per_root", C.c_int),
+        ("die_if_not_converged", C.c_int),
+        ("print_", C.c_int),
+        ("precision", C.c_int),
+        ("preconditioner", C.c_int),
+        ("mixed_switch", C.c_double),
+    ]
+
+
+class FcibError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"fcib error {code}: {msg}")
+        self.code = code
+
+
+#: exported symbols and their (restype, argtypes)
+_dp = C.POINTER(C.c_double)
+_vp = C.c_void_p
+SIGNATURES = {
+    "fcib_default_options": (None, [C.POINTER(FcibOptions)]),
+    "fcib_last_error": (C.c_char_p, []),
+    "fcib_version": (C.c_char_p, []),
+    "fcib_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int]),
+    "fcib_destroy": (C.c_int, [_vp]),
+    "fcib_set_integrals": (C.c_int, [_vp, C.c_int, C.c_int, C.POINTER(C.c_int), C.c_double, _dp, _dp, _dp, _dp, _dp]),
+    "fcib_set_state": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
+    "fcib_set_options": (C.c_int, [_vp, C.POINTER(FcibOptions)]),
+    "fcib_size": (C.c_int, [_vp, C.POINTER(C.c_int64)]),
+    "fcib_solve": (C.c_int, [_vp, _dp, _dp, C.POINTER(C.c_int)]),
+    "fcib_get_vector": (C.c_int, [_vp, C.c_int, _dp]),
+    "fcib_sigma": (C.c_int, [_vp, _dp, _dp]),
+    "fcib_sigma_device": (C.c_int, [_vp, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    "fcib_hdiag": (C.c_int, [_vp, _dp]),
+    "fcib_spin2": (C.c_int, [_vp, _dp, _dp]),
+    "fcib_rdms": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp]),
+    "fcib_num_strings": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_int64)]),
+    "fcib_strings": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_uint32)]),
+    "fcib_string_list": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                    C.POINTER(C.c_int64), C.POINTER(C.c_int8), C.POINTER(C.c_uint32),
+                                    C.POINTER(C.c_uint32)]),
+    "fcib_last_timing": (C.c_int, [_vp, _dp, C.POINTER(C.c_int), _dp]),
+}
+
+
+def lib():
+    """Loads libfcib200.so (built in-tree by forte_b200.build)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise FcibError(FCIB_ERR_STATE, f"{LIB_PATH} is missing: run forte_b200.build.build() first")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _LIB = L
+    return _LIB
+
+
+def check(rc):
+    if rc != FCIB_OK:
+        raise FcibError(rc, lib().fcib_last_error().decode())
+
+
+def dptr(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+def default_options() -> FcibOptions:
+    o = FcibOptions()
+    lib().fcib_default_options(C.byref(o))
+    return o

@@ -1,0 +1,422 @@
+// extern "C" boundary of the engine (declared in include/fcib.h).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "fcib_internal.h"
+
+struct fcib_ctx {
+    fcib::Context c;
+};
+
+namespace fcib {
+
+static thread_local std::string g_last_error;
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+template <typename F>
+static int guarded(fcib_ctx* ctx, F&& f) {
+    try {
+        if (ctx) FCIB_CUDA(cudaSetDevice(ctx->c.device));
+        f();
+        return FCIB_OK;
+    } catch (const Error& e) {
+        set_error(e.msg);
+        return e.code;
+    } catch (const std::exception& e) {
+        set_error(e.what());
+        return FCIB_ERR_ARG;
+    }
+}
+
+static void build_mask_and_maps(Context& c) {
+    c.block_to_c1.clear();
+    if (c.nirrep <= 1) {
+        c.mask.release();
+        return;
+    }
+    std::vector<uint32_t> sa(c.nas), sb(c.nbs);
+    FCIB_CUDA(cudaMemcpy(sa.data(), c.A.str.p, 4 * c.nas, cudaMemcpyDeviceToHost));
+    FCIB_CUDA(cudaMemcpy(sb.data(), c.B.str.p, 4 * c.nbs, cudaMemcpyDeviceToHost));
+    auto sym = [&](uint32_t s) {
+        int h = 0;
+        for (int i = 0; i < c.n; i++)
+            if (s >> i & 1u) h ^= c.orbsym[i];
+        return h;
+    };
+    std::vector<int> ha(c.nas), hb(c.nbs);
+    for (int64_t i = 0; i < c.nas; i++) ha[i] = sym(sa[i]);
+    for (int64_t i = 0; i < c.nbs; i++) hb[i] = sym(sb[i]);
+    std::vector<uint8_t> m((size_t)c.ndet);
+    for (int64_t i = 0; i < c.nas; i++)
+        for (int64_t j = 0; j < c.nbs; j++) m[i * c.nbs + j] = ((ha[i] ^ hb[j]) == c.irrep);
+    c.mask.upload(m, c.stream);
+    // FCIVector flat order: alpha irrep blocks h, rows = alpha strings of irrep h in string
+    // order, columns = beta strings of irrep h ^ symmetry (forte/fci/fci_string_lists.cc:318-331)
+    for (int h = 0; h < c.nirrep; h++)
+        for (int64_t i = 0; i < c.nas; i++) {
+            if (ha[i] != h) continue;
+            for (int64_t j = 0; j < c.nbs; j++)
+                if (hb[j] == (h ^ c.irrep)) c.block_to_c1.push_back(i * c.nbs + j);
+        }
+}
+
+void ensure_setup(Context& c) {
+    FCIB_CHECK(c.has_ints, FCIB_ERR_STATE, "integrals have not been set");
+    FCIB_CHECK(c.has_state, FCIB_ERR_STATE, "state has not been set");
+    if (c.tables_ready) return;
+    FCIB_CHECK(c.na <= c.n && c.nb <= c.n, FCIB_ERR_ARG, "more electrons than orbitals");
+    bool fold = (c.na >= 1 && c.nb >= 1);
+    build_spin_tables(c.A, c.n, c.na, !fold, c.stream);
+    build_spin_tables(c.B, c.n, c.nb, !fold, c.stream);
+    c.nas = c.A.nstr;
+    c.nbs = c.B.nstr;
+    c.ndet = c.nas * c.nbs;
+    FCIB_CUDA(cudaStreamSynchronize(c.stream));
+    prepare_integrals(c);
+    build_mask_and_maps(c);
+    c.hdiag.alloc((size_t)c.ndet);
+    compute_hdiag(c, c.hdiag.p);
+    FCIB_CUDA(cudaStreamSynchronize(c.stream));
+    c.tables_ready = true;
+}
+
+void sigma_dispatch(Context& c, const double* b, double* s, int precision) {
+    (void)precision;
+    sigma_fp64(c, b, s);
+}
+
+// host flat (FCIVector order) <-> device C1 layout
+static void upload_flat(Context& c, const double* flat, double* dev) {
+    if (c.nirrep <= 1) {
+        FCIB_CUDA(cudaMemcpyAsync(dev, flat, sizeof(double) * c.ndet, cudaMemcpyHostToDevice, c.stream));
+        return;
+    }
+    std::vector<double> full((size_t)c.ndet, 0.0);
+    for (size_t i = 0; i < c.block_to_c1.size(); i++) full[c.block_to_c1[i]] = flat[i];
+    FCIB_CUDA(cudaMemcpyAsync(dev, full.data(), sizeof(double) * c.ndet, cudaMemcpyHostToDevice, c.stream));
+    FCIB_CUDA(cudaStreamSynchronize(c.stream));
+}
+static void download_flat(Context& c, const double* dev, double* flat) {
+    if (c.nirrep <= 1) {
+        FCIB_CUDA(cudaMemcpyAsync(flat, dev, sizeof(double) * c.ndet, cudaMemcpyDeviceToHost, c.stream));
+        FCIB_CUDA(cudaStreamSynchronize(c.stream));
+        return;
+    }
+    std::vector<double> full((size_t)c.ndet);
+    FCIB_CUDA(cudaMemcpyAsync(full.data(), dev, sizeof(double) * c.ndet, cudaMemcpyDeviceToHost, c.stream));
+    FCIB_CUDA(cudaStreamSynchronize(c.stream));
+    for (size_t i = 0; i < c.block_to_c1.size(); i++) flat[i] = full[c.block_to_c1[i]];
+}
+static int64_t flat_size(const Context& c) {
+    return c.nirrep <= 1 ? c.ndet : (int64_t)c.block_to_c1.size();
+}
+
+}  // namespace fcib
+
+using namespace fcib;
+
+extern "C" {
+
+void fcib_default_options(fcib_options* o) {
+    if (!o) return;
+    o->maxiter = 100;
+    o->e_convergence = 1.0e-9;
+    o->r_convergence = 1.0e-6;
+    o->guess_per_root = 1;
+    o->dets_per_guess = 50;
+    o->collapse_per_root = 2;
+    o->subspace_per_root = 10;
+    o->die_if_not_converged = 0;
+    o->print = 0;
+    o->precision = FCIB_PREC_FP64;
+    o->preconditioner = FCIB_PRECOND_DIAG;
+    o->mixed_switch = 1.0e-4;
+}
+
+const char* fcib_last_error(void) { return g_last_error.c_str(); }
+const char* fcib_version(void) { return "fcib 0.1 (sm_100a)"; }
+
+int fcib_create(fcib_ctx** out, int device) {
+    if (!out) {
+        set_error("fcib_create: null output pointer");
+        return FCIB_ERR_ARG;
+    }
+    *out = nullptr;
+    fcib_ctx* ctx = new fcib_ctx();
+    int rc = guarded(nullptr, [&] {
+        int ndev = 0;
+        FCIB_CUDA(cudaGetDeviceCount(&ndev));
+        FCIB_CHECK(device >= 0 && device < ndev, FCIB_ERR_ARG, "fcib_create: no such CUDA device");
+        FCIB_CUDA(cudaSetDevice(device));
+        cudaDeviceProp prop;
+        FCIB_CUDA(cudaGetDeviceProperties(&prop, device));
+        FCIB_CHECK(prop.major == 10, FCIB_ERR_UNSUPPORTED, "fcib requires an sm_100 (B200) device");
+        ctx->c.device = device;
+        ctx->c.num_sms = prop.multiProcessorCount;
+        ctx->c.smem_optin = (int)prop.sharedMemPerBlockOptin;
+        ctx->c.smem_per_sm = (int)prop.sharedMemPerMultiprocessor;
+        FCIB_CUDA(cudaStreamCreateWithFlags(&ctx->c.stream, cudaStreamNonBlocking));
+        fcib_default_options(&ctx->c.opt);
+    });
+    if (rc != FCIB_OK) {
+        delete ctx;
+        return rc;
+    }
+    *out = ctx;
+    return FCIB_OK;
+}
+
+int fcib_destroy(fcib_ctx* ctx) {
+    if (!ctx) return FCIB_OK;
+    cudaSetDevice(ctx->c.device);
+    cudaStreamSynchronize(ctx->c.stream);
+    cudaStream_t s = ctx->c.stream;
+    delete ctx;
+    if (s) cudaStreamDestroy(s);
+    return FCIB_OK;
+}
+
+int fcib_set_integrals(fcib_ctx* ctx, int n, int nirrep, const int* orbsym, double scalar,
+                       const double* oei_a, const double* oei_b, const double* tei_aa,
+                       const double* tei_ab, const double* tei_bb) {
+    if (!ctx) { set_error("null context"); return FCIB_ERR_ARG; }
+    return guarded(ctx, [&] {
+        FCIB_CHECK(n >= 1 && n <= kMaxOrb, FCIB_ERR_UNSUPPORTED, "number of active orbitals must be 1..22");
+        FCIB_CHECK(nirrep >= 1 && nirrep <= 8, FCIB_ERR_ARG, "nirrep must be 1..8");
+        FCIB_CHECK(oei_a && oei_b && tei_aa && tei_ab && tei_bb, FCIB_ERR_ARG, "null integral pointer");
+        FCIB_CHECK(std::isfinite(scalar), FCIB_ERR_NUMERIC, "scalar energy is not finite");
+        Context& c = ctx->c;
+        const size_t n2 = (size_t)n * n, n4 = n2 * n2;
+        c.n = n;
+        c.nirrep = nirrep;
+        c.orbsym.assign(n, 0);
+        if (orbsym)
+            for (int i = 0; i < n; i++) {
+                FCIB_CHECK(orbsym[i] >= 0 && orbsym[i] < nirrep, FCIB_ERR_ARG, "orbital irrep out of range");
+                c.orbsym[i] = orbsym[i];
+            }
+        c.scalar = scalar;
+        c.oei_a.assign(oei_a, oei_a + n2);
+        c.oei_b.assign(oei_b, oei_b + n2);
+        c.tei_aa.assign(tei_aa, tei_aa + n4);
+        c.tei_ab.assign(tei_ab, tei_ab + n4);
+        c.tei_bb.assign(tei_bb, tei_bb + n4);
+        double mx = 0.0, dev = 0.0;
+        for (size_t i = 0; i < n4; i++) {
+            FCIB_CHECK(std::isfinite(c.tei_ab[i]) && std::isfinite(c.tei_aa[i]) && std::isfinite(c.tei_bb[i]),
+                       FCIB_ERR_NUMERIC, "two-electron integrals contain non-finite values");
+            mx = std::max(mx, std::fabs(c.tei_ab[i]));
+        }
+        for (size_t i = 0; i < n2; i++)
+            FCIB_CHECK(std::isfinite(c.oei_a[i]) && std::isfinite(c.oei_b[i]), FCIB_ERR_NUMERIC,
+                       "one-electron integrals contain non-finite values");
+        // real-orbital symmetry used by the pair-symmetrised sigma: (pq|rs) = (qp|rs) = (rs|pq)
+        auto tab = [&](int p, int q, int r, int s) { return c.tei_ab[((size_t)p * n + q) * n2 + r * n + s]; };
+        for (int p = 0; p < n; p++)
+            for (int q = 0; q < n; q++) {
+                dev = std::max(dev, std::fabs(c.oei_a[p * n + q] - c.oei_a[q * n + p]));
+                dev = std::max(dev, std::fabs(c.oei_b[p * n + q] - c.oei_b[q * n + p]));
+                for (int r = 0; r < n; r++)
+                    for (int s = 0; s < n; s++) {
+                        double v = tab(p, r, q, s);  // (pq|rs)
+                        dev = std::max(dev, std::fabs(v - tab(q, r, p, s)));
+                        dev = std::max(dev, std::fabs(v - tab(r, p, s, q)));
+                    }
+            }
+        FCIB_CHECK(dev <= 1e-10 * std::max(1.0, mx), FCIB_ERR_UNSUPPORTED,
+                   "integrals must be real with 8-fold symmetry (h_pq = h_qp, (pq|rs) = (qp|rs) = (rs|pq))");
+        c.has_ints = true;
+        c.tables_ready = false;
+        c.solved = false;
+    });
+}
+
+int fcib_set_state(fcib_ctx* ctx, int na, int nb, int irrep, int multiplicity, int nroot, int root) {
+    if (!ctx) { set_error("null context"); return FCIB_ERR_ARG; }
+    return guarded(ctx, [&] {
+        Context& c = ctx->c;
+        FCIB_CHECK(c.has_ints, FCIB_ERR_STATE, "set integrals before the state");
+        FCIB_CHECK(na >= 0 && nb >= 0 && na <= c.n && nb <= c.n, FCIB_ERR_ARG, "electron counts out of range");
+        FCIB_CHECK(irrep >= 0 && irrep < c.nirrep, FCIB_ERR_ARG, "target irrep out of range");
+        FCIB_CHECK(multiplicity >= 0, FCIB_ERR_ARG, "multiplicity must be >= 1 (0 = no spin selection in the guess)");
+        FCIB_CHECK(nroot >= 1, FCIB_ERR_ARG, "nroot must be >= 1");
+        FCIB_CHECK(root >= 0 && root < nroot, FCIB_ERR_ARG, "root must be < nroot");
+        bool same = (c.na == na && c.nb == nb && c.irrep == irrep);
+        c.na = na; c.nb = nb; c.irrep = irrep; c.multiplicity = multiplicity;
+        c.nroot = nroot; c.root = root;
+        c.has_state = true;
+        if (!same) c.tables_ready = false;
+        c.solved = false;
+    });
+}
+
+int fcib_set_options(fcib_ctx* ctx, const fcib_options* o) {
+    if (!ctx || !o) { set_error("null argument"); return FCIB_ERR_ARG; }
+    return guarded(ctx, [&] {
+        FCIB_CHECK(o->maxiter >= 1, FCIB_ERR_ARG, "maxiter must be >= 1");
+        FCIB_CHECK(o->e_convergence > 0 && o->r_convergence > 0, FCIB_ERR_ARG, "convergence thresholds must be > 0");
+        FCIB_CHECK(o->guess_per_root >= 1 && o->dets_per_guess >= 1, FCIB_ERR_ARG, "guess options must be >= 1");
+        FCIB_CHECK(o->collapse_per_root >= 1, FCIB_ERR_ARG,
+                   "DavidsonLiuSolver: collapse_per_root must be greater or equal to one");
+        FCIB_CHECK(o->subspace_per_root >= o->collapse_per_root + 1, FCIB_ERR_ARG,
+                   "DavidsonLiuSolver: subspace_per_root must be greater or equal to collapse_per_root + 1");
+        FCIB_CHECK(o->precision >= FCIB_PREC_FP64 && o->precision <= FCIB_PREC_MIXED_TF32, FCIB_ERR_ARG, "bad precision mode");
+        FCIB_CHECK(o->preconditioner == FCIB_PRECOND_DIAG || o->preconditioner == FCIB_PRECOND_MLP, FCIB_ERR_ARG,
+                   "bad preconditioner");
+        ctx->c.opt = *o;
+    });
+}
+
+int fcib_size(fcib_ctx* ctx, int64_t* ndet) {
+    if (!ctx || !ndet) { set_error("null argument"); return FCIB_ERR_ARG; }
+    return guarded(ctx, [&] {
+        ensure_setup(ctx->c);
+        *ndet = flat_size(ctx->c);
+    });
+}
+
+int fcib_solve(fcib_ctx* ctx, double* energies, double* spin2, int* iterations) {
+    if (!ctx) { set_error("null context"); return FCIB_ERR_ARG; }
+    int rc = guarded(ctx, [&] {
+        Context& c = ctx->c;
+        ensure_setup(c);
+        dl_solve(c);
+        for (int k = 0; k < c.nroot; k++) {
+            if (energies) energies[k] = c.energies[k];
+            if (spin2) spin2[k] = c.spin2[k];
+        }
+        if (iterations) *iterations = c.iterations;
+    });
+    if (rc == FCIB_OK && !ctx->c.converged && ctx->c.opt.die_if_not_converged) {
+        set_error("Davidson-Liu solver did not converge. Try to increase DL_MAXITER, DL_SUBSPACE_PER_ROOT or DL_GUESS_PER_ROOT");
+        return FCIB_ERR_NOT_CONVERGED;
+    }
+    return rc;
+}
+
+int fcib_get_vector(fcib_ctx* ctx, int root, double* out) {
+    if (!ctx || !out) { set_error("null argument"); return FCIB_ERR_ARG; }
+    return guarded(ctx, [&] {
+        Context& c = ctx->c;
+        FCIB_CHECK(c.solved, FCIB_ERR_STATE, "no solution available");
+        FCIB_CHECK(root >= 0 && root < c.nroot, FCIB_ERR_ARG, "root out of range");
+        download_flat(c, c.b.p + (size_t)root * c.ndet, out);
+    });
+}
+
+int fcib_sigma(fcib_ctx* ctx, const double* b, double* sigma) {
+    if (!ctx || !b || !sigma) { set_error("null argument"); return FCIB_ERR_ARG; }
+    return guarded(ctx, [&] {
+        Context& c = ctx->c;
+        ensure_setup(c);
+        DBuf<double> db, ds;
+        db.alloc(c.ndet);
+        ds.alloc(c.ndet);
+        upload_flat(c, b, db.p);
+        sigma_dispatch(c, db.p, ds.p, c.opt.precision);
+        download_flat(c, ds.p, sigma);
+    });
+}
+
+int fcib_sigma_device(fcib_ctx* ctx, const double* d_b, double* d_sigma, int precision, void* stream) {
+    if (!ctx || !d_b || !d_sigma) { set_error("null argument"); return FCIB_ERR_ARG; }
+    return guarded(ctx, [&] {
+        Context& c = ctx->c;
+        ensure_setup(c);
+        cudaStream_t keep = c.stream;
+        if (stream) c.stream = (cudaStream_t)stream;
+        try {
+            sigma_dispatch(c, d_b, d_sigma, precision);
+        } catch (...) {
+            c.stream = keep;
+            throw;
+        }
+        c.stream = keep;
+    });
+}
+
+int fcib_hdiag(fcib_ctx* ctx, double* out) {
+    if (!ctx || !out) { set_error("null argument"); return FCIB_ERR_ARG; }
+    return guarded(ctx, [&] {
+        ensure_setup(ctx->c);
+        download_flat(ctx->c, ctx->c.hdiag.p, out);
+    });
+}
+
+int fcib_spin2(fcib_ctx* ctx, const double* cvec, double* s2) {
+    if (!ctx || !cvec || !s2) { set_error("null argument"); return FCIB_ERR_ARG; }
+    return guarded(ctx, [&] {
+        Context& c = ctx->c;
+        ensure_setup(c);
+        DBuf<double> d;
+        d.alloc(c.ndet);
+        if (c.nirrep > 1) FCIB_CUDA(cudaMemsetAsync(d.p, 0, sizeof(double) * c.ndet, c.stream));
+        upload_flat(c, cvec, d.p);
+        *s2 = spin2_device(c, d.p);
+    });
+}
+
+int fcib_rdms(fcib_ctx* ctx, int root_left, int root_right, int level, int spin_free, double* g1a,
+              double* g1b, double* g2aa, double* g2ab, double* g2bb) {
+    (void)root_left; (void)root_right; (void)level; (void)spin_free;
+    (void)g1a; (void)g1b; (void)g2aa; (void)g2ab; (void)g2bb;
+    if (!ctx) { set_error("null context"); return FCIB_ERR_ARG; }
+    set_error("fcib_rdms: not available in this build");
+    return FCIB_ERR_UNSUPPORTED;
+}
+
+int fcib_num_strings(fcib_ctx* ctx, int spin, int64_t* count) {
+    if (!ctx || !count) { set_error("null argument"); return FCIB_ERR_ARG; }
+    return guarded(ctx, [&] {
+        ensure_setup(ctx->c);
+        *count = spin ? ctx->c.nbs : ctx->c.nas;
+    });
+}
+
+int fcib_strings(fcib_ctx* ctx, int spin, uint32_t* out) {
+    if (!ctx || !out) { set_error("null argument"); return FCIB_ERR_ARG; }
+    return guarded(ctx, [&] {
+        Context& c = ctx->c;
+        ensure_setup(c);
+        const SpinTables& t = spin ? c.B : c.A;
+        FCIB_CUDA(cudaMemcpy(out, t.str.p, 4 * (size_t)t.nstr, cudaMemcpyDeviceToHost));
+    });
+}
+
+int fcib_string_list(fcib_ctx* ctx, int spin, int kind, int p, int q, int r, int s, int64_t* len,
+                     int8_t* sign, uint32_t* I, uint32_t* J) {
+    if (!ctx || !len) { set_error("null argument"); return FCIB_ERR_ARG; }
+    return guarded(ctx, [&] {
+        Context& c = ctx->c;
+        ensure_setup(c);
+        int n = c.n;
+        FCIB_CHECK(kind >= 0 && kind <= 2, FCIB_ERR_ARG, "kind must be 0 (VO), 1 (OO) or 2 (VVOO)");
+        FCIB_CHECK(p >= 0 && q >= 0 && r >= 0 && s >= 0, FCIB_ERR_ARG, "negative orbital index");
+        if (kind == 0) FCIB_CHECK(p < n && q < n, FCIB_ERR_ARG, "orbital index out of range");
+        if (kind == 1) FCIB_CHECK(p < n * (n - 1) / 2, FCIB_ERR_ARG, "pair index out of range");
+        if (kind == 2)
+            FCIB_CHECK(p < n && q < n && r < n && s < n && p > q && r > s && !(p == r && q == s), FCIB_ERR_ARG,
+                       "VVOO lists need p > q, r > s, (p,q) != (r,s)");
+        std::vector<int8_t> hs;
+        std::vector<uint32_t> hI, hJ;
+        export_list(n, spin ? c.nb : c.na, kind, p, q, r, s, hs, hI, hJ, c.stream);
+        *len = (int64_t)hs.size();
+        if (sign) {
+            std::copy(hs.begin(), hs.end(), sign);
+            if (I) std::copy(hI.begin(), hI.end(), I);
+            if (J) std::copy(hJ.begin(), hJ.end(), J);
+        }
+    });
+}
+
+int fcib_last_timing(fcib_ctx* ctx, double* sigma_ms, int* n_sigma, double* total_ms) {
+    if (!ctx) { set_error("null context"); return FCIB_ERR_ARG; }
+    if (sigma_ms) *sigma_ms = ctx->c.t_sigma_ms;
+    if (n_sigma) *n_sigma = ctx->c.n_sigma;
+    if (total_ms) *total_ms = ctx->c.t_total_ms;
+    return FCIB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,6 @@
+// Single translation unit of the engine: the device constants (binomial table, diagonal
+// integrals) and __device__ helpers are shared by all kernels without relocatable device code.
+#include "strings.cu"
+#include "sigma.cu"
+#include "davidson.cu"
+#include "capi.cu"

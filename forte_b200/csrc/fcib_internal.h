@@ -1,0 +1,164 @@
+// Internal declarations shared by the engine's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/fcib.h"
+
+namespace fcib {
+
+// ------------------------------------------------------------------------------------------
+// error handling: every public entry point returns FCIB_OK or an error code and sets a
+// thread-local message readable with fcib_last_error().
+// ------------------------------------------------------------------------------------------
+struct Error {
+    int code;
+    std::string msg;
+};
+void set_error(const std::string& msg);
+
+#define FCIB_CUDA(call)                                                                          \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess)                                                                   \
+            throw fcib::Error{FCIB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)}; \
+    } while (0)
+
+#define FCIB_CHECK(cond, code, msg)                   \
+    do {                                              \
+        if (!(cond)) throw fcib::Error{(code), (msg)}; \
+    } while (0)
+
+// ------------------------------------------------------------------------------------------
+// device buffers
+// ------------------------------------------------------------------------------------------
+template <typename T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    ~DBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void alloc(size_t count) {
+        if (count == n && p) return;
+        release();
+        if (count == 0) return;
+        FCIB_CUDA(cudaMalloc((void**)&p, count * sizeof(T)));
+        n = count;
+    }
+    void upload(const T* h, size_t count, cudaStream_t s = 0) {
+        alloc(count);
+        if (count) FCIB_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+    }
+    void upload(const std::vector<T>& v, cudaStream_t s = 0) { upload(v.data(), v.size(), s); }
+};
+
+// ------------------------------------------------------------------------------------------
+// string machinery (strings.cu)
+// ------------------------------------------------------------------------------------------
+constexpr int kMaxOrb = 22;          // strings are uint32 masks; addresses fit in 21 bits
+constexpr uint32_t kConnIdxMask = (1u << 21) - 1;
+constexpr uint32_t kSignBit = 0x80000000u;
+constexpr int32_t kNoTarget = 0x7FFFFFFF;
+
+// Binomial table C(i, j) for i, j <= 32 (host and device copies)
+struct Binom {
+    uint32_t c[33][33];
+};
+const Binom& host_binom();
+// rank of a string in the reference enumeration order (colex over reversed orbital positions)
+uint32_t host_rank(uint32_t s, int n);
+uint32_t host_unrank(uint32_t idx, int n, int k);
+
+// Per-spin string tables resident in HBM.
+struct SpinTables {
+    int n = 0, k = 0;
+    int nstr = 0;         // C(n,k)
+    int s1 = 0;           // single-replacement connections per string (diagonal included)
+    int npair = 0;        // unordered pairs with diagonal: n(n+1)/2
+    int npair_pad = 0;    // padded to a multiple of 8
+    DBuf<uint32_t> str;   // [nstr] bit masks in reference order
+    DBuf<uint32_t> conn;  // [nstr * s1]: source J | pair P << 21 | sign << 31 (I = +-F_P J)
+    DBuf<int32_t> tgt;    // [nstr * npair_pad]: F_R J = +-I -> I | sign << 31, or kNoTarget
+    // (N-2)-electron groups for the same-spin two-body term
+    int ng2 = 0, g2 = 0;  // number of groups, rows per group
+    DBuf<uint32_t> g2row; // [ng2 * g2]: row I | sign << 31
+    DBuf<uint16_t> g2lab; // [ng2 * g2]: pair label (p>q) index p(p-1)/2+q
+    // (N-1)-electron groups for the one-body term when it is not folded
+    int ng1 = 0, g1 = 0;
+    DBuf<uint32_t> g1row;
+    DBuf<uint16_t> g1lab;
+};
+void build_spin_tables(SpinTables& t, int n, int k, bool need_g1, cudaStream_t s);
+
+// ------------------------------------------------------------------------------------------
+// engine context
+// ------------------------------------------------------------------------------------------
+struct Context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int num_sms = 0;
+    int smem_optin = 0;   // max dynamic+static shared memory per block
+    int smem_per_sm = 0;
+    // problem
+    int n = 0, nirrep = 1;
+    std::vector<int> orbsym;
+    double scalar = 0.0;
+    std::vector<double> oei_a, oei_b, tei_aa, tei_ab, tei_bb;  // host copies (guess, checks)
+    bool has_ints = false;
+    int na = -1, nb = -1, irrep = 0, multiplicity = 1, nroot = 1, root = 0;
+    bool has_state = false;
+    fcib_options opt;
+    // device tables
+    SpinTables A, B;
+    bool tables_ready = false;
+    int64_t nas = 0, nbs = 0, ndet = 0;
+    DBuf<double> V;       // [npair_pad_a x npair_pad_b] pair-pair (pq|rs) (+ folded h)
+    DBuf<double> M2a, M2b;  // same-spin <pq||rs> over pairs p>q, r>s
+    DBuf<double> Ha, Hb;  // one-body matrices (used when h is not folded)
+    bool fold_h = true;
+    DBuf<uint8_t> mask;   // determinant in target irrep (only when nirrep > 1)
+    // work vectors
+    DBuf<double> ct, st;  // transposed C and sigma for beta same-spin terms
+    DBuf<double> hdiag;
+    // solver storage
+    DBuf<double> b, sig, r, tmp;
+    int subspace = 0;
+    std::vector<double> energies, spin2;
+    int iterations = 0;
+    bool solved = false;
+    // flat-order maps for nirrep > 1 (reference block layout <-> C1 layout)
+    std::vector<int64_t> block_to_c1;
+    DBuf<int> counter;    // work counters for persistent kernels
+    DBuf<double> red;     // reduction scratch
+    // timers and status of the last solve
+    double t_sigma_ms = 0.0;
+    int n_sigma = 0;
+    double t_total_ms = 0.0;
+    bool converged = false;
+};
+
+// kernels / launchers (sigma.cu)
+void prepare_integrals(Context& c);
+void sigma_fp64(Context& c, const double* C, double* S);
+void apply_mask(Context& c, double* v);
+void export_list(int n, int k, int kind, int p, int q, int r, int s, std::vector<int8_t>& sign,
+                 std::vector<uint32_t>& I, std::vector<uint32_t>& J, cudaStream_t st);
+void compute_hdiag(Context& c, double* out);
+void sigma_dispatch(Context& c, const double* b, double* s, int precision);
+void ensure_setup(Context& c);
+// davidson.cu
+void dl_solve(Context& c);
+double spin2_device(Context& c, const double* C);
+
+}  // namespace fcib

@@ -1,0 +1,439 @@
+// FP64 sigma = H C on the device, plus the Hamiltonian diagonal.
+//
+// Reference: FCIVector::Hamiltonian (forte/fci/fci_vector_hamiltonian.cc:46-272) builds
+// sigma as H0 + H1a + H1b + H2ab + H2aa + H2bb with BLAS-1 loops over substitution lists.
+// Here the same operator is regrouped into dense blocks:
+//
+// * opposite spin (+ both one-body terms folded in, + H0):  for a target alpha row Ia,
+//       sigma[Ia, Ib] = sum_{P in conn(Ia)} sgn_P sum_R V[P,R] sum_{Jb} <Ib|F_R|Jb> C[Ja(P), Jb]
+//   with unordered orbital pairs P=(p>=q), F_P = E_pq + E_qp (E_pp on the diagonal) and
+//   V[P,R] = (pq|rs).  One CTA owns a row: it gathers the connected C rows, multiplies the
+//   tile by V[P(Ia), :] and scatters the result over beta single replacements into a sigma
+//   row held in shared memory.  The one-body terms are exact parts of V: on strings with nb
+//   beta electrons sum_r E^b_rr = nb, so h^a_pq E^a_pq = (1/nb) sum_r h^a_pq E^a_pq E^b_rr.
+// * same spin:  a+_p a+_q a_s a_r = sum_K a+_p a+_q |K><K| a_s a_r over (N-2)-electron
+//   strings K, so for each K the 45 (n=16) strings K+{p,q} couple through the dense block
+//   <pq||rs> restricted to the orbitals K leaves empty.  One CTA applies that block to a
+//   column chunk of the gathered rows and adds the result back with atomics.  The beta term
+//   runs on the transposed vector.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+
+#include "fcib_internal.h"
+
+namespace fcib {
+
+// ------------------------------------------------------------------------------------------
+// host-side integral preparation
+// ------------------------------------------------------------------------------------------
+void prepare_integrals(Context& c) {
+    const int n = c.n;
+    const size_t n2 = (size_t)n * n, n3 = n2 * n;
+    auto tab = [&](int p, int q, int r, int s) { return c.tei_ab[p * n3 + q * n2 + r * n + s]; };
+    const int np = n * (n + 1) / 2, npp = (np + 7) / 8 * 8;
+    c.fold_h = (c.na >= 1 && c.nb >= 1);
+    std::vector<double> V((size_t)npp * npp, 0.0);
+    for (int p = 0; p < n; p++)
+        for (int q = 0; q <= p; q++)
+            for (int r = 0; r < n; r++)
+                for (int s = 0; s <= r; s++) {
+                    int P = p * (p + 1) / 2 + q, R = r * (r + 1) / 2 + s;
+                    double v = tab(p, r, q, s);  // <pr|qs> = (pq|rs)
+                    if (c.fold_h) {
+                        if (r == s) v += c.oei_a[p * n + q] / c.nb;
+                        if (p == q) v += c.oei_b[r * n + s] / c.na;
+                    }
+                    V[(size_t)P * npp + R] = v;
+                }
+    c.V.upload(V, c.stream);
+    const int np2 = n * (n - 1) / 2;
+    if (np2 > 0) {
+        std::vector<double> Ma((size_t)np2 * np2), Mb((size_t)np2 * np2);
+        for (int p = 0; p < n; p++)
+            for (int q = 0; q < p; q++)
+                for (int r = 0; r < n; r++)
+                    for (int s = 0; s < r; s++) {
+                        int PQ = p * (p - 1) / 2 + q, RS = r * (r - 1) / 2 + s;
+                        size_t idx = (size_t)p * n3 + q * n2 + r * n + s;
+                        Ma[(size_t)PQ * np2 + RS] = c.tei_aa[idx];
+                        Mb[(size_t)PQ * np2 + RS] = c.tei_bb[idx];
+                    }
+        c.M2a.upload(Ma, c.stream);
+        c.M2b.upload(Mb, c.stream);
+    }
+    c.Ha.upload(c.oei_a, c.stream);
+    c.Hb.upload(c.oei_b, c.stream);
+}
+
+// ------------------------------------------------------------------------------------------
+// opposite-spin kernel (FP64)
+// ------------------------------------------------------------------------------------------
+constexpr int kAbTM = 64;  // beta rows per tile
+constexpr int kAbRows = 8; // tile rows per thread (broadcast operand)
+constexpr int kAbCols = 2; // pair columns per thread
+
+size_t ab_fp64_smem(int nbs, int s1a, int npp) {
+    return (size_t)((nbs + 1) & ~1) * 8 + (size_t)s1a * npp * 8 + (size_t)s1a * kAbTM * 8 + (size_t)s1a * 4 + 16;
+}
+
+__global__ void __launch_bounds__(576) k_ab_fp64(
+    const double* __restrict__ C, double* __restrict__ S, const uint32_t* __restrict__ connA,
+    int s1a, const int32_t* __restrict__ tgtB, int npp, const double* __restrict__ V, int nas,
+    int nbs, double e0, int* __restrict__ row_counter) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    double* srow = reinterpret_cast<double*>(smem);
+    double* Bm = srow + ((nbs + 1) & ~1);          // [s1a][npp], 16-byte aligned
+    double* At = Bm + (size_t)s1a * npp;           // [s1a][kAbTM]
+    uint32_t* cs = reinterpret_cast<uint32_t*>(At + (size_t)s1a * kAbTM);
+    __shared__ int s_row;
+
+    const int tid = threadIdx.x;
+    const int ncg = npp / kAbCols;
+    const int nmt = (kAbTM / kAbRows) * ncg;
+    const int cg = tid % ncg, rg = tid / ncg;
+    const bool active = tid < nmt;
+
+    while (true) {
+        if (tid == 0) s_row = atomicAdd(row_counter, 1);
+        __syncthreads();
+        const int Ia = s_row;
+        if (Ia >= nas) break;
+        for (int k = tid; k < s1a; k += blockDim.x) cs[k] = connA[(size_t)Ia * s1a + k];
+        __syncthreads();
+        for (int idx = tid; idx < s1a * npp; idx += blockDim.x) {
+            int k = idx / npp, R = idx - k * npp;
+            uint32_t e = cs[k];
+            int P = (e >> 21) & 1023;
+            double v = V[(size_t)P * npp + R];
+            Bm[idx] = (e & kSignBit) ? -v : v;
+        }
+        const double* Crow = C + (size_t)Ia * nbs;
+        for (int j = tid; j < nbs; j += blockDim.x) srow[j] = e0 * Crow[j];
+        __syncthreads();
+
+        for (int jb0 = 0; jb0 < nbs; jb0 += kAbTM) {
+            for (int idx = tid; idx < s1a * kAbTM; idx += blockDim.x) {
+                int k = idx / kAbTM, t = idx - k * kAbTM;
+                int jb = jb0 + t;
+                uint32_t J = cs[k] & kConnIdxMask;
+                At[idx] = (jb < nbs) ? C[(size_t)J * nbs + jb] : 0.0;
+            }
+            __syncthreads();
+            if (active) {
+                double acc[kAbRows][kAbCols];
+#pragma unroll
+                for (int i = 0; i < kAbRows; i++)
+#pragma unroll
+                    for (int j = 0; j < kAbCols; j++) acc[i][j] = 0.0;
+                const double* ap = At + rg * kAbRows;
+                const double* bp = Bm + cg * kAbCols;
+#pragma unroll 2
+                for (int k = 0; k < s1a; k++) {
+                    double a[kAbRows];
+                    const double2* a2 = reinterpret_cast<const double2*>(ap + (size_t)k * kAbTM);
+#pragma unroll
+                    for (int i = 0; i < kAbRows / 2; i++) {
+                        double2 t2 = a2[i];
+                        a[2 * i] = t2.x;
+                        a[2 * i + 1] = t2.y;
+                    }
+                    double2 b2 = *reinterpret_cast<const double2*>(bp + (size_t)k * npp);
+#pragma unroll
+                    for (int i = 0; i < kAbRows; i++) {
+                        acc[i][0] = fma(a[i], b2.x, acc[i][0]);
+                        acc[i][1] = fma(a[i], b2.y, acc[i][1]);
+                    }
+                }
+#pragma unroll
+                for (int i = 0; i < kAbRows; i++) {
+                    int jb = jb0 + rg * kAbRows + i;
+                    if (jb < nbs) {
+                        int2 tg = *reinterpret_cast<const int2*>(tgtB + (size_t)jb * npp + cg * kAbCols);
+                        if (tg.x != kNoTarget) {
+                            double v = acc[i][0];
+                            atomicAdd(&srow[tg.x & kConnIdxMask], (tg.x & (int)kSignBit) ? -v : v);
+                        }
+                        if (tg.y != kNoTarget) {
+                            double v = acc[i][1];
+                            atomicAdd(&srow[tg.y & kConnIdxMask], (tg.y & (int)kSignBit) ? -v : v);
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        double* Srow = S + (size_t)Ia * nbs;
+        for (int j = tid; j < nbs; j += blockDim.x) Srow[j] = srow[j];
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// group kernel: sigma[row_i, :] += sgn_i sum_j M[lab_i, lab_j] sgn_j C[row_j, :]  (FP64)
+// one CTA per (group, column chunk)
+// ------------------------------------------------------------------------------------------
+constexpr int kGrTN = 128;   // columns per CTA
+constexpr int kGrRows = 8;   // rows per thread
+
+__global__ void __launch_bounds__(1024) k_group_fp64(
+    const double* __restrict__ C, double* __restrict__ S, int ncols,
+    const uint32_t* __restrict__ rows, const uint16_t* __restrict__ labs, int G, int Gp,
+    const double* __restrict__ M, int ldm) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    double* Wt = reinterpret_cast<double*>(smem);   // [G][Gp]  Wt[j][i] = M[lab_i][lab_j]
+    double* X = Wt + (size_t)G * Gp;                 // [G][kGrTN]
+    uint32_t* rs = reinterpret_cast<uint32_t*>(X + (size_t)G * kGrTN);
+    uint16_t* ls = reinterpret_cast<uint16_t*>(rs + Gp);
+    const int g = blockIdx.x;
+    const int c0 = blockIdx.y * kGrTN;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < Gp; i += blockDim.x) {
+        rs[i] = i < G ? rows[(size_t)g * G + i] : 0u;
+        ls[i] = i < G ? labs[(size_t)g * G + i] : 0;
+    }
+    __syncthreads();
+    for (int idx = tid; idx < G * Gp; idx += blockDim.x) {
+        int j = idx / Gp, i = idx - j * Gp;
+        Wt[idx] = i < G ? M[(size_t)ls[i] * ldm + ls[j]] : 0.0;
+    }
+    for (int idx = tid; idx < G * kGrTN; idx += blockDim.x) {
+        int j = idx / kGrTN, cc = idx - j * kGrTN;
+        int col = c0 + cc;
+        uint32_t e = rs[j];
+        double v = (col < ncols) ? C[(size_t)(e & kConnIdxMask) * ncols + col] : 0.0;
+        X[idx] = (e & kSignBit) ? -v : v;
+    }
+    __syncthreads();
+    const int npairs = kGrTN / 2;
+    const int cp = tid % npairs, rc = tid / npairs;
+    const int i0 = rc * kGrRows;
+    if (i0 < G) {
+        double acc[kGrRows][2];
+#pragma unroll
+        for (int i = 0; i < kGrRows; i++) acc[i][0] = acc[i][1] = 0.0;
+        for (int j = 0; j < G; j++) {
+            const double2* w2 = reinterpret_cast<const double2*>(Wt + (size_t)j * Gp + i0);
+            double w[kGrRows];
+#pragma unroll
+            for (int i = 0; i < kGrRows / 2; i++) {
+                double2 t = w2[i];
+                w[2 * i] = t.x;
+                w[2 * i + 1] = t.y;
+            }
+            double2 x = *reinterpret_cast<const double2*>(X + (size_t)j * kGrTN + 2 * cp);
+#pragma unroll
+            for (int i = 0; i < kGrRows; i++) {
+                acc[i][0] = fma(w[i], x.x, acc[i][0]);
+                acc[i][1] = fma(w[i], x.y, acc[i][1]);
+            }
+        }
+        const int col = c0 + 2 * cp;
+#pragma unroll
+        for (int i = 0; i < kGrRows; i++) {
+            int ii = i0 + i;
+            if (ii < G) {
+                uint32_t e = rs[ii];
+                double* dst = S + (size_t)(e & kConnIdxMask) * ncols + col;
+                double s = (e & kSignBit) ? -1.0 : 1.0;
+                if (col < ncols) atomicAdd(dst, s * acc[i][0]);
+                if (col + 1 < ncols) atomicAdd(dst + 1, s * acc[i][1]);
+            }
+        }
+    }
+}
+
+static void launch_group(Context& c, const double* C, double* S, int ncols, int ngroups, int G,
+                         const uint32_t* rows, const uint16_t* labs, const double* M, int ldm) {
+    if (ngroups == 0 || G == 0) return;
+    int Gp = (G + kGrRows - 1) / kGrRows * kGrRows;
+    size_t smem = (size_t)G * Gp * 8 + (size_t)G * kGrTN * 8 + (size_t)Gp * 4 + (size_t)Gp * 2 + 16;
+    FCIB_CHECK(smem + 1024 <= (size_t)c.smem_optin, FCIB_ERR_UNSUPPORTED, "same-spin group block exceeds shared memory");
+    int threads = (kGrTN / 2) * (Gp / kGrRows);
+    threads = (threads + 31) / 32 * 32;
+    FCIB_CHECK(threads <= 1024, FCIB_ERR_UNSUPPORTED, "same-spin group block too large");
+    FCIB_CUDA(cudaFuncSetAttribute(k_group_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dim3 grid(ngroups, (ncols + kGrTN - 1) / kGrTN);
+    k_group_fp64<<<grid, threads, smem, c.stream>>>(C, S, ncols, rows, labs, G, Gp, M, ldm);
+    FCIB_CUDA(cudaGetLastError());
+}
+
+// ------------------------------------------------------------------------------------------
+// small helpers
+// ------------------------------------------------------------------------------------------
+__global__ void k_transpose(const double* __restrict__ in, double* __restrict__ out, int rows, int cols) {
+    __shared__ double tile[32][33];
+    int x = blockIdx.x * 32 + threadIdx.x;
+    int y0 = blockIdx.y * 32;
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        int y = y0 + j;
+        if (x < cols && y < rows) tile[j][threadIdx.x] = in[(size_t)y * cols + x];
+    }
+    __syncthreads();
+    int ox = y0 + threadIdx.x;
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        int oy = blockIdx.x * 32 + j;
+        if (ox < rows && oy < cols) out[(size_t)oy * rows + ox] = tile[threadIdx.x][j];
+    }
+}
+
+// out[r][c] += in[c][r]; in is [cols][rows]
+__global__ void k_transpose_add(const double* __restrict__ in, double* __restrict__ out, int rows, int cols) {
+    __shared__ double tile[32][33];
+    int x = blockIdx.x * 32 + threadIdx.x;  // index into in's columns (= out rows)
+    int y0 = blockIdx.y * 32;               // in's rows (= out cols)
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        int y = y0 + j;
+        if (x < rows && y < cols) tile[j][threadIdx.x] = in[(size_t)y * rows + x];
+    }
+    __syncthreads();
+    int oc = y0 + threadIdx.x;
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        int orow = blockIdx.x * 32 + j;
+        if (orow < rows && oc < cols) out[(size_t)orow * cols + oc] += tile[threadIdx.x][j];
+    }
+}
+
+__global__ void k_scale_copy(const double* __restrict__ in, double* __restrict__ out, double a, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = a * in[i];
+}
+
+__global__ void k_apply_mask(double* __restrict__ v, const uint8_t* __restrict__ m, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        if (!m[i]) v[i] = 0.0;
+}
+
+static void transpose(Context& c, const double* in, double* out, int rows, int cols) {
+    dim3 grid((cols + 31) / 32, (rows + 31) / 32), block(32, 8);
+    k_transpose<<<grid, block, 0, c.stream>>>(in, out, rows, cols);
+    FCIB_CUDA(cudaGetLastError());
+}
+// out[rows][cols] += transpose(in[cols][rows])
+static void transpose_add(Context& c, const double* in, double* out, int rows, int cols) {
+    dim3 grid((rows + 31) / 32, (cols + 31) / 32), block(32, 8);
+    k_transpose_add<<<grid, block, 0, c.stream>>>(in, out, rows, cols);
+    FCIB_CUDA(cudaGetLastError());
+}
+
+void apply_mask(Context& c, double* v) {
+    if (c.nirrep <= 1 || !c.mask.p) return;
+    k_apply_mask<<<4 * c.num_sms, 256, 0, c.stream>>>(v, c.mask.p, (size_t)c.ndet);
+    FCIB_CUDA(cudaGetLastError());
+}
+
+// ------------------------------------------------------------------------------------------
+// sigma orchestration
+// ------------------------------------------------------------------------------------------
+void sigma_fp64(Context& c, const double* C, double* S) {
+    const int nas = (int)c.nas, nbs = (int)c.nbs;
+    const size_t N = (size_t)c.ndet;
+    if (!c.counter.p) c.counter.alloc(16);
+    if (c.fold_h) {
+        const int s1a = c.A.s1, npp = c.A.npair_pad;
+        size_t smem = ab_fp64_smem(nbs, s1a, npp);
+        FCIB_CHECK(smem + 1024 <= (size_t)c.smem_optin, FCIB_ERR_UNSUPPORTED,
+                   "opposite-spin row block exceeds shared memory (beta string count too large)");
+        FCIB_CUDA(cudaFuncSetAttribute(k_ab_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int threads = (kAbTM / kAbRows) * (npp / kAbCols);
+        threads = (threads + 31) / 32 * 32;
+        FCIB_CHECK(threads <= 576, FCIB_ERR_UNSUPPORTED, "too many orbitals for the FP64 opposite-spin kernel");
+        int per_sm = std::max(1, (int)(c.smem_per_sm / (smem + 1024)));
+        per_sm = std::min(per_sm, 2048 / threads);
+        int grid = std::min(nas, per_sm * c.num_sms);
+        FCIB_CUDA(cudaMemsetAsync(c.counter.p, 0, sizeof(int), c.stream));
+        k_ab_fp64<<<grid, threads, smem, c.stream>>>(C, S, c.A.conn.p, s1a, c.B.tgt.p, npp, c.V.p,
+                                                     nas, nbs, c.scalar, c.counter.p);
+        FCIB_CUDA(cudaGetLastError());
+    } else {
+        k_scale_copy<<<4 * c.num_sms, 256, 0, c.stream>>>(C, S, c.scalar, N);
+        FCIB_CUDA(cudaGetLastError());
+        if (c.A.ng1)
+            launch_group(c, C, S, nbs, c.A.ng1, c.A.g1, c.A.g1row.p, c.A.g1lab.p, c.Ha.p, c.n);
+    }
+    const int np2 = c.n * (c.n - 1) / 2;
+    if (c.A.ng2) launch_group(c, C, S, nbs, c.A.ng2, c.A.g2, c.A.g2row.p, c.A.g2lab.p, c.M2a.p, np2);
+    bool beta_g1 = (!c.fold_h && c.B.ng1);
+    if (c.B.ng2 || beta_g1) {
+        c.ct.alloc(N);
+        c.st.alloc(N);
+        transpose(c, C, c.ct.p, nas, nbs);
+        FCIB_CUDA(cudaMemsetAsync(c.st.p, 0, N * sizeof(double), c.stream));
+        if (beta_g1) launch_group(c, c.ct.p, c.st.p, nas, c.B.ng1, c.B.g1, c.B.g1row.p, c.B.g1lab.p, c.Hb.p, c.n);
+        if (c.B.ng2) launch_group(c, c.ct.p, c.st.p, nas, c.B.ng2, c.B.g2, c.B.g2row.p, c.B.g2lab.p, c.M2b.p, np2);
+        transpose_add(c, c.st.p, S, nas, nbs);
+    }
+    apply_mask(c, S);
+}
+
+// ------------------------------------------------------------------------------------------
+// Hamiltonian diagonal, summed in the order of ActiveSpaceIntegrals::energy
+// (forte/integrals/active_space_integrals.cc:206-245) starting from the scalar energy
+// ------------------------------------------------------------------------------------------
+struct DiagInts {
+    double ha[kMaxOrb], hb[kMaxOrb];
+    double aa[kMaxOrb * kMaxOrb], ab[kMaxOrb * kMaxOrb], bb[kMaxOrb * kMaxOrb];
+};
+__constant__ DiagInts d_diag;
+
+__global__ void k_hdiag(const uint32_t* __restrict__ sa, const uint32_t* __restrict__ sb, int nas,
+                        int nbs, int n, double e0, double* __restrict__ out, size_t N) {
+    for (size_t I = blockIdx.x * (size_t)blockDim.x + threadIdx.x; I < N; I += (size_t)gridDim.x * blockDim.x) {
+        uint32_t Ia = sa[I / nbs], Ib = sb[I % nbs];
+        double e = e0;
+        uint32_t a = Ia;
+        while (a) {
+            int p = __ffs(a) - 1;
+            a &= a - 1;
+            e = __dadd_rn(e, d_diag.ha[p]);
+            uint32_t ac = a;
+            while (ac) {
+                int q = __ffs(ac) - 1;
+                ac &= ac - 1;
+                e = __dadd_rn(e, d_diag.aa[p * n + q]);
+            }
+            uint32_t bc = Ib;
+            while (bc) {
+                int q = __ffs(bc) - 1;
+                bc &= bc - 1;
+                e = __dadd_rn(e, d_diag.ab[p * n + q]);
+            }
+        }
+        uint32_t b = Ib;
+        while (b) {
+            int p = __ffs(b) - 1;
+            b &= b - 1;
+            e = __dadd_rn(e, d_diag.hb[p]);
+            uint32_t bc = b;
+            while (bc) {
+                int q = __ffs(bc) - 1;
+                bc &= bc - 1;
+                e = __dadd_rn(e, d_diag.bb[p * n + q]);
+            }
+        }
+        out[I] = e;
+    }
+}
+
+void compute_hdiag(Context& c, double* out) {
+    DiagInts d;
+    memset(&d, 0, sizeof(d));
+    const int n = c.n;
+    const size_t n2 = (size_t)n * n, n3 = n2 * n;
+    for (int p = 0; p < n; p++) {
+        d.ha[p] = c.oei_a[p * n + p];
+        d.hb[p] = c.oei_b[p * n + p];
+        for (int q = 0; q < n; q++) {
+            size_t idx = p * n3 + q * n2 + p * n + q;
+            d.aa[p * n + q] = c.tei_aa[idx];
+            d.ab[p * n + q] = c.tei_ab[idx];
+            d.bb[p * n + q] = c.tei_bb[idx];
+        }
+    }
+    FCIB_CUDA(cudaMemcpyToSymbolAsync(d_diag, &d, sizeof(d), 0, cudaMemcpyHostToDevice, c.stream));
+    k_hdiag<<<8 * c.num_sms, 256, 0, c.stream>>>(c.A.str.p, c.B.str.p, (int)c.nas, (int)c.nbs, n,
+                                                c.scalar, out, (size_t)c.ndet);
+    FCIB_CUDA(cudaGetLastError());
+}
+
+}  // namespace fcib

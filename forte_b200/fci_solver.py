@@ -1,0 +1,265 @@
+"""FCISolver: the B200 engine behind Forte's ActiveSpaceMethod interface.
+
+Mirrors forte::FCISolver (forte/fci/fci_solver.h:51-246) and the ActiveSpaceMethod contract
+(forte/base_classes/active_space_method.h:95-388): same option names and defaults
+(forte/options.yaml), ``compute_energy()`` returning the energy of ``root``, ``energies()``,
+``spin2()``, ``evals()``, ``evecs()`` in FCIVector flat order, ``rdms(root_list,
+max_rdm_level, rdm_type)`` and the set_* convergence knobs.  Errors surface as RuntimeError
+subclasses like the reference's std::runtime_error.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import capi
+from .integrals import ActiveSpaceIntegrals
+
+
+@dataclass(frozen=True)
+class StateInfo:
+    """Active-space state: electron counts, 2S+1, 2*Ms and irrep (forte StateInfo)."""
+    na: int
+    nb: int
+    multiplicity: int = 1
+    twice_ms: int = 0
+    irrep: int = 0
+
+
+#: Forte option names understood by FCISolver.set_options with their defaults
+DEFAULT_OPTIONS = {
+    "DL_MAXITER": 100,
+    "E_CONVERGENCE": 1.0e-9,
+    "R_CONVERGENCE": 1.0e-6,
+    "DL_GUESS_PER_ROOT": 1,
+    "DL_DETS_PER_GUESS": 50,
+    "DL_COLLAPSE_PER_ROOT": 2,
+    "DL_SUBSPACE_PER_ROOT": 10,
+    "ROOT": 0,
+    "PRINT": 0,
+    # engine-specific knobs
+    "FCI_PRECISION": "FP64",        # FP64 | MIXED | MIXED_TF32
+    "FCI_PRECONDITIONER": "DIAG",   # DIAG | MLP
+    "FCI_MIXED_SWITCH": 1.0e-4,
+}
+
+
+class RDMs:
+    """Spin-dependent (g1a, g1b, g2aa, g2ab, g2bb) or spin-free (g1, g2) RDMs."""
+
+    def __init__(self, spin_free, **t):
+        self.spin_free = spin_free
+        self.__dict__.update(t)
+
+
+class FCISolver:
+    def __init__(self, state: StateInfo, nroot: int, ints: ActiveSpaceIntegrals, options=None, device=0):
+        L = capi.lib()
+        h = C.c_void_p()
+        capi.check(L.fcib_create(C.byref(h), device))
+        self._h = h
+        self.state = state
+        self.nroot = nroot
+        self.ints = ints
+        self._opts = dict(DEFAULT_OPTIONS)
+        self._die = False
+        self._energies = None
+        self._spin2 = None
+        self._iterations = 0
+        self.set_integrals(ints)
+        self._root = 0
+        if options:
+            self.set_options(options)
+        self._push_state()
+
+    def __del__(self):
+        try:
+            if getattr(self, "_h", None):
+                capi.lib().fcib_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+    # ---- configuration -------------------------------------------------------------------
+    def set_integrals(self, ints: ActiveSpaceIntegrals):
+        self.ints = ints
+        n = ints.n
+        self._keep = [np.ascontiguousarray(x, dtype=np.float64) for x in
+                      (ints.oei_a, ints.oei_b, ints.tei_aa, ints.tei_ab, ints.tei_bb)]
+        nirrep = max(ints.orbsym) + 1 if ints.orbsym else 1
+        nirrep = 1 << (nirrep - 1).bit_length() if nirrep > 1 else 1
+        osym = (C.c_int * n)(*ints.orbsym)
+        capi.check(capi.lib().fcib_set_integrals(self._h, n, nirrep, osym, float(ints.scalar),
+                                                 *[capi.dptr(x) for x in self._keep]))
+        self._nirrep = nirrep
+
+    def _push_state(self):
+        s = self.state
+        capi.check(capi.lib().fcib_set_state(self._h, s.na, s.nb, s.irrep, s.multiplicity, self.nroot,
+                                             self._root))
+        self._push_options()
+
+    def _push_options(self):
+        o = capi.default_options()
+        d = self._opts
+        o.maxiter = int(d["DL_MAXITER"])
+        o.e_convergence = float(d["E_CONVERGENCE"])
+        o.r_convergence = float(d["R_CONVERGENCE"])
+        o.guess_per_root = int(d["DL_GUESS_PER_ROOT"])
+        o.dets_per_guess = int(d["DL_DETS_PER_GUESS"])
+        o.collapse_per_root = int(d["DL_COLLAPSE_PER_ROOT"])
+        o.subspace_per_root = int(d["DL_SUBSPACE_PER_ROOT"])
+        o.die_if_not_converged = 1 if self._die else 0
+        o.print_ = int(d["PRINT"])
+        o.precision = {"FP64": capi.PREC_FP64, "MIXED": capi.PREC_MIXED,
+                       "MIXED_TF32": capi.PREC_MIXED_TF32}[str(d["FCI_PRECISION"]).upper()]
+        o.preconditioner = {"DIAG": capi.PRECOND_DIAG, "MLP": capi.PRECOND_MLP}[str(d["FCI_PRECONDITIONER"]).upper()]
+        o.mixed_switch = float(d["FCI_MIXED_SWITCH"])
+        capi.check(capi.lib().fcib_set_options(self._h, C.byref(o)))
+
+    def set_options(self, options: dict):
+        """FCISolver::set_options (forte/fci/fci_solver.cc:156-172)."""
+        for k, v in options.items():
+            K = k.upper()
+            if K not in DEFAULT_OPTIONS:
+                raise KeyError(f"unknown FCI option {k}")
+            self._opts[K] = v
+        self._root = int(self._opts["ROOT"])
+        if self._root >= self.nroot:
+            raise RuntimeError(f"ROOT ({self._root}) must be smaller than nroot ({self.nroot})")
+        self._push_state()
+
+    def set_e_convergence(self, v):
+        self.set_options({"E_CONVERGENCE": v})
+
+    def set_r_convergence(self, v):
+        self.set_options({"R_CONVERGENCE": v})
+
+    def set_maxiter(self, v):
+        self.set_options({"DL_MAXITER": v})
+
+    def set_root(self, v):
+        self.set_options({"ROOT": v})
+
+    def set_print(self, v):
+        self.set_options({"PRINT": v})
+
+    def set_die_if_not_converged(self, v: bool):
+        self._die = bool(v)
+        self._push_options()
+
+    # ---- results ---------------------------------------------------------------------------
+    def size(self) -> int:
+        n = C.c_int64()
+        capi.check(capi.lib().fcib_size(self._h, C.byref(n)))
+        return n.value
+
+    def compute_energy(self) -> float:
+        """FCISolver::compute_energy (forte/fci/fci_solver.cc:177-314)."""
+        e = np.zeros(self.nroot)
+        s2 = np.zeros(self.nroot)
+        it = C.c_int()
+        rc = capi.lib().fcib_solve(self._h, capi.dptr(e), capi.dptr(s2), C.byref(it))
+        if rc == capi.FCIB_ERR_NOT_CONVERGED:
+            raise RuntimeError("Davidson-Liu solver did not converge.\nPlease try to increase the number of "
+                               "Davidson-Liu iterations (DL_MAXITER).")
+        capi.check(rc)
+        self._energies, self._spin2, self._iterations = e, s2, it.value
+        return float(e[self._root])
+
+    def energies(self):
+        return list(self._energies)
+
+    def evals(self):
+        return np.array(self._energies)
+
+    def spin2(self):
+        return list(self._spin2)
+
+    def iterations(self):
+        return self._iterations
+
+    def evecs(self) -> np.ndarray:
+        N = self.size()
+        out = np.zeros((self.nroot, N))
+        for r in range(self.nroot):
+            capi.check(capi.lib().fcib_get_vector(self._h, r, capi.dptr(out[r])))
+        return out
+
+    def sigma(self, b: np.ndarray) -> np.ndarray:
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        s = np.zeros_like(b)
+        capi.check(capi.lib().fcib_sigma(self._h, capi.dptr(b), capi.dptr(s)))
+        return s
+
+    def hdiag(self) -> np.ndarray:
+        out = np.zeros(self.size())
+        capi.check(capi.lib().fcib_hdiag(self._h, capi.dptr(out)))
+        return out
+
+    def compute_spin2(self, c) -> float:
+        c = np.ascontiguousarray(c, dtype=np.float64)
+        s = C.c_double()
+        capi.check(capi.lib().fcib_spin2(self._h, capi.dptr(c), C.byref(s)))
+        return s.value
+
+    def timing(self):
+        sm = C.c_double()
+        ns = C.c_int()
+        tt = C.c_double()
+        capi.check(capi.lib().fcib_last_timing(self._h, C.byref(sm), C.byref(ns), C.byref(tt)))
+        return {"sigma_ms": sm.value, "n_sigma": ns.value, "total_ms": tt.value}
+
+    def rdms(self, root_list, max_rdm_level=2, rdm_type="spin_dependent"):
+        """FCISolver::rdms (forte/fci/fci_solver_rdms.cc:40-64)."""
+        if max_rdm_level > 2:
+            raise RuntimeError("RDMs of order 3 or higher are not implemented in this engine")
+        n = self.ints.n
+        out = []
+        sf = rdm_type in ("spin_free", 1)
+        for (rl, rr) in root_list:
+            if rl >= self.nroot or rr >= self.nroot:
+                raise RuntimeError(f"FCISolver::rdms: root {max(rl, rr)} is larger than the number of "
+                                   f"computed roots ({self.nroot})")
+            g1a = np.zeros((n, n)); g1b = np.zeros((n, n))
+            g2aa = np.zeros((n,) * 4); g2ab = np.zeros((n,) * 4); g2bb = np.zeros((n,) * 4)
+            capi.check(capi.lib().fcib_rdms(self._h, rl, rr, max_rdm_level, 1 if sf else 0,
+                                            capi.dptr(g1a), capi.dptr(g1b), capi.dptr(g2aa),
+                                            capi.dptr(g2ab), capi.dptr(g2bb)))
+            if sf:
+                out.append(RDMs(True, g1=g1a, g2=g2aa if max_rdm_level > 1 else None))
+            else:
+                out.append(RDMs(False, g1a=g1a, g1b=g1b, g2aa=g2aa, g2ab=g2ab, g2bb=g2bb))
+        return out
+
+    # ---- string tables (parity checks) ----------------------------------------------------
+    def strings(self, spin):
+        cnt = C.c_int64()
+        capi.check(capi.lib().fcib_num_strings(self._h, spin, C.byref(cnt)))
+        out = np.zeros(cnt.value, dtype=np.uint32)
+        capi.check(capi.lib().fcib_strings(self._h, spin, out.ctypes.data_as(C.POINTER(C.c_uint32))))
+        return out
+
+    def string_list(self, spin, kind, p=0, q=0, r=0, s=0):
+        ln = C.c_int64()
+        L = capi.lib()
+        capi.check(L.fcib_string_list(self._h, spin, kind, p, q, r, s, C.byref(ln), None, None, None))
+        n = ln.value
+        sg = np.zeros(max(n, 1), dtype=np.int8)
+        I = np.zeros(max(n, 1), dtype=np.uint32)
+        J = np.zeros(max(n, 1), dtype=np.uint32)
+        capi.check(L.fcib_string_list(self._h, spin, kind, p, q, r, s, C.byref(ln),
+                                      sg.ctypes.data_as(C.POINTER(C.c_int8)),
+                                      I.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                      J.ctypes.data_as(C.POINTER(C.c_uint32))))
+        return sg[:n], I[:n], J[:n]
+
+
+def make_active_space_method(method: str, state: StateInfo, nroot: int, ints: ActiveSpaceIntegrals,
+                             options=None, device=0):
+    """make_active_space_method (forte/base_classes/active_space_method.cc:126-184), FCI only."""
+    if method.upper() != "FCI":
+        raise ValueError(f"active space method {method} is not provided by the B200 engine")
+    return FCISolver(state, nroot, ints, options, device)

@@ -1,0 +1,131 @@
+/*
+ * fcib.h -- C ABI of the B200 determinant-space FCI engine.
+ *
+ * Plain C types only (no CUDA or torch types).  Every function returns FCIB_OK (0) or a
+ * negative error code; fcib_last_error() returns the calling thread's last message.
+ * Host-buffer entry points take and return host memory; *_device entry points take device
+ * pointers in the engine's C1 layout and a CUDA stream handle passed as void*.
+ *
+ * Each entry point replaces a piece of Forte's FCISolver path (paths relative to the Forte
+ * project root):
+ *   fcib_create/destroy     -- FCISolver construction (forte/fci/fci_solver.cc:57-64)
+ *   fcib_set_integrals      -- ActiveSpaceIntegrals input (forte/integrals/active_space_integrals.h:103-120,
+ *                              make_active_space_ints active_space_integrals.cc:553-592)
+ *   fcib_set_state          -- StateInfo / nroot / root (active_space_method.h:105, fci_solver.h:87-122)
+ *   fcib_set_options        -- FCISolver::set_options (forte/fci/fci_solver.cc:156-172)
+ *   fcib_solve              -- FCISolver::compute_energy (forte/fci/fci_solver.cc:177-314)
+ *   fcib_get_vector         -- eigenvector rows of DavidsonLiuSolver::eigenvectors (davidson_liu_solver.h:86)
+ *                              in FCIVector flat order (forte/fci/fci_vector.cc:139-169)
+ *   fcib_sigma              -- the sigma builder FCIVector::Hamiltonian (fci_vector_hamiltonian.cc:46-82)
+ *   fcib_hdiag              -- FCISolver::form_Hdiag_det (fci_solver_initial_guess.cc:151-172)
+ *   fcib_rdms               -- FCISolver::rdms / FCIVector::compute_rdms (fci_solver_rdms.cc:40-104,
+ *                              fci_vector_rdm.cc:43-393)
+ *   fcib_spin2              -- FCIVector::compute_spin2 (fci_vector_spin2.cc:38-75)
+ *   fcib_strings / fcib_string_list -- FCIStringLists strings and VO/OO/VVOO lists
+ *                              (fci_string_lists.cc:52-205, fci_string_vo_list.cc:54-140,
+ *                              fci_string_oo_list.cc:59-115, fci_string_vvoo_list.cc:56-187)
+ */
+#ifndef FCIB_H
+#define FCIB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FCIB_OK 0
+#define FCIB_ERR_ARG -1        /* invalid argument */
+#define FCIB_ERR_STATE -2      /* call out of order (e.g. solve before set_integrals) */
+#define FCIB_ERR_CUDA -3       /* CUDA runtime failure */
+#define FCIB_ERR_UNSUPPORTED -4 /* size or feature outside the engine's range */
+#define FCIB_ERR_NOT_CONVERGED -5 /* Davidson-Liu did not converge and die_if_not_converged */
+#define FCIB_ERR_NUMERIC -6    /* non-finite values or a failed numerical invariant */
+
+/* precision of the sigma build */
+#define FCIB_PREC_FP64 0       /* everything in FP64 */
+#define FCIB_PREC_MIXED 1      /* tensor-core TF32x3 sigma, FP64 subspace/residual/final energy */
+#define FCIB_PREC_MIXED_TF32 2 /* single-pass TF32 sigma for the early iterations */
+
+/* Davidson correction-vector preconditioner */
+#define FCIB_PRECOND_DIAG 0    /* r_I / (lambda - H_II), the reference's */
+#define FCIB_PRECOND_MLP 1     /* learned per-determinant MLP correction on top of the diagonal */
+
+typedef struct fcib_options {
+    int maxiter;               /* DL_MAXITER (default 100) */
+    double e_convergence;      /* E_CONVERGENCE (default 1e-9) */
+    double r_convergence;      /* R_CONVERGENCE (default 1e-6) */
+    int guess_per_root;        /* DL_GUESS_PER_ROOT (default 1) */
+    int dets_per_guess;        /* DL_DETS_PER_GUESS (default 50) */
+    int collapse_per_root;     /* DL_COLLAPSE_PER_ROOT (default 2) */
+    int subspace_per_root;     /* DL_SUBSPACE_PER_ROOT (default 10) */
+    int die_if_not_converged;  /* throw on non-convergence (ActiveSpaceMethod::set_die_if_not_converged) */
+    int print;                 /* PRINT level: 0 quiet, 1 iteration table to stdout */
+    int precision;             /* FCIB_PREC_* */
+    int preconditioner;        /* FCIB_PRECOND_* */
+    double mixed_switch;       /* mixed modes: residual norm at which sigma switches to FP64 */
+} fcib_options;
+
+typedef struct fcib_ctx fcib_ctx;
+
+/* defaults of Forte's options.yaml for the FCI solver */
+void fcib_default_options(fcib_options* opt);
+const char* fcib_last_error(void);
+const char* fcib_version(void);
+
+int fcib_create(fcib_ctx** ctx, int device);
+int fcib_destroy(fcib_ctx* ctx);
+
+/* n active orbitals; orbsym[n] irreps (psi4 order, NULL = C1); scalar = nuclear repulsion +
+ * scalar + frozen-core energy; oei_*[n*n]; tei_aa/bb[n^4] = <pq||rs>; tei_ab[n^4] = <pq|rs>
+ * (row-major p,q,r,s).  The integrals must be real (8-fold symmetric two-electron block). */
+int fcib_set_integrals(fcib_ctx* ctx, int n, int nirrep, const int* orbsym, double scalar,
+                       const double* oei_a, const double* oei_b, const double* tei_aa,
+                       const double* tei_ab, const double* tei_bb);
+/* na/nb active alpha/beta electrons, target irrep, multiplicity (2S+1) used to select the
+ * guess, number of roots and the root returned by the solver's energy. */
+int fcib_set_state(fcib_ctx* ctx, int na, int nb, int irrep, int multiplicity, int nroot, int root);
+int fcib_set_options(fcib_ctx* ctx, const fcib_options* opt);
+
+/* determinant-space size in FCIVector flat order (sum over irrep blocks) */
+int fcib_size(fcib_ctx* ctx, int64_t* ndet);
+
+/* Runs the Davidson-Liu FCI.  energies[nroot], spin2[nroot] (either may be NULL), iterations
+ * (may be NULL).  Returns FCIB_ERR_NOT_CONVERGED when the solver did not converge and
+ * die_if_not_converged is set (the results are still stored). */
+int fcib_solve(fcib_ctx* ctx, double* energies, double* spin2, int* iterations);
+/* eigenvector of a root in FCIVector flat order (size from fcib_size) */
+int fcib_get_vector(fcib_ctx* ctx, int root, double* out);
+
+/* sigma = H b for a host vector in FCIVector flat order */
+int fcib_sigma(fcib_ctx* ctx, const double* b, double* sigma);
+/* sigma for device vectors in the engine's C1 layout (na_str x nb_str row-major), on a
+ * stream (void* = cudaStream_t, NULL = the context's stream); precision = FCIB_PREC_* */
+int fcib_sigma_device(fcib_ctx* ctx, const double* d_b, double* d_sigma, int precision, void* stream);
+/* diagonal of H in FCIVector flat order */
+int fcib_hdiag(fcib_ctx* ctx, double* out);
+/* <S^2> of a host vector in FCIVector flat order */
+int fcib_spin2(fcib_ctx* ctx, const double* c, double* s2);
+
+/* Reduced density matrices between roots (root_left, root_right) of the last solve:
+ * level 1 or 2.  spin_free = 0: g1a, g1b [n*n]; g2aa, g2ab, g2bb [n^4] (NULL to skip);
+ * spin_free = 1: g1a <- g1a + g1b and g2aa <- g2aa + g2ab + g2ab(qpsr) + g2bb. */
+int fcib_rdms(fcib_ctx* ctx, int root_left, int root_right, int level, int spin_free,
+              double* g1a, double* g1b, double* g2aa, double* g2ab, double* g2bb);
+
+/* String tables for parity checks.  spin 0 = alpha, 1 = beta. */
+int fcib_num_strings(fcib_ctx* ctx, int spin, int64_t* count);
+int fcib_strings(fcib_ctx* ctx, int spin, uint32_t* out);
+/* Substitution list in the reference's order: kind 0 = VO(p,q), 1 = OO(pair index p),
+ * 2 = VVOO(p,q,r,s).  With sign == NULL only *len is written. */
+int fcib_string_list(fcib_ctx* ctx, int spin, int kind, int p, int q, int r, int s,
+                     int64_t* len, int8_t* sign, uint32_t* I, uint32_t* J);
+
+/* timing of the last solve: total sigma milliseconds and number of sigma builds */
+int fcib_last_timing(fcib_ctx* ctx, double* sigma_ms, int* n_sigma, double* total_ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FCIB_H */

@@ -1104,6 +1104,26 @@ static int make_guess(orc_ctx* c, const double* hdiag, int num_guess_states, int
         if (gm[g] == multiplicity) target = g;
     }
     int ret = num_guess_states;
+    if (multiplicity == 0) {
+        /* extension used by the synthetic benchmarks: no spin selection, the lowest states of the
+         * guess Hamiltonian of any multiplicity, nothing projected out */
+        double* Hc = (double*)malloc(sizeof(double) * nd * nd);
+        double* ev = (double*)malloc(sizeof(double) * nd);
+        double* evv = (double*)malloc(sizeof(double) * nd * nd);
+        memcpy(Hc, H, sizeof(double) * nd * nd);
+        orc_jacobi(nd, Hc, ev, evv);
+        if (nd < num_guess_states) { ret = fail("guess space smaller than the number of guess states"); }
+        else {
+            double* G = (double*)calloc((size_t)N * num_guess_states, sizeof(double));
+            for (int r = 0; r < num_guess_states; r++)
+                for (int i = 0; i < nd; i++) G[(int64_t)r * N + pos[i]] = evv[i * nd + r];
+            *guesses_out = G;
+            *nbad_out = 0;
+            *bad_out = NULL;
+        }
+        free(Hc); free(ev); free(evv);
+        goto done;
+    }
     if (target < 0) { ret = fail("No guess with the requested multiplicity was found."); goto done; }
     if (gsz[target] < num_guess_states) {
         ret = fail("Found fewer guesses with the requested multiplicity than requested; increase DL_DETS_PER_GUESS");
