@@ -68,6 +68,8 @@ void ensure_setup(Context& c) {
     if (c.tables_ready) return;
     FCIB_CHECK(c.na <= c.n && c.nb <= c.n, FCIB_ERR_ARG, "more electrons than orbitals");
     bool fold = (c.na >= 1 && c.nb >= 1);
+    c.tgtR16.release();
+    c.vmax = 0.0f;
     build_spin_tables(c.A, c.n, c.na, !fold, c.stream);
     build_spin_tables(c.B, c.n, c.nb, !fold, c.stream);
     c.nas = c.A.nstr;
@@ -83,8 +85,10 @@ void ensure_setup(Context& c) {
 }
 
 void sigma_dispatch(Context& c, const double* b, double* s, int precision) {
-    (void)precision;
-    sigma_fp64(c, b, s);
+    if (precision == FCIB_PREC_FP64) sigma_fp64(c, b, s);
+    else if (precision == FCIB_PREC_MIXED) sigma_mixed(c, b, s, true);
+    else if (precision == FCIB_PREC_MIXED_TF32) sigma_mixed(c, b, s, false);
+    else throw Error{FCIB_ERR_ARG, "unknown sigma precision"};
 }
 
 // host flat (FCIVector order) <-> device C1 layout

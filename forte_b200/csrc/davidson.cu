@@ -20,114 +20,201 @@
 
 namespace fcib {
 
-constexpr int kMaxV = 32;
-struct VecSet {
-    const double* p[kMaxV];
-    double coef[kMaxV];
+constexpr int kRedThreads = 256;
+constexpr int kMaxIn = 64;     // input vectors per fused pass
+constexpr int kMaxOut = 4;     // output vectors per fused pass
+constexpr int kSlots = 2 * kMaxOut + kMaxIn + 1;  // partial sums per block
+
+// d_j = V_j . (sel_j ? x1 : x0) for j < nv, plus x0 . x0 when self != 0 (slot kMaxIn)
+struct DotArgs {
+    const double* v[kMaxIn];
+    unsigned long long sel;
+    int nv, self;
+    const double* x0;
+    const double* x1;
 };
 
-constexpr int kRedThreads = 256;
-
-// partial[block][j] = sum_I V_j[I] * x[I]   (j < nv); slot nv holds x.x when self != 0
-__global__ void __launch_bounds__(kRedThreads) k_multidot(VecSet vs, int nv, const double* __restrict__ x,
-                                                          size_t N, int self, double* __restrict__ partial) {
-    double acc[kMaxV + 1];
+template <int NV>
+__global__ void __launch_bounds__(kRedThreads) k_dots(DotArgs a, size_t N, double* __restrict__ partial) {
+    double acc[NV + 1];
 #pragma unroll
-    for (int j = 0; j <= kMaxV; j++) acc[j] = 0.0;
-    for (size_t I = blockIdx.x * (size_t)blockDim.x + threadIdx.x; I < N; I += (size_t)gridDim.x * blockDim.x) {
-        double xv = x[I];
+    for (int j = 0; j <= NV; j++) acc[j] = 0.0;
+    const size_t G = (size_t)gridDim.x * blockDim.x;
+    size_t I = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    // four elements per thread per step, all loads issued before the FMAs
+    for (; I + 3 * G < N; I += 4 * G) {
+        double x0[4], x1[4];
 #pragma unroll
-        for (int j = 0; j < kMaxV; j++)
-            if (j < nv) acc[j] = fma(vs.p[j][I], xv, acc[j]);
-        if (self) acc[kMaxV] = fma(xv, xv, acc[kMaxV]);
+        for (int u = 0; u < 4; u++) {
+            x0[u] = a.x0[I + u * G];
+            x1[u] = a.x1 ? a.x1[I + u * G] : 0.0;
+        }
+#pragma unroll
+        for (int j = 0; j < NV; j++) {
+            if (j < a.nv) {
+                double v[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) v[u] = a.v[j][I + u * G];
+                const bool s1 = (a.sel >> j) & 1ull;
+#pragma unroll
+                for (int u = 0; u < 4; u++) acc[j] = fma(v[u], s1 ? x1[u] : x0[u], acc[j]);
+            }
+        }
+        if (a.self)
+#pragma unroll
+            for (int u = 0; u < 4; u++) acc[NV] = fma(x0[u], x0[u], acc[NV]);
     }
-    __shared__ double red[kRedThreads / 32][kMaxV + 1];
+    for (; I < N; I += G) {
+        double x0 = a.x0[I];
+        double x1 = a.x1 ? a.x1[I] : 0.0;
+#pragma unroll
+        for (int j = 0; j < NV; j++)
+            if (j < a.nv) acc[j] = fma(a.v[j][I], ((a.sel >> j) & 1ull) ? x1 : x0, acc[j]);
+        if (a.self) acc[NV] = fma(x0, x0, acc[NV]);
+    }
+    __shared__ double red[kRedThreads / 32][NV + 1];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-    for (int j = 0; j <= kMaxV; j++) {
-        if (j < nv || (j == kMaxV && self)) {
+    for (int j = 0; j <= NV; j++) {
+        if (j < a.nv || (j == NV && a.self)) {
             double v = acc[j];
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
             if (lane == 0) red[warp][j] = v;
         }
     }
     __syncthreads();
-    if (threadIdx.x <= kMaxV) {
-        int j = threadIdx.x;
-        if (j < nv || (j == kMaxV && self)) {
-            double s = 0.0;
-            for (int w = 0; w < kRedThreads / 32; w++) s += red[w][j];
-            partial[(size_t)blockIdx.x * (kMaxV + 1) + j] = s;
+    for (int j = threadIdx.x; j <= NV; j += blockDim.x) {
+        if (j < a.nv || (j == NV && a.self)) {
+            double t = 0.0;
+            for (int w = 0; w < kRedThreads / 32; w++) t += red[w][j];
+            partial[(size_t)blockIdx.x * kSlots + (j < NV ? j : kMaxIn)] = t;
         }
     }
 }
 
-__global__ void k_reduce_partials(const double* __restrict__ partial, int nblocks, int nv, int self,
-                                  double* __restrict__ out) {
-    int j = threadIdx.x;
-    if (j <= kMaxV && (j < nv || (j == kMaxV && self))) {
-        double s = 0.0;
-        for (int b = 0; b < nblocks; b++) s += partial[(size_t)b * (kMaxV + 1) + j];
-        out[j] = s;
-    }
-}
+// out_k = beta*out_k + sum_j coef[k][j] V_j (k < nout); optional diagonal preconditioning
+// corr_k = out_k / (lambda_k - hd) (0 when |lambda_k - hd| <= 1e-6) written instead of out_k.
+// partial slots: 2k = out_k.out_k (before preconditioning), 2k+1 = corr_k.corr_k
+struct ComboArgs {
+    const double* v[kMaxIn];
+    double coef[kMaxOut][kMaxIn];
+    double* out[kMaxOut];
+    double lambda[kMaxOut];
+    const double* hd;
+    int nv, nout, precond;
+    double beta;
+};
 
-// out[I] = beta * out[I] + sum_j coef_j V_j[I]; optional partial sums of out^2
-__global__ void __launch_bounds__(kRedThreads) k_lincomb(VecSet vs, int nv, double* __restrict__ out, double beta,
-                                                         size_t N, double* __restrict__ partial) {
-    double nrm = 0.0;
-    for (size_t I = blockIdx.x * (size_t)blockDim.x + threadIdx.x; I < N; I += (size_t)gridDim.x * blockDim.x) {
-        double v = (beta == 0.0) ? 0.0 : beta * out[I];
+template <int NV, int NO>
+__device__ __forceinline__ void combo_elem(const ComboArgs& a, size_t I, double hd, double (&acc)[2 * NO],
+                                           const double (&o)[NO]) {
 #pragma unroll
-        for (int j = 0; j < kMaxV; j++)
-            if (j < nv) v = fma(vs.coef[j], vs.p[j][I], v);
-        out[I] = v;
-        nrm = fma(v, v, nrm);
-    }
-    if (partial) {
-        __shared__ double red[kRedThreads / 32];
-        for (int o = 16; o > 0; o >>= 1) nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
-        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = nrm;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double s = 0.0;
-            for (int w = 0; w < kRedThreads / 32; w++) s += red[w];
-            partial[(size_t)blockIdx.x * (kMaxV + 1)] = s;
+    for (int k = 0; k < NO; k++) {
+        if (k < a.nout) {
+            acc[2 * k] = fma(o[k], o[k], acc[2 * k]);
+            double w = o[k];
+            if (a.precond) {
+                double den = a.lambda[k] - hd;
+                w = (fabs(den) > 1.0e-6) ? o[k] / den : 0.0;
+            }
+            a.out[k][I] = w;
+            acc[2 * k + 1] = fma(w, w, acc[2 * k + 1]);
         }
     }
 }
 
-// corr = r / (lambda - H_II) (0 when |lambda - H_II| <= 1e-6); partial[b][0] = r.r, [1] = corr.corr
-__global__ void __launch_bounds__(kRedThreads) k_precond_diag(double* __restrict__ r, const double* __restrict__ hd,
-                                                              double lambda, size_t N, double* __restrict__ partial) {
-    double rr = 0.0, cc = 0.0;
-    for (size_t I = blockIdx.x * (size_t)blockDim.x + threadIdx.x; I < N; I += (size_t)gridDim.x * blockDim.x) {
-        double v = r[I];
-        rr = fma(v, v, rr);
-        double den = lambda - hd[I];
-        double c = (fabs(den) > 1.0e-6) ? v / den : 0.0;
-        r[I] = c;
-        cc = fma(c, c, cc);
+template <int NV, int NO>
+__global__ void __launch_bounds__(kRedThreads) k_combo(ComboArgs a, size_t N, double* __restrict__ partial) {
+    double acc[2 * NO];
+#pragma unroll
+    for (int k = 0; k < 2 * NO; k++) acc[k] = 0.0;
+    const size_t G = (size_t)gridDim.x * blockDim.x;
+    size_t I = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    for (; I + 3 * G < N; I += 4 * G) {
+        double o[4][NO];
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+#pragma unroll
+            for (int k = 0; k < NO; k++) o[u][k] = (k < a.nout && a.beta != 0.0) ? a.beta * a.out[k][I + u * G] : 0.0;
+#pragma unroll
+        for (int j = 0; j < NV; j++) {
+            if (j < a.nv) {
+                double v[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) v[u] = a.v[j][I + u * G];
+#pragma unroll
+                for (int u = 0; u < 4; u++)
+#pragma unroll
+                    for (int k = 0; k < NO; k++) o[u][k] = fma(a.coef[k][j], v[u], o[u][k]);
+            }
+        }
+        double hd[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) hd[u] = a.precond ? a.hd[I + u * G] : 0.0;
+#pragma unroll
+        for (int u = 0; u < 4; u++) combo_elem<NV, NO>(a, I + u * G, hd[u], acc, o[u]);
     }
-    __shared__ double red[2][kRedThreads / 32];
-    for (int o = 16; o > 0; o >>= 1) {
-        rr += __shfl_xor_sync(0xffffffffu, rr, o);
-        cc += __shfl_xor_sync(0xffffffffu, cc, o);
+    for (; I < N; I += G) {
+        double o[NO];
+#pragma unroll
+        for (int k = 0; k < NO; k++) o[k] = (k < a.nout && a.beta != 0.0) ? a.beta * a.out[k][I] : 0.0;
+#pragma unroll
+        for (int j = 0; j < NV; j++) {
+            if (j < a.nv) {
+                double v = a.v[j][I];
+#pragma unroll
+                for (int k = 0; k < NO; k++) o[k] = fma(a.coef[k][j], v, o[k]);
+            }
+        }
+        combo_elem<NV, NO>(a, I, a.precond ? a.hd[I] : 0.0, acc, o);
     }
-    if ((threadIdx.x & 31) == 0) {
-        red[0][threadIdx.x >> 5] = rr;
-        red[1][threadIdx.x >> 5] = cc;
+    __shared__ double red[kRedThreads / 32][2 * NO];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < 2 * NO; j++) {
+        if (j < 2 * a.nout) {
+            double v = acc[j];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) red[warp][j] = v;
+        }
     }
     __syncthreads();
-    if (threadIdx.x < 2) {
-        double s = 0.0;
-        for (int w = 0; w < kRedThreads / 32; w++) s += red[threadIdx.x][w];
-        partial[(size_t)blockIdx.x * (kMaxV + 1) + threadIdx.x] = s;
+    for (int j = threadIdx.x; j < 2 * a.nout; j += blockDim.x) {
+        double t = 0.0;
+        for (int w = 0; w < kRedThreads / 32; w++) t += red[w][j];
+        partial[(size_t)blockIdx.x * kSlots + j] = t;
+    }
+}
+
+// out[j] = sum_b partial[b][j] for j < nslots (one block per slot, deterministic order)
+__global__ void k_final_reduce(const double* __restrict__ partial, int nblocks, double* __restrict__ out) {
+    const int j = blockIdx.x;
+    double s = 0.0;
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s += partial[(size_t)b * kSlots + j];
+    __shared__ double red[32];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)blockDim.x / 32; w++) t += red[w];
+        out[j] = t;
     }
 }
 
 __global__ void k_scale(double* __restrict__ v, double a, size_t N) {
     for (size_t I = blockIdx.x * (size_t)blockDim.x + threadIdx.x; I < N; I += (size_t)gridDim.x * blockDim.x) v[I] *= a;
+}
+
+// v[I] += scale * u(I) with u uniform in [-1, 1) from a counter-based hash of (seed, I)
+__global__ void k_add_random(double* __restrict__ v, size_t N, unsigned long long seed, double scale) {
+    for (size_t I = blockIdx.x * (size_t)blockDim.x + threadIdx.x; I < N; I += (size_t)gridDim.x * blockDim.x) {
+        unsigned long long z = seed + 0x9E3779B97F4A7C15ull * (I + 1);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        v[I] += scale * ((double)(z >> 11) * (2.0 / 9007199254740992.0) - 1.0);
+    }
 }
 
 __global__ void k_fill_sparse(double* __restrict__ v, const int64_t* __restrict__ idx, const double* __restrict__ val, int cnt) {
@@ -232,7 +319,7 @@ __global__ void __launch_bounds__(kRedThreads) k_spin2(const double* __restrict_
     if (threadIdx.x == 0) {
         double s = 0.0;
         for (int w = 0; w < kRedThreads / 32; w++) s += red[w];
-        partial[(size_t)blockIdx.x * (kMaxV + 1)] = s;
+        partial[(size_t)blockIdx.x * kSlots] = s;
     }
 }
 
@@ -248,67 +335,99 @@ struct Ops {
     explicit Ops(Context& cc) : c(cc) {
         N = (size_t)c.ndet;
         nblk = std::max(1, std::min(4 * c.num_sms, (int)((N + kRedThreads - 1) / kRedThreads)));
-        partial.alloc((size_t)nblk * (kMaxV + 1));
-        out.alloc(kMaxV + 1);
-        hout.resize(kMaxV + 1);
+        partial.alloc((size_t)nblk * kSlots);
+        out.alloc(kSlots);
+        hout.resize(kSlots);
     }
-    // d[j] = V_j . x for j < nv (any nv), optionally x.x
-    void dots(const std::vector<const double*>& V, const double* x, std::vector<double>& d, double* xx = nullptr) {
+    void fetch(int nslots) {
+        k_final_reduce<<<nslots, 256, 0, c.stream>>>(partial.p, nblk, out.p);
+        FCIB_CUDA(cudaGetLastError());
+        FCIB_CUDA(cudaMemcpyAsync(hout.data(), out.p, sizeof(double) * nslots, cudaMemcpyDeviceToHost, c.stream));
+        FCIB_CUDA(cudaStreamSynchronize(c.stream));
+    }
+    // d[j] = V[j] . (sel[j] ? x1 : x0); optionally *self = x0 . x0
+    void dots(const std::vector<const double*>& V, const std::vector<int>& sel, const double* x0, const double* x1,
+              std::vector<double>& d, double* self = nullptr) {
         d.assign(V.size(), 0.0);
         size_t done = 0;
-        bool self = xx != nullptr;
-        do {
-            VecSet vs;
-            int nv = (int)std::min<size_t>(kMaxV, V.size() - done);
-            for (int j = 0; j < nv; j++) vs.p[j] = V[done + j];
-            int want_self = (self && done == 0) ? 1 : 0;
-            k_multidot<<<nblk, kRedThreads, 0, c.stream>>>(vs, nv, x, N, want_self, partial.p);
-            FCIB_CUDA(cudaGetLastError());
-            k_reduce_partials<<<1, 64, 0, c.stream>>>(partial.p, nblk, nv, want_self, out.p);
-            FCIB_CUDA(cudaGetLastError());
-            FCIB_CUDA(cudaMemcpyAsync(hout.data(), out.p, sizeof(double) * (kMaxV + 1), cudaMemcpyDeviceToHost, c.stream));
-            FCIB_CUDA(cudaStreamSynchronize(c.stream));
-            for (int j = 0; j < nv; j++) d[done + j] = hout[j];
-            if (want_self) *xx = hout[kMaxV];
-            done += nv;
-        } while (done < V.size());
-    }
-    // out = beta*out + sum coef_j V_j ; returns out.out when want_norm
-    double lincomb(const std::vector<const double*>& V, const std::vector<double>& coef, double* o, double beta,
-                   bool want_norm) {
-        size_t done = 0;
-        double nrm = 0.0;
-        if (V.empty()) {
-            if (beta != 1.0) {
-                k_scale<<<nblk, kRedThreads, 0, c.stream>>>(o, beta, N);
-                FCIB_CUDA(cudaGetLastError());
-            }
-            if (want_norm) {
-                std::vector<double> dd;
-                dots({}, o, dd, &nrm);
-            }
-            return nrm;
-        }
-        while (done < V.size()) {
-            VecSet vs;
-            int nv = (int)std::min<size_t>(kMaxV, V.size() - done);
+        bool first = true;
+        while (first || done < V.size()) {
+            DotArgs a;
+            int nv = (int)std::min<size_t>(kMaxIn, V.size() - done);
+            a.sel = 0;
             for (int j = 0; j < nv; j++) {
-                vs.p[j] = V[done + j];
-                vs.coef[j] = coef[done + j];
+                a.v[j] = V[done + j];
+                if (!sel.empty() && sel[done + j]) a.sel |= 1ull << j;
             }
-            bool last = done + nv == V.size();
-            k_lincomb<<<nblk, kRedThreads, 0, c.stream>>>(vs, nv, o, done == 0 ? beta : 1.0, N,
-                                                          (last && want_norm) ? partial.p : nullptr);
+            a.nv = nv;
+            a.self = (self && first) ? 1 : 0;
+            a.x0 = x0;
+            a.x1 = x1;
+            if (nv <= 8) k_dots<8><<<nblk, kRedThreads, 0, c.stream>>>(a, N, partial.p);
+            else if (nv <= 16) k_dots<16><<<nblk, kRedThreads, 0, c.stream>>>(a, N, partial.p);
+            else if (nv <= 32) k_dots<32><<<nblk, kRedThreads, 0, c.stream>>>(a, N, partial.p);
+            else k_dots<64><<<nblk, kRedThreads, 0, c.stream>>>(a, N, partial.p);
             FCIB_CUDA(cudaGetLastError());
+            fetch(kMaxIn + 1);
+            for (int j = 0; j < nv; j++) d[done + j] = hout[j];
+            if (a.self) *self = hout[kMaxIn];
             done += nv;
+            first = false;
         }
-        if (want_norm) {
-            k_reduce_partials<<<1, 64, 0, c.stream>>>(partial.p, nblk, 1, 0, out.p);
-            FCIB_CUDA(cudaMemcpyAsync(hout.data(), out.p, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
-            FCIB_CUDA(cudaStreamSynchronize(c.stream));
-            nrm = hout[0];
+    }
+    double norm2(const double* x) {
+        std::vector<double> d;
+        double s = 0.0;
+        dots({}, {}, x, nullptr, d, &s);
+        return s;
+    }
+    // outs[k] = beta*outs[k] + sum_j coef[k][j] V[j];  optional diagonal preconditioning with
+    // lambda[k].  Returns (out.out, corr.corr) per output of the last chunk.
+    std::vector<std::pair<double, double>> combo(const std::vector<const double*>& V,
+                                                 const std::vector<std::vector<double>>& coef,
+                                                 const std::vector<double*>& outs, double beta,
+                                                 const double* lambda = nullptr) {
+        const int nout_all = (int)outs.size();
+        std::vector<std::pair<double, double>> res(nout_all, {0.0, 0.0});
+        for (int k0 = 0; k0 < nout_all; k0 += kMaxOut) {
+            int nout = std::min(kMaxOut, nout_all - k0);
+            size_t done = 0;
+            do {
+                ComboArgs a;
+                int nv = (int)std::min<size_t>(kMaxIn, V.size() - done);
+                bool last = done + nv >= V.size();
+                for (int j = 0; j < nv; j++) a.v[j] = V[done + j];
+                for (int k = 0; k < nout; k++) {
+                    for (int j = 0; j < nv; j++) a.coef[k][j] = coef[k0 + k][done + j];
+                    a.out[k] = outs[k0 + k];
+                    a.lambda[k] = lambda ? lambda[k0 + k] : 0.0;
+                }
+                a.hd = c.hdiag.p;
+                a.nv = nv;
+                a.nout = nout;
+                a.precond = (lambda && last) ? 1 : 0;
+                a.beta = (done == 0) ? beta : 1.0;
+#define FCIB_COMBO(NVv, NOv) k_combo<NVv, NOv><<<nblk, kRedThreads, 0, c.stream>>>(a, N, partial.p)
+                if (nout == 1) {
+                    if (nv <= 8) FCIB_COMBO(8, 1); else if (nv <= 16) FCIB_COMBO(16, 1);
+                    else if (nv <= 32) FCIB_COMBO(32, 1); else FCIB_COMBO(64, 1);
+                } else if (nout == 2) {
+                    if (nv <= 8) FCIB_COMBO(8, 2); else if (nv <= 16) FCIB_COMBO(16, 2);
+                    else if (nv <= 32) FCIB_COMBO(32, 2); else FCIB_COMBO(64, 2);
+                } else {
+                    if (nv <= 8) FCIB_COMBO(8, 4); else if (nv <= 16) FCIB_COMBO(16, 4);
+                    else if (nv <= 32) FCIB_COMBO(32, 4); else FCIB_COMBO(64, 4);
+                }
+#undef FCIB_COMBO
+                FCIB_CUDA(cudaGetLastError());
+                done += nv;
+                if (last) {
+                    fetch(2 * nout);
+                    for (int k = 0; k < nout; k++) res[k0 + k] = {hout[2 * k], hout[2 * k + 1]};
+                }
+            } while (done < V.size());
         }
-        return nrm;
+        return res;
     }
     void scale(double* v, double a) {
         k_scale<<<nblk, kRedThreads, 0, c.stream>>>(v, a, N);
@@ -316,15 +435,6 @@ struct Ops {
     }
     void copy(double* dst, const double* src) {
         FCIB_CUDA(cudaMemcpyAsync(dst, src, N * sizeof(double), cudaMemcpyDeviceToDevice, c.stream));
-    }
-    // returns (r.r, corr.corr)
-    std::pair<double, double> precond(double* r, double lambda) {
-        k_precond_diag<<<nblk, kRedThreads, 0, c.stream>>>(r, c.hdiag.p, lambda, N, partial.p);
-        FCIB_CUDA(cudaGetLastError());
-        k_reduce_partials<<<1, 64, 0, c.stream>>>(partial.p, nblk, 2, 0, out.p);
-        FCIB_CUDA(cudaMemcpyAsync(hout.data(), out.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
-        FCIB_CUDA(cudaStreamSynchronize(c.stream));
-        return {hout[0], hout[1]};
     }
 };
 
@@ -334,34 +444,44 @@ struct SparseDev {
     int cnt = 0;
 };
 
-// add_row_and_orthonormalize (davidson_liu_solver.cc:634-687): copy v into A[rowsA] and
-// Gram-Schmidt it against A[0..rowsA); false if discarded.
-static bool add_row_orth(Ops& ops, std::vector<double*>& A, int rowsA, const double* v) {
+// add_row_and_orthonormalize (davidson_liu_solver.cc:634-687): A[rowsA] <- s*src Gram-Schmidt
+// orthonormalised against A[0..rowsA); false if discarded (norm < 1e-7 after projection).
+// Classical Gram-Schmidt with a re-orthogonalisation check, the same thresholds as the
+// reference's modified Gram-Schmidt loop.
+static bool add_row_orth(Ops& ops, std::vector<double*>& A, int rowsA, const double* src, double s = 1.0) {
     double* w = A[rowsA];
-    if (w != v) ops.copy(w, v);
     std::vector<const double*> B(A.begin(), A.begin() + rowsA);
     std::vector<double> d;
     double vv = 0.0;
-    ops.dots(B, w, d, &vv);
+    ops.dots(B, {}, src, nullptr, d, &vv);
+    // first projection reads src and writes w
+    std::vector<const double*> V(B);
+    V.push_back(src);
+    std::vector<std::vector<double>> coef(1, std::vector<double>(rowsA + 1));
+    for (int i = 0; i < rowsA; i++) coef[0][i] = -s * d[i];
+    coef[0][rowsA] = s;
+    auto nn = ops.combo(V, coef, {w}, 0.0);
     for (int cycle = 0; cycle < 10; cycle++) {
-        std::vector<double> coef(rowsA);
-        for (int i = 0; i < rowsA; i++) coef[i] = -d[i];
-        double nn = ops.lincomb(B, coef, w, 1.0, true);
-        double nv = std::sqrt(nn);
-        if (nv < 1.0e-7) return false;
-        ops.scale(w, 1.0 / nv);
-        ops.dots(B, w, d, &vv);
+        double nv = std::sqrt(nn[0].first);
+        if (!(nv >= 1.0e-7)) return false;  // also rejects NaN
+        ops.dots(B, {}, w, nullptr, d, &vv);
         double mo = 0.0;
-        for (int i = 0; i < rowsA; i++) mo = std::max(mo, std::fabs(d[i]));
-        if (mo < 1.0e-12 && std::fabs(vv - 1.0) < 1.0e-12) return true;
+        for (int i = 0; i < rowsA; i++) mo = std::max(mo, std::fabs(d[i] / nv));
+        ops.scale(w, 1.0 / nv);
+        if (mo < 1.0e-12 && std::fabs(vv / (nv * nv) - 1.0) < 1.0e-12) return true;
+        // re-orthogonalise the normalised vector
+        std::vector<std::vector<double>> c2(1, std::vector<double>(rowsA));
+        for (int i = 0; i < rowsA; i++) c2[0][i] = -d[i] / nv;
+        nn = ops.combo(B, c2, {w}, 1.0);
     }
     return false;
 }
 
-static int add_rows_orth(Ops& ops, std::vector<double*>& A, int rowsA, const std::vector<double*>& Bv, int rowsB) {
+static int add_rows_orth(Ops& ops, std::vector<double*>& A, int rowsA, const std::vector<double*>& Bv, int rowsB,
+                         const std::vector<double>* scales = nullptr) {
     int added = 0;
     for (int j = 0; j < rowsB; j++)
-        if (add_row_orth(ops, A, rowsA + added, Bv[j])) added++;
+        if (add_row_orth(ops, A, rowsA + added, Bv[j], scales ? (*scales)[j] : 1.0)) added++;
     return added;
 }
 
@@ -377,10 +497,8 @@ double spin2_device(Context& c, const double* C) {
     Ops ops(c);
     k_spin2<<<ops.nblk, kRedThreads, 0, c.stream>>>(C, c.A.str.p, c.B.str.p, (int)c.nas, (int)c.nbs, c.n, ops.partial.p);
     FCIB_CUDA(cudaGetLastError());
-    k_reduce_partials<<<1, 64, 0, c.stream>>>(ops.partial.p, ops.nblk, 1, 0, ops.out.p);
-    double s = 0.0;
-    FCIB_CUDA(cudaMemcpyAsync(&s, ops.out.p, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
-    FCIB_CUDA(cudaStreamSynchronize(c.stream));
+    ops.fetch(1);
+    double s = ops.hout[0];
     double na = c.na, nb = c.nb;
     return -s + 0.25 * (na - nb) * (na - nb) + 0.5 * (na + nb);
 }
@@ -442,6 +560,9 @@ static double now_ms() {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
+// Precision of the sigma build for a new basis vector in each solver phase.
+enum class Phase { LowPrecision, Refine, FP64Only };
+
 void dl_solve(Context& c) {
     const int64_t N = c.ndet;
     int64_t Neff = N;
@@ -458,9 +579,11 @@ void dl_solve(Context& c) {
     FCIB_CHECK(o.subspace_per_root >= o.collapse_per_root + 1, FCIB_ERR_ARG,
                "DavidsonLiuSolver: subspace_per_root must be >= collapse_per_root + 1");
     const int nroot = c.nroot;
+    FCIB_CHECK(nroot <= kMaxOut * 8, FCIB_ERR_UNSUPPORTED, "too many roots");
     const int collapse = (int)std::min<int64_t>((int64_t)o.collapse_per_root * nroot, Neff);
     const int m = (int)std::min<int64_t>((int64_t)o.subspace_per_root * nroot, Neff);
     FCIB_CHECK(nroot <= m, FCIB_ERR_ARG, "more roots than determinants");
+    FCIB_CHECK(2 * m <= kMaxIn * 4, FCIB_ERR_UNSUPPORTED, "Davidson subspace too large");
     c.subspace = m;
     c.b.alloc((size_t)m * N);
     c.sig.alloc((size_t)m * N);
@@ -474,13 +597,21 @@ void dl_solve(Context& c) {
     }
     for (int k = 0; k < nroot; k++) r[k] = c.r.p + (size_t)k * N;
     Ops ops(c);
+    cudaEvent_t ev_start, e0, e1;
+    FCIB_CUDA(cudaEventCreate(&ev_start));
+    FCIB_CUDA(cudaEventCreate(&e0));
+    FCIB_CUDA(cudaEventCreate(&e1));
+    FCIB_CUDA(cudaEventRecord(ev_start, c.stream));
     double t_start = now_ms();
     c.t_sigma_ms = 0.0;
     c.n_sigma = 0;
+    c.n_sigma_fp64 = 0;
+    c.trace.clear();
 
     // ---- initial guess ----
     int num_guess_states = (int)std::min<int64_t>((int64_t)o.guess_per_root * nroot, Neff);
     int ng = (int)std::min<int64_t>((int64_t)num_guess_states * o.dets_per_guess, Neff);
+    double t_guess0 = now_ms();
     auto lowest = lowest_diagonal(c, ng);
     std::vector<uint32_t> sa(c.nas), sbv(c.nbs);
     FCIB_CUDA(cudaMemcpy(sa.data(), c.A.str.p, 4 * c.nas, cudaMemcpyDeviceToHost));
@@ -500,6 +631,8 @@ void dl_solve(Context& c) {
         throw Error{FCIB_ERR_ARG, e.what()};
     }
     int nguess = (int)gr.guesses.size();
+    c.t_guess_ms = now_ms() - t_guess0;
+    c.guess_dets = gr.guesses.empty() ? 0 : (int)gr.guesses[0].size();
     FCIB_CHECK(nguess >= nroot && nguess <= m, FCIB_ERR_ARG,
                "DavidsonLiuSolver: number of guess vectors must be between nroot and the subspace size");
     std::vector<SparseDev> bad(gr.bad_roots.size());
@@ -511,7 +644,6 @@ void dl_solve(Context& c) {
         bad[i].val.upload(vv, c.stream);
         bad[i].cnt = (int)ix.size();
     }
-    // guesses -> tmp rows
     FCIB_CUDA(cudaMemsetAsync(c.tmp.p, 0, sizeof(double) * (size_t)m * N, c.stream));
     for (int g = 0; g < nguess; g++) {
         SparseDev sd;
@@ -524,51 +656,86 @@ void dl_solve(Context& c) {
         FCIB_CUDA(cudaGetLastError());
         FCIB_CUDA(cudaStreamSynchronize(c.stream));
     }
+    if (gr.perturb) {
+        // Without spin selection the lowest state may lie in a spin sector the guess space does
+        // not contain; exact FP64 iterations never leave the sectors of the guess, so every
+        // guess gets a seeded pseudo-random component of norm ~1e-3 over all determinants.
+        for (int k = 0; k < nguess; k++) {
+            k_add_random<<<ops.nblk, kRedThreads, 0, c.stream>>>(tmp[k], N, 0x9E3779B97F4A7C15ull * (k + 1),
+                                                                 1.0e-3 * std::sqrt(3.0 / (double)N));
+            FCIB_CUDA(cudaGetLastError());
+            apply_mask(c, tmp[k]);
+        }
+    }
     project_out(c, bad, tmp, std::min(nroot, nguess));
     int should = std::max(nroot, nguess);
     int basis = add_rows_orth(ops, b, 0, std::vector<double*>(tmp.begin(), tmp.begin() + should), should);
     FCIB_CHECK(basis == should, FCIB_ERR_NUMERIC, "DavidsonLiuSolver: guess vectors are zero or linearly dependent");
+
+    const bool mixed = (o.precision != FCIB_PREC_FP64);
+    const int lowp = o.precision;
+    Phase phase = mixed ? Phase::LowPrecision : Phase::FP64Only;
+    std::vector<int> sig_fp64(m, 0);  // sigma of basis vector j computed in FP64
+    int restarts = 0;
+    double best_r = 1e300;
+    int stall = 0;
+
     int nsig = 0;
     std::vector<double> G((size_t)m * m, 0.0), alpha((size_t)m * m, 0.0), lambda(m, 0.0), lambda_old(m, 0.0);
-    std::vector<double> rnorm(nroot, 0.0);
-    int gvalid = 0;  // G[i][j] valid for i, j < gvalid
+    std::vector<double> rnorm(nroot, 0.0), cnorm(nroot, 0.0);
+    int gvalid = 0;
     bool converged = false;
     int iter = 0;
     std::mt19937_64 rng(12345);
     if (o.print)
-        printf("\n  Davidson-Liu (B200): %lld determinants, %d roots, subspace %d, collapse %d\n",
-               (long long)Neff, nroot, m, collapse);
+        printf("\n  Davidson-Liu (B200): %lld determinants, %d roots, subspace %d, collapse %d, precision %d\n",
+               (long long)Neff, nroot, m, collapse, o.precision);
+
+    // Restart the basis from the current Ritz vectors with FP64 sigma (mixed modes).
+    auto restart_fp64 = [&]() {
+        std::vector<const double*> Bp(b.begin(), b.begin() + basis);
+        std::vector<std::vector<double>> coef(nroot, std::vector<double>(basis));
+        for (int k = 0; k < nroot; k++)
+            for (int j = 0; j < basis; j++) coef[k][j] = alpha[j * m + k];
+        ops.combo(Bp, coef, std::vector<double*>(tmp.begin(), tmp.begin() + nroot), 0.0);
+        int got = add_rows_orth(ops, b, 0, std::vector<double*>(tmp.begin(), tmp.begin() + nroot), nroot);
+        FCIB_CHECK(got == nroot, FCIB_ERR_NUMERIC, "DavidsonLiuSolver: restart generated fewer vectors than expected");
+        basis = nroot;
+        nsig = 0;
+        gvalid = 0;
+        restarts++;
+    };
+
     for (iter = 0; iter < o.maxiter; iter++) {
         // 1. sigma of the new basis vectors
         for (int j = nsig; j < basis; j++) {
-            cudaEvent_t e0, e1;
-            FCIB_CUDA(cudaEventCreate(&e0));
-            FCIB_CUDA(cudaEventCreate(&e1));
+            bool fp64 = (phase == Phase::FP64Only) || (phase == Phase::Refine && j < nroot && nsig == 0);
             FCIB_CUDA(cudaEventRecord(e0, c.stream));
-            sigma_dispatch(c, b[j], sg[j], FCIB_PREC_FP64);
+            sigma_dispatch(c, b[j], sg[j], fp64 ? FCIB_PREC_FP64 : lowp);
             FCIB_CUDA(cudaEventRecord(e1, c.stream));
             FCIB_CUDA(cudaEventSynchronize(e1));
             float ms = 0.f;
             cudaEventElapsedTime(&ms, e0, e1);
             c.t_sigma_ms += ms;
             c.n_sigma++;
-            cudaEventDestroy(e0);
-            cudaEventDestroy(e1);
+            c.n_sigma_fp64 += fp64 ? 1 : 0;
+            sig_fp64[j] = fp64 ? 1 : 0;
         }
+        bool all_fp64 = true;
+        for (int j = 0; j < basis; j++) all_fp64 = all_fp64 && sig_fp64[j];
         nsig = basis;
-        // 2. subspace matrix: new rows and columns of G = b sigma^T
-        {
+        // 2. new rows/columns of G = b sigma^T in one pass per new vector
+        for (int j = gvalid; j < basis; j++) {
+            std::vector<const double*> V;
+            std::vector<int> sel;
+            for (int i = 0; i < basis; i++) { V.push_back(b[i]); sel.push_back(0); }
+            for (int i = 0; i < gvalid; i++) { V.push_back(sg[i]); sel.push_back(1); }
             std::vector<double> d;
-            std::vector<const double*> Bp(b.begin(), b.begin() + basis), Sp(sg.begin(), sg.begin() + basis);
-            for (int j = gvalid; j < basis; j++) {
-                ops.dots(Bp, sg[j], d);
-                for (int i = 0; i < basis; i++) G[i * m + j] = d[i];
-                std::vector<const double*> So(sg.begin(), sg.begin() + gvalid);
-                ops.dots(So, b[j], d);
-                for (int i = 0; i < gvalid; i++) G[j * m + i] = d[i];
-            }
-            gvalid = basis;
+            ops.dots(V, sel, sg[j], b[j], d);
+            for (int i = 0; i < basis; i++) G[i * m + j] = d[i];
+            for (int i = 0; i < gvalid; i++) G[j * m + i] = d[basis + i];
         }
+        gvalid = basis;
         std::vector<double> Gb((size_t)basis * basis), ab((size_t)basis * basis), lb(basis);
         for (int i = 0; i < basis; i++)
             for (int j = 0; j < basis; j++) Gb[i * basis + j] = 0.5 * (G[i * m + j] + G[j * m + i]);
@@ -577,34 +744,29 @@ void dl_solve(Context& c) {
         for (int i = 0; i < basis; i++)
             for (int j = 0; j < basis; j++) alpha[i * m + j] = ab[i * basis + j];
         for (int i = 0; i < m; i++) lambda[i] = i < basis ? lb[i] : 0.0;
-        // 3. residuals, norms and corrections
-        std::vector<double> cnorm(nroot);
-        for (int k = 0; k < nroot; k++) {
+        for (int i = 0; i < nroot; i++)
+            FCIB_CHECK(std::isfinite(lambda[i]), FCIB_ERR_NUMERIC, "non-finite eigenvalue in the Davidson subspace");
+        // 3. residuals r_k = sum_j alpha_jk (sigma_j - lambda_k b_j), norms and corrections
+        {
             std::vector<const double*> V;
-            std::vector<double> coef;
-            for (int j = 0; j < basis; j++) {
-                V.push_back(sg[j]);
-                coef.push_back(alpha[j * m + k]);
-                V.push_back(b[j]);
-                coef.push_back(-lambda[k] * alpha[j * m + k]);
+            for (int j = 0; j < basis; j++) V.push_back(sg[j]);
+            for (int j = 0; j < basis; j++) V.push_back(b[j]);
+            std::vector<std::vector<double>> coef(nroot, std::vector<double>(2 * basis));
+            for (int k = 0; k < nroot; k++)
+                for (int j = 0; j < basis; j++) {
+                    coef[k][j] = alpha[j * m + k];
+                    coef[k][basis + j] = -lambda[k] * alpha[j * m + k];
+                }
+            auto rc = ops.combo(V, coef, r, 0.0, lambda.data());
+            for (int k = 0; k < nroot; k++) {
+                rnorm[k] = std::sqrt(rc[k].first);
+                cnorm[k] = std::sqrt(rc[k].second);
             }
-            ops.lincomb(V, coef, r[k], 0.0, false);
-            auto rc = ops.precond(r[k], lambda[k]);
-            rnorm[k] = std::sqrt(rc.first);
-            cnorm[k] = std::sqrt(rc.second);
         }
-        // 4. project out undesired roots, normalize
+        // 4. project out undesired roots; normalisation is folded into Gram-Schmidt
         project_out(c, bad, r, nroot);
-        for (int k = 0; k < nroot; k++) {
-            double nn = cnorm[k];
-            if (!bad.empty()) {
-                std::vector<double> dd;
-                double xx = 0.0;
-                ops.dots({}, r[k], dd, &xx);
-                nn = std::sqrt(xx);
-            }
-            ops.scale(r[k], 1.0 / nn);
-        }
+        if (!bad.empty())
+            for (int k = 0; k < nroot; k++) cnorm[k] = std::sqrt(ops.norm2(r[k]));
         // 5./6. convergence
         int ne = 0, nr = 0;
         double maxde = 0.0, maxr = 0.0;
@@ -615,48 +777,70 @@ void dl_solve(Context& c) {
             ne += de < o.e_convergence;
             nr += rnorm[k] < o.r_convergence;
         }
+        c.trace.push_back({(double)iter, now_ms() - t_start, lambda[0], maxr, all_fp64 ? 1.0 : 0.0});
         if (o.print) {
             double avg = 0.0;
             for (int k = 0; k < nroot; k++) avg += lambda[k] / nroot;
-            printf("  %4d  %20.12f  %12.3e  %12.3e  %3d\n", iter, avg, maxde, maxr, basis);
+            printf("  %4d  %20.12f  %12.3e  %12.3e  %3d %s\n", iter, avg, maxde, maxr, basis,
+                   all_fp64 ? "fp64" : "low");
         }
         bool e_ok = ne == nroot, r_ok = nr == nroot;
         if ((e_ok && r_ok) || basis == Neff) {
-            converged = true;
-            break;
+            if (!mixed || all_fp64) {
+                converged = true;
+                break;
+            }
+        }
+        // mixed modes: restart from the Ritz vectors with FP64 sigma when the low-precision
+        // residual reaches its floor or the low-precision iteration claims convergence
+        if (mixed && phase != Phase::FP64Only) {
+            if (maxr < 0.9 * best_r) { best_r = maxr; stall = 0; } else stall++;
+            bool want = (e_ok && r_ok) || basis == Neff ||
+                        (phase == Phase::LowPrecision && maxr < std::max(o.mixed_switch, o.r_convergence)) ||
+                        (stall >= 4 && maxr < 1.0e-2);
+            if (want) {
+                if (restarts >= 6) phase = Phase::FP64Only;
+                else phase = Phase::Refine;
+                restart_fp64();
+                best_r = 1e300;
+                stall = 0;
+                lambda_old = lambda;
+                continue;
+            }
         }
         // 7. collapse
         if (basis + nroot > m) {
             int cs = std::min(std::max(collapse, nroot), basis);
             std::vector<const double*> Bp(b.begin(), b.begin() + basis), Sp(sg.begin(), sg.begin() + basis);
-            for (int k = 0; k < cs; k++) {
-                std::vector<double> coef(basis);
-                for (int j = 0; j < basis; j++) coef[j] = alpha[j * m + k];
-                ops.lincomb(Bp, coef, tmp[k], 0.0, false);
-            }
+            std::vector<std::vector<double>> coef(cs, std::vector<double>(basis));
+            for (int k = 0; k < cs; k++)
+                for (int j = 0; j < basis; j++) coef[k][j] = alpha[j * m + k];
+            ops.combo(Bp, coef, std::vector<double*>(tmp.begin(), tmp.begin() + cs), 0.0);
             int a2 = add_rows_orth(ops, b, 0, std::vector<double*>(tmp.begin(), tmp.begin() + cs), cs);
             FCIB_CHECK(a2 == cs, FCIB_ERR_NUMERIC, "DavidsonLiuSolver: collapse generated fewer vectors than expected");
+            ops.combo(Sp, coef, std::vector<double*>(tmp.begin(), tmp.begin() + cs), 0.0);
+            bool f64 = true;
+            for (int j = 0; j < basis; j++) f64 = f64 && sig_fp64[j];
             for (int k = 0; k < cs; k++) {
-                std::vector<double> coef(basis);
-                for (int j = 0; j < basis; j++) coef[j] = alpha[j * m + k];
-                ops.lincomb(Sp, coef, tmp[k], 0.0, false);
+                std::swap(sg[k], tmp[k]);
+                sig_fp64[k] = f64 ? 1 : 0;
             }
-            for (int k = 0; k < cs; k++) std::swap(sg[k], tmp[k]);
             basis = cs;
             nsig = cs;
             gvalid = 0;
         }
-        // 8. add correction vectors
+        // 8. add the normalised correction vectors
         int num_to_add = std::min(nroot, m - basis);
-        int added = add_rows_orth(ops, b, basis, r, num_to_add);
+        std::vector<double> sc(nroot);
+        for (int k = 0; k < nroot; k++) sc[k] = 1.0 / cnorm[k];
+        int added = add_rows_orth(ops, b, basis, r, num_to_add, &sc);
         basis += added;
         int missing = num_to_add - added;
         if (missing > 0) {
-            std::vector<double> rv(N);
-            std::uniform_real_distribution<double> dist(-1.0, 1.0);
             for (int k = 0; k < missing; k++) {
-                for (auto& x : rv) x = dist(rng);
-                FCIB_CUDA(cudaMemcpy(tmp[m - 1], rv.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
+                FCIB_CUDA(cudaMemsetAsync(tmp[m - 1], 0, sizeof(double) * N, c.stream));
+                k_add_random<<<ops.nblk, kRedThreads, 0, c.stream>>>(tmp[m - 1], N, 0xD1B54A32D192ED03ull + rng(), 1.0);
+                FCIB_CUDA(cudaGetLastError());
                 apply_mask(c, tmp[m - 1]);
                 std::vector<double*> one{tmp[m - 1]};
                 project_out(c, bad, one, 1);
@@ -666,34 +850,36 @@ void dl_solve(Context& c) {
             }
         }
         if (added == 0) {
-            converged = r_ok;
+            converged = r_ok && (!mixed || all_fp64);
             break;
         }
         lambda_old = lambda;
     }
     c.iterations = std::min(iter + 1, o.maxiter);
-    // get_results: final eigenvectors
+    // get_results (davidson_liu_solver.cc:488-501): final eigenvectors in b[0..nroot)
     {
         std::vector<const double*> Bp(b.begin(), b.begin() + basis);
-        for (int k = 0; k < nroot; k++) {
-            std::vector<double> coef(basis);
-            for (int j = 0; j < basis; j++) coef[j] = alpha[j * m + k];
-            ops.lincomb(Bp, coef, tmp[k], 0.0, false);
-        }
+        std::vector<std::vector<double>> coef(nroot, std::vector<double>(basis));
+        for (int k = 0; k < nroot; k++)
+            for (int j = 0; j < basis; j++) coef[k][j] = alpha[j * m + k];
+        ops.combo(Bp, coef, std::vector<double*>(tmp.begin(), tmp.begin() + nroot), 0.0);
         int got = add_rows_orth(ops, b, 0, std::vector<double*>(tmp.begin(), tmp.begin() + nroot), nroot);
         FCIB_CHECK(got == nroot, FCIB_ERR_NUMERIC, "DavidsonLiuSolver: get_results generated fewer vectors than expected");
-        // keep the eigenvectors at the start of the b buffer
-        for (int k = 0; k < nroot; k++)
-            if (b[k] != c.b.p + (size_t)k * N)
-                ops.copy(c.b.p + (size_t)k * N, b[k]);
     }
     c.energies.assign(lambda.begin(), lambda.begin() + nroot);
+    FCIB_CUDA(cudaEventRecord(e1, c.stream));
+    FCIB_CUDA(cudaEventSynchronize(e1));
+    float tot = 0.f;
+    cudaEventElapsedTime(&tot, ev_start, e1);
+    c.t_total_ms = tot;
     c.solved = true;
+    c.converged = converged;
     c.spin2.resize(nroot);
     for (int k = 0; k < nroot; k++) c.spin2[k] = spin2_device(c, c.b.p + (size_t)k * N);
     FCIB_CUDA(cudaStreamSynchronize(c.stream));
-    c.t_total_ms = now_ms() - t_start;
-    c.converged = converged;
+    cudaEventDestroy(ev_start);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
 }
 
 }  // namespace fcib

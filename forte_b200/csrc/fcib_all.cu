@@ -2,5 +2,6 @@
 // integrals) and __device__ helpers are shared by all kernels without relocatable device code.
 #include "strings.cu"
 #include "sigma.cu"
+#include "sigma_tc.cu"
 #include "davidson.cu"
 #include "capi.cu"

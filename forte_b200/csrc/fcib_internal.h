@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <array>
 #include <string>
 #include <vector>
 
@@ -130,6 +131,9 @@ struct Context {
     DBuf<uint8_t> mask;   // determinant in target irrep (only when nirrep > 1)
     // work vectors
     DBuf<double> ct, st;  // transposed C and sigma for beta same-spin terms
+    DBuf<uint16_t> tgtR16; // beta replacement targets [string][pair] for the tensor-core kernel
+    DBuf<float> tf_hi, tf_lo; // tf32 split planes of the sigma input (mixed path)
+    float vmax = 0.0f;    // max |V| (fixed-point grid of the tensor-core scatter)
     DBuf<double> hdiag;
     // solver storage
     DBuf<double> b, sig, r, tmp;
@@ -145,12 +149,17 @@ struct Context {
     double t_sigma_ms = 0.0;
     int n_sigma = 0;
     double t_total_ms = 0.0;
+    int n_sigma_fp64 = 0;
+    double t_guess_ms = 0.0;
+    int guess_dets = 0;
     bool converged = false;
+    std::vector<std::array<double, 5>> trace;  // iteration, ms, lambda_0, max residual, fp64 basis
 };
 
 // kernels / launchers (sigma.cu)
 void prepare_integrals(Context& c);
 void sigma_fp64(Context& c, const double* C, double* S);
+void sigma_mixed(Context& c, const double* C, double* S, bool three);
 void apply_mask(Context& c, double* v);
 void export_list(int n, int k, int kind, int p, int q, int r, int s, std::vector<int8_t>& sign,
                  std::vector<uint32_t>& I, std::vector<uint32_t>& J, cudaStream_t st);

@@ -18,59 +18,126 @@
 
 namespace fcib {
 
+// Symmetric eigensolver: Householder reduction to tridiagonal form followed by the implicit
+// QL algorithm with Wilkinson-type shifts (the classical tred2/tql2 scheme, O(n^3)).  Eigenvalues
+// ascending, eigenvectors in the columns of V; each eigenvector's largest component positive.
 void sym_eigen(int n, const double* Ain, double* evals, double* V) {
-    std::vector<double> A(Ain, Ain + (size_t)n * n);
-    for (int i = 0; i < n * n; i++) V[i] = 0.0;
-    for (int i = 0; i < n; i++) V[i * n + i] = 1.0;
-    for (int sweep = 0; sweep < 100; sweep++) {
-        double off = 0.0, tot = 0.0;
-        for (int i = 0; i < n; i++)
-            for (int j = 0; j < n; j++) {
-                double a = A[i * n + j] * A[i * n + j];
-                tot += a;
-                if (i != j) off += a;
+    if (n <= 0) return;
+    std::vector<double> a(Ain, Ain + (size_t)n * n);  // row-major, becomes the transform
+    std::vector<double> d(n), e(n);
+    auto A = [&](int i, int j) -> double& { return a[(size_t)i * n + j]; };
+    // --- tridiagonalisation (Householder), accumulating the orthogonal transform in a ---
+    for (int i = n - 1; i > 0; i--) {
+        int l = i - 1;
+        double h = 0.0, scale = 0.0;
+        if (l > 0) {
+            for (int k = 0; k <= l; k++) scale += std::fabs(A(i, k));
+            if (scale == 0.0) {
+                e[i] = A(i, l);
+            } else {
+                for (int k = 0; k <= l; k++) {
+                    A(i, k) /= scale;
+                    h += A(i, k) * A(i, k);
+                }
+                double f = A(i, l);
+                double g = (f >= 0.0) ? -std::sqrt(h) : std::sqrt(h);
+                e[i] = scale * g;
+                h -= f * g;
+                A(i, l) = f - g;
+                f = 0.0;
+                for (int j = 0; j <= l; j++) {
+                    A(j, i) = A(i, j) / h;
+                    g = 0.0;
+                    for (int k = 0; k <= j; k++) g += A(j, k) * A(i, k);
+                    for (int k = j + 1; k <= l; k++) g += A(k, j) * A(i, k);
+                    e[j] = g / h;
+                    f += e[j] * A(i, j);
+                }
+                double hh = f / (h + h);
+                for (int j = 0; j <= l; j++) {
+                    f = A(i, j);
+                    e[j] = g = e[j] - hh * f;
+                    for (int k = 0; k <= j; k++) A(j, k) -= (f * e[k] + g * A(i, k));
+                }
             }
-        if (off <= 1e-30 * (tot > 0 ? tot : 1.0) || off < 1e-300) break;
-        for (int p = 0; p < n - 1; p++)
-            for (int q = p + 1; q < n; q++) {
-                double apq = A[p * n + q];
-                if (std::fabs(apq) < 1e-300) continue;
-                double theta = (A[q * n + q] - A[p * n + p]) / (2.0 * apq);
-                double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
-                double cs = 1.0 / std::sqrt(t * t + 1.0), sn = t * cs;
-                for (int k = 0; k < n; k++) {
-                    double akp = A[k * n + p], akq = A[k * n + q];
-                    A[k * n + p] = cs * akp - sn * akq;
-                    A[k * n + q] = sn * akp + cs * akq;
-                }
-                for (int k = 0; k < n; k++) {
-                    double apk = A[p * n + k], aqk = A[q * n + k];
-                    A[p * n + k] = cs * apk - sn * aqk;
-                    A[q * n + k] = sn * apk + cs * aqk;
-                }
-                for (int k = 0; k < n; k++) {
-                    double vkp = V[k * n + p], vkq = V[k * n + q];
-                    V[k * n + p] = cs * vkp - sn * vkq;
-                    V[k * n + q] = sn * vkp + cs * vkq;
-                }
-            }
-    }
-    for (int i = 0; i < n; i++) evals[i] = A[i * n + i];
-    for (int i = 0; i < n; i++) {
-        int m = i;
-        for (int j = i + 1; j < n; j++)
-            if (evals[j] < evals[m]) m = j;
-        if (m != i) {
-            std::swap(evals[i], evals[m]);
-            for (int k = 0; k < n; k++) std::swap(V[k * n + i], V[k * n + m]);
+        } else {
+            e[i] = A(i, l);
         }
+        d[i] = h;
+    }
+    d[0] = 0.0;
+    e[0] = 0.0;
+    for (int i = 0; i < n; i++) {
+        int l = i - 1;
+        if (d[i] != 0.0) {
+            for (int j = 0; j <= l; j++) {
+                double g = 0.0;
+                for (int k = 0; k <= l; k++) g += A(i, k) * A(k, j);
+                for (int k = 0; k <= l; k++) A(k, j) -= g * A(k, i);
+            }
+        }
+        d[i] = A(i, i);
+        A(i, i) = 1.0;
+        for (int j = 0; j <= l; j++) A(j, i) = A(i, j) = 0.0;
+    }
+    // --- implicit QL on the tridiagonal matrix (d, e), rotating the columns of a ---
+    for (int i = 1; i < n; i++) e[i - 1] = e[i];
+    e[n - 1] = 0.0;
+    for (int l = 0; l < n; l++) {
+        int iter = 0, m;
+        do {
+            for (m = l; m < n - 1; m++) {
+                double dd = std::fabs(d[m]) + std::fabs(d[m + 1]);
+                if (std::fabs(e[m]) <= 1e-15 * dd) break;
+            }
+            if (m != l) {
+                if (iter++ == 200) break;
+                double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+                double r = std::hypot(g, 1.0);
+                g = d[m] - d[l] + e[l] / (g + (g >= 0.0 ? std::fabs(r) : -std::fabs(r)));
+                double s = 1.0, c = 1.0, p = 0.0;
+                int i;
+                for (i = m - 1; i >= l; i--) {
+                    double f = s * e[i], b = c * e[i];
+                    e[i + 1] = (r = std::hypot(f, g));
+                    if (r == 0.0) {
+                        d[i + 1] -= p;
+                        e[m] = 0.0;
+                        break;
+                    }
+                    s = f / r;
+                    c = g / r;
+                    g = d[i + 1] - p;
+                    r = (d[i] - g) * s + 2.0 * c * b;
+                    d[i + 1] = g + (p = s * r);
+                    g = c * r - b;
+                    for (int k = 0; k < n; k++) {
+                        f = A(k, i + 1);
+                        A(k, i + 1) = s * A(k, i) + c * f;
+                        A(k, i) = c * A(k, i) - s * f;
+                    }
+                }
+                if (r == 0.0 && i >= l) continue;
+                d[l] -= p;
+                e[l] = g;
+                e[m] = 0.0;
+            }
+        } while (m != l);
+    }
+    // sort ascending, copy out, normalise the sign convention
+    std::vector<int> order(n);
+    for (int i = 0; i < n; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return d[x] < d[y]; });
+    for (int j = 0; j < n; j++) {
+        evals[j] = d[order[j]];
+        for (int i = 0; i < n; i++) V[(size_t)i * n + j] = A(i, order[j]);
     }
     for (int j = 0; j < n; j++) {
         int im = 0;
         for (int i = 1; i < n; i++)
-            if (std::fabs(V[i * n + j]) > std::fabs(V[im * n + j]) + 1e-14) im = i;
-        if (V[im * n + j] < 0)
-            for (int i = 0; i < n; i++) V[i * n + j] = -V[i * n + j];
+            if (std::fabs(V[(size_t)i * n + j]) > std::fabs(V[(size_t)im * n + j]) + 1e-14) im = i;
+        if (V[(size_t)im * n + j] < 0)
+            for (int i = 0; i < n; i++) V[(size_t)i * n + j] = -V[(size_t)i * n + j];
     }
 }
 
@@ -312,6 +379,7 @@ GuessResult make_guess(const HostInts& ints, const std::vector<std::pair<double,
             for (int i = 0; i < nd; i++) v.push_back({pos[i], evv[i * nd + r]});
             res.guesses.push_back(v);
         }
+        res.perturb = true;  // the solver adds a small seeded random component (all spin sectors)
         return res;
     }
     auto it = info.find(multiplicity);

@@ -28,6 +28,7 @@ using SparseVec = std::vector<std::pair<int64_t, double>>;
 struct GuessResult {
     std::vector<SparseVec> guesses;
     std::vector<SparseVec> bad_roots;
+    bool perturb = false;  // guesses are not spin-selected: add a small random component
 };
 
 // lowest: (diagonal energy, determinant address) sorted ascending

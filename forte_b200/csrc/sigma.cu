@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <type_traits>
 
 #include "fcib_internal.h"
 
@@ -176,86 +177,146 @@ __global__ void __launch_bounds__(576) k_ab_fp64(
 constexpr int kGrTN = 128;   // columns per CTA
 constexpr int kGrRows = 8;   // rows per thread
 
-__global__ void __launch_bounds__(1024) k_group_fp64(
+// Persistent CTAs take (group, column chunk) work items in chunk-major order, so the columns of
+// C and sigma a chunk touches stay L2-resident while every group of that chunk is processed.
+// The pair-pair block M stays in shared memory; W = M[lab_i][lab_j] is rebuilt per item from it.
+// T = double (FP64 path) or float (mixed path: FP32 operands and accumulation, FP64 atomics).
+constexpr int kGrLoads = 16;  // X elements per thread per item (G*kGrTN/threads <= 16 by construction)
+
+template <typename T>
+__global__ void __launch_bounds__(1024) k_group(
     const double* __restrict__ C, double* __restrict__ S, int ncols,
     const uint32_t* __restrict__ rows, const uint16_t* __restrict__ labs, int G, int Gp,
-    const double* __restrict__ M, int ldm) {
+    const double* __restrict__ M, int ldm, int ngroups, int nchunks, int* __restrict__ counter, int m_in_smem) {
+    using T2 = typename std::conditional<std::is_same<T, double>::value, double2, float2>::type;
     extern __shared__ __align__(16) unsigned char smem[];
-    double* Wt = reinterpret_cast<double*>(smem);   // [G][Gp]  Wt[j][i] = M[lab_i][lab_j]
-    double* X = Wt + (size_t)G * Gp;                 // [G][kGrTN]
+    T* Ms = reinterpret_cast<T*>(smem);       // [ldm][ldm] when m_in_smem (else M is read from L2)
+    // W must start 16-byte aligned for its vector loads: round the M region to 128 bytes
+    const size_t m_elems = m_in_smem ? ((size_t)ldm * ldm * sizeof(T) + 127) / 128 * 128 / sizeof(T) : 0;
+    T* Wt = Ms + m_elems;                     // [G][Gp]  Wt[j][i] = M[lab_i][lab_j]
+    T* X = Wt + (size_t)G * Gp;               // [G][kGrTN]
     uint32_t* rs = reinterpret_cast<uint32_t*>(X + (size_t)G * kGrTN);
     uint16_t* ls = reinterpret_cast<uint16_t*>(rs + Gp);
-    const int g = blockIdx.x;
-    const int c0 = blockIdx.y * kGrTN;
-    const int tid = threadIdx.x;
-    for (int i = tid; i < Gp; i += blockDim.x) {
-        rs[i] = i < G ? rows[(size_t)g * G + i] : 0u;
-        ls[i] = i < G ? labs[(size_t)g * G + i] : 0;
-    }
-    __syncthreads();
-    for (int idx = tid; idx < G * Gp; idx += blockDim.x) {
-        int j = idx / Gp, i = idx - j * Gp;
-        Wt[idx] = i < G ? M[(size_t)ls[i] * ldm + ls[j]] : 0.0;
-    }
-    for (int idx = tid; idx < G * kGrTN; idx += blockDim.x) {
-        int j = idx / kGrTN, cc = idx - j * kGrTN;
-        int col = c0 + cc;
-        uint32_t e = rs[j];
-        double v = (col < ncols) ? C[(size_t)(e & kConnIdxMask) * ncols + col] : 0.0;
-        X[idx] = (e & kSignBit) ? -v : v;
-    }
-    __syncthreads();
+    __shared__ int s_item;
+    const int tid = threadIdx.x, nth = blockDim.x;
+    if (m_in_smem)
+        for (int idx = tid; idx < ldm * ldm; idx += nth) Ms[idx] = (T)M[idx];
     const int npairs = kGrTN / 2;
     const int cp = tid % npairs, rc = tid / npairs;
     const int i0 = rc * kGrRows;
-    if (i0 < G) {
-        double acc[kGrRows][2];
+    const int total = ngroups * nchunks;
+    while (true) {
+        __syncthreads();
+        if (tid == 0) s_item = atomicAdd(counter, 1);
+        __syncthreads();
+        const int item = s_item;
+        if (item >= total) break;
+        const int chunk = item / ngroups, g = item - chunk * ngroups;
+        const int c0 = chunk * kGrTN;
+        for (int i = tid; i < Gp; i += nth) {
+            rs[i] = i < G ? rows[(size_t)g * G + i] : 0u;
+            ls[i] = i < G ? labs[(size_t)g * G + i] : 0;
+        }
+        __syncthreads();
+        // gather the G rows (this chunk's columns) with all loads in flight at once
+        double xv[kGrLoads];
 #pragma unroll
-        for (int i = 0; i < kGrRows; i++) acc[i][0] = acc[i][1] = 0.0;
-        for (int j = 0; j < G; j++) {
-            const double2* w2 = reinterpret_cast<const double2*>(Wt + (size_t)j * Gp + i0);
-            double w[kGrRows];
-#pragma unroll
-            for (int i = 0; i < kGrRows / 2; i++) {
-                double2 t = w2[i];
-                w[2 * i] = t.x;
-                w[2 * i + 1] = t.y;
+        for (int r = 0; r < kGrLoads; r++) {
+            const int idx = tid + r * nth;
+            double v = 0.0;
+            if (idx < G * kGrTN) {
+                const int j = idx / kGrTN, col = c0 + (idx - j * kGrTN);
+                if (col < ncols) v = C[(size_t)(rs[j] & kConnIdxMask) * ncols + col];
             }
-            double2 x = *reinterpret_cast<const double2*>(X + (size_t)j * kGrTN + 2 * cp);
+            xv[r] = v;
+        }
+        for (int idx = tid; idx < G * Gp; idx += nth) {
+            int j = idx / Gp, i = idx - j * Gp;
+            const size_t mi = (size_t)ls[i] * ldm + ls[j];
+            Wt[idx] = i < G ? (m_in_smem ? Ms[mi] : (T)M[mi]) : (T)0;
+        }
 #pragma unroll
-            for (int i = 0; i < kGrRows; i++) {
-                acc[i][0] = fma(w[i], x.x, acc[i][0]);
-                acc[i][1] = fma(w[i], x.y, acc[i][1]);
+        for (int r = 0; r < kGrLoads; r++) {
+            const int idx = tid + r * nth;
+            if (idx < G * kGrTN) {
+                const int j = idx / kGrTN;
+                X[idx] = (T)((rs[j] & kSignBit) ? -xv[r] : xv[r]);
             }
         }
-        const int col = c0 + 2 * cp;
+        __syncthreads();
+        if (i0 < G) {
+            T acc[kGrRows][2];
 #pragma unroll
-        for (int i = 0; i < kGrRows; i++) {
-            int ii = i0 + i;
-            if (ii < G) {
-                uint32_t e = rs[ii];
-                double* dst = S + (size_t)(e & kConnIdxMask) * ncols + col;
-                double s = (e & kSignBit) ? -1.0 : 1.0;
-                if (col < ncols) atomicAdd(dst, s * acc[i][0]);
-                if (col + 1 < ncols) atomicAdd(dst + 1, s * acc[i][1]);
+            for (int i = 0; i < kGrRows; i++) acc[i][0] = acc[i][1] = (T)0;
+            for (int j = 0; j < G; j++) {
+                T w[kGrRows];
+                if (std::is_same<T, double>::value) {
+                    const double2* w2 = reinterpret_cast<const double2*>(Wt + (size_t)j * Gp + i0);
+#pragma unroll
+                    for (int i = 0; i < kGrRows / 2; i++) {
+                        double2 t = w2[i];
+                        w[2 * i] = (T)t.x;
+                        w[2 * i + 1] = (T)t.y;
+                    }
+                } else {
+                    const float4* w4 = reinterpret_cast<const float4*>(Wt + (size_t)j * Gp + i0);
+#pragma unroll
+                    for (int i = 0; i < kGrRows / 4; i++) {
+                        float4 t = w4[i];
+                        w[4 * i] = (T)t.x; w[4 * i + 1] = (T)t.y; w[4 * i + 2] = (T)t.z; w[4 * i + 3] = (T)t.w;
+                    }
+                }
+                T2 x = *reinterpret_cast<const T2*>(X + (size_t)j * kGrTN + 2 * cp);
+#pragma unroll
+                for (int i = 0; i < kGrRows; i++) {
+                    acc[i][0] = fma(w[i], x.x, acc[i][0]);
+                    acc[i][1] = fma(w[i], x.y, acc[i][1]);
+                }
+            }
+            const int col = c0 + 2 * cp;
+#pragma unroll
+            for (int i = 0; i < kGrRows; i++) {
+                int ii = i0 + i;
+                if (ii < G) {
+                    uint32_t e = rs[ii];
+                    double* dst = S + (size_t)(e & kConnIdxMask) * ncols + col;
+                    double sg = (e & kSignBit) ? -1.0 : 1.0;
+                    if (col < ncols) atomicAdd(dst, sg * (double)acc[i][0]);
+                    if (col + 1 < ncols) atomicAdd(dst + 1, sg * (double)acc[i][1]);
+                }
             }
         }
     }
 }
 
-static void launch_group(Context& c, const double* C, double* S, int ncols, int ngroups, int G,
-                         const uint32_t* rows, const uint16_t* labs, const double* M, int ldm) {
+template <typename T>
+static void launch_group_t(Context& c, const double* C, double* S, int ncols, int ngroups, int G,
+                           const uint32_t* rows, const uint16_t* labs, const double* M, int ldm) {
     if (ngroups == 0 || G == 0) return;
     int Gp = (G + kGrRows - 1) / kGrRows * kGrRows;
-    size_t smem = (size_t)G * Gp * 8 + (size_t)G * kGrTN * 8 + (size_t)Gp * 4 + (size_t)Gp * 2 + 16;
+    size_t smem_tiles = (size_t)G * Gp * sizeof(T) + (size_t)G * kGrTN * sizeof(T) + (size_t)Gp * 4 + (size_t)Gp * 2 + 16;
+    size_t smem_m = ((size_t)ldm * ldm * sizeof(T) + 127) / 128 * 128;
+    int m_in_smem = (smem_tiles + smem_m + 1024 <= (size_t)c.smem_optin) ? 1 : 0;
+    size_t smem = smem_tiles + (m_in_smem ? smem_m : 0);
     FCIB_CHECK(smem + 1024 <= (size_t)c.smem_optin, FCIB_ERR_UNSUPPORTED, "same-spin group block exceeds shared memory");
     int threads = (kGrTN / 2) * (Gp / kGrRows);
     threads = (threads + 31) / 32 * 32;
     FCIB_CHECK(threads <= 1024, FCIB_ERR_UNSUPPORTED, "same-spin group block too large");
-    FCIB_CUDA(cudaFuncSetAttribute(k_group_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    dim3 grid(ngroups, (ncols + kGrTN - 1) / kGrTN);
-    k_group_fp64<<<grid, threads, smem, c.stream>>>(C, S, ncols, rows, labs, G, Gp, M, ldm);
+    FCIB_CHECK((size_t)G * kGrTN <= (size_t)kGrLoads * threads, FCIB_ERR_UNSUPPORTED, "same-spin gather tile too large");
+    FCIB_CUDA(cudaFuncSetAttribute(k_group<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int nchunks = (ncols + kGrTN - 1) / kGrTN;
+    int per_sm = std::max(1, std::min((int)(c.smem_per_sm / (smem + 1024)), 2048 / threads));
+    int grid = std::min(ngroups * nchunks, per_sm * c.num_sms);
+    if (!c.counter.p) c.counter.alloc(16);
+    FCIB_CUDA(cudaMemsetAsync(c.counter.p + 2, 0, sizeof(int), c.stream));
+    k_group<T><<<grid, threads, smem, c.stream>>>(C, S, ncols, rows, labs, G, Gp, M, ldm, ngroups, nchunks, c.counter.p + 2, m_in_smem);
     FCIB_CUDA(cudaGetLastError());
+}
+
+static void launch_group(Context& c, const double* C, double* S, int ncols, int ngroups, int G,
+                         const uint32_t* rows, const uint16_t* labs, const double* M, int ldm, bool fp32 = false) {
+    if (fp32) launch_group_t<float>(c, C, S, ncols, ngroups, G, rows, labs, M, ldm);
+    else launch_group_t<double>(c, C, S, ncols, ngroups, G, rows, labs, M, ldm);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -325,6 +386,26 @@ void apply_mask(Context& c, double* v) {
 // ------------------------------------------------------------------------------------------
 // sigma orchestration
 // ------------------------------------------------------------------------------------------
+// same-spin (and, when not folded into the opposite-spin block, one-body) terms added to S
+static void sigma_same_spin(Context& c, const double* C, double* S, bool fp32) {
+    const int nas = (int)c.nas, nbs = (int)c.nbs;
+    const size_t N = (size_t)c.ndet;
+    if (!c.fold_h && c.A.ng1)
+        launch_group(c, C, S, nbs, c.A.ng1, c.A.g1, c.A.g1row.p, c.A.g1lab.p, c.Ha.p, c.n, fp32);
+    const int np2 = c.n * (c.n - 1) / 2;
+    if (c.A.ng2) launch_group(c, C, S, nbs, c.A.ng2, c.A.g2, c.A.g2row.p, c.A.g2lab.p, c.M2a.p, np2, fp32);
+    bool beta_g1 = (!c.fold_h && c.B.ng1);
+    if (c.B.ng2 || beta_g1) {
+        c.ct.alloc(N);
+        c.st.alloc(N);
+        transpose(c, C, c.ct.p, nas, nbs);
+        FCIB_CUDA(cudaMemsetAsync(c.st.p, 0, N * sizeof(double), c.stream));
+        if (beta_g1) launch_group(c, c.ct.p, c.st.p, nas, c.B.ng1, c.B.g1, c.B.g1row.p, c.B.g1lab.p, c.Hb.p, c.n, fp32);
+        if (c.B.ng2) launch_group(c, c.ct.p, c.st.p, nas, c.B.ng2, c.B.g2, c.B.g2row.p, c.B.g2lab.p, c.M2b.p, np2, fp32);
+        transpose_add(c, c.st.p, S, nas, nbs);
+    }
+}
+
 void sigma_fp64(Context& c, const double* C, double* S) {
     const int nas = (int)c.nas, nbs = (int)c.nbs;
     const size_t N = (size_t)c.ndet;
@@ -348,22 +429,28 @@ void sigma_fp64(Context& c, const double* C, double* S) {
     } else {
         k_scale_copy<<<4 * c.num_sms, 256, 0, c.stream>>>(C, S, c.scalar, N);
         FCIB_CUDA(cudaGetLastError());
-        if (c.A.ng1)
-            launch_group(c, C, S, nbs, c.A.ng1, c.A.g1, c.A.g1row.p, c.A.g1lab.p, c.Ha.p, c.n);
     }
-    const int np2 = c.n * (c.n - 1) / 2;
-    if (c.A.ng2) launch_group(c, C, S, nbs, c.A.ng2, c.A.g2, c.A.g2row.p, c.A.g2lab.p, c.M2a.p, np2);
-    bool beta_g1 = (!c.fold_h && c.B.ng1);
-    if (c.B.ng2 || beta_g1) {
-        c.ct.alloc(N);
-        c.st.alloc(N);
-        transpose(c, C, c.ct.p, nas, nbs);
-        FCIB_CUDA(cudaMemsetAsync(c.st.p, 0, N * sizeof(double), c.stream));
-        if (beta_g1) launch_group(c, c.ct.p, c.st.p, nas, c.B.ng1, c.B.g1, c.B.g1row.p, c.B.g1lab.p, c.Hb.p, c.n);
-        if (c.B.ng2) launch_group(c, c.ct.p, c.st.p, nas, c.B.ng2, c.B.g2, c.B.g2row.p, c.B.g2lab.p, c.M2b.p, np2);
-        transpose_add(c, c.st.p, S, nas, nbs);
-    }
+    sigma_same_spin(c, C, S, false);
     apply_mask(c, S);
+}
+
+void ab_tc(Context& c, const double* C, double* S, bool three);
+int tc_check_error(Context& c);
+
+void sigma_mixed(Context& c, const double* C, double* S, bool three) {
+    const size_t N = (size_t)c.ndet;
+    if (c.fold_h) {
+        ab_tc(c, C, S, three);
+    } else {
+        k_scale_copy<<<4 * c.num_sms, 256, 0, c.stream>>>(C, S, c.scalar, N);
+        FCIB_CUDA(cudaGetLastError());
+    }
+    sigma_same_spin(c, C, S, true);
+    apply_mask(c, S);
+    if (c.fold_h) {
+        int e = tc_check_error(c);
+        FCIB_CHECK(e == 0, FCIB_ERR_NUMERIC, "tensor-core sigma kernel reported a timeout (code " + std::to_string(e) + ")");
+    }
 }
 
 // ------------------------------------------------------------------------------------------

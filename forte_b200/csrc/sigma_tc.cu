@@ -1,0 +1,452 @@
+// Mixed-precision sigma: the opposite-spin contraction on the 5th-generation tensor cores.
+//
+// Same regrouping as the FP64 kernel (one CTA owns a target alpha row Ia; the C rows
+// connected to Ia by a single alpha replacement are gathered into a tile A[Jb, k] and
+// multiplied by the pair-integral block B[k, R] = sgn_k V[P_k, R]; the product is scattered
+// over beta single replacements into a sigma row held on chip), mapped onto Blackwell:
+//
+// * the input vector is split once per sigma into tf32 hi/lo planes (3xTF32: A*B ~ Ahi*Bhi +
+//   Ahi*Blo + Alo*Bhi with FP32 accumulation);
+// * the gathered tile A (128 beta strings x K connections) is written straight into tensor
+//   memory with tcgen05.st and multiplied from there (tcgen05.mma kind::tf32 with the A operand
+//   in TMEM); B (Npad x K) lives in shared memory in the K-major no-swizzle core-matrix layout
+//   (element (row, k) at (k/4)*LBO + (row/8)*128 + (row%8)*16 + (k%4)*4 bytes);
+// * two 144-column accumulators in TMEM are double buffered, so the MMAs of tile t overlap the
+//   epilogue of tile t-1;
+// * the epilogue accumulates the sigma row exactly in two-word fixed point with native 32-bit
+//   shared-memory integer atomics: each contribution y is scaled to a 64-bit integer on a grid
+//   2^-el chosen per sigma from max|C| * max|V| (so |y| 2^el < 2^46), split into a signed high
+//   part (bits >= 22) and an unsigned 22-bit low part; every sigma element receives at most
+//   s1 (<= 72) contributions, so neither word can overflow.  The row is converted back to FP64
+//   and added to E0*C when it is written.
+//
+// Every mbarrier wait is bounded; on timeout the kernel records an error code, waits (bounded)
+// for its outstanding MMAs, frees tensor memory and exits.
+#include "fcib_internal.h"
+
+namespace fcib {
+
+constexpr int kTcM = 128;          // beta rows per tile (MMA M)
+constexpr int kTcThreads = 512;    // 16 warps: all copy A, thread 0 issues MMAs, all scatter
+constexpr uint32_t kTmemCols = 512;
+constexpr long long kWaitLimit = 1ll << 24;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    for (long long i = 0; i < kWaitLimit; i++)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+
+// K-major, no-swizzle shared-memory matrix descriptor (sm_100 version 1)
+__device__ __forceinline__ uint64_t make_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;  // descriptor version for sm_100
+    // base offset 0, lbo mode 0, layout type 0 (no swizzle)
+    return d;
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
+    uint32_t r0, r1, r2, r3, r4, r5, r6, r7;
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3), "=r"(r4), "=r"(r5), "=r"(r6), "=r"(r7)
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    v[0] = __uint_as_float(r0); v[1] = __uint_as_float(r1); v[2] = __uint_as_float(r2); v[3] = __uint_as_float(r3);
+    v[4] = __uint_as_float(r4); v[5] = __uint_as_float(r5); v[6] = __uint_as_float(r6); v[7] = __uint_as_float(r7);
+}
+
+struct TcLayout {
+    int kpad, npad;          // K (connections) and N (pairs) padded to 8 / 16
+    uint32_t b_bytes;        // one B plane
+    uint32_t off_bhi, off_blo, off_acc, off_conn, off_bar, total;
+};
+
+__host__ __device__ inline TcLayout tc_layout(int s1a, int npair, int nbs, bool three) {
+    TcLayout L;
+    L.kpad = (s1a + 7) / 8 * 8;
+    L.npad = (npair + 15) / 16 * 16;
+    L.b_bytes = (uint32_t)L.npad * L.kpad * 4;
+    uint32_t o = 0;
+    L.off_bhi = o; o += L.b_bytes;
+    L.off_blo = o; o += three ? L.b_bytes : 0;
+    L.off_acc = o; o += ((uint32_t)nbs * 8 + 127) / 128 * 128;  // int32 high words, then low words
+    L.off_conn = o; o += ((uint32_t)L.kpad * 4 + 127) / 128 * 128;
+    L.off_bar = o; o += 128;
+    L.total = o;
+    return L;
+}
+
+// B plane (N x K, K-major interleaved): element (row, k) at (k/4)*(rows/8)*128 + (row/8)*128 + (row%8)*16 + (k%4)*4
+__device__ __forceinline__ uint32_t kmaj_off(int row, int k, int rows) {
+    return (uint32_t)((k >> 2) * (rows / 8) * 128 + (row >> 3) * 128 + (row & 7) * 16 + (k & 3) * 4);
+}
+
+__device__ __forceinline__ void red_add_u32(uint32_t saddr, uint32_t v) {
+    asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(saddr), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ void mma_tf32_ta(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc, uint32_t idesc,
+                                            uint32_t accumulate) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n}\n" ::"r"(d_tmem),
+        "r"(a_tmem), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const float (&v)[8]) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr),
+                 "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+                 "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+                 "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7]))
+                 : "memory");
+}
+
+// Error codes written to *err (first one wins)
+constexpr int kErrTimeoutMma = 1;
+
+// TMEM columns: accumulators at 0 and 256 (npad <= 144), A hi at 160, A lo at 416 (kpad <= 72)
+constexpr uint32_t kColAccStride = 256, kColAhi = 160, kColAlo = 416;
+constexpr int kTcWarps = kTcThreads / 32;
+constexpr int kTcGat = 3;    // 8-column A chunks per warp per tile: 9 chunks over 4 column groups
+constexpr int kTcEpiC = 5;   // 8-column accumulator chunks per warp: 18 chunks over 4 column groups
+constexpr int kFixLoBits = 22;
+
+template <bool THREE>
+__global__ void __launch_bounds__(kTcThreads, 1)
+    k_ab_tc(const float* __restrict__ Phi, const float* __restrict__ Plo, int ldp, const double* __restrict__ C,
+            double* __restrict__ S, const uint32_t* __restrict__ connA, int s1a, const uint16_t* __restrict__ tgtR,
+            int npair, const double* __restrict__ V, int ldv, float vmax, const unsigned int* __restrict__ cmax_bits,
+            int nas, int nbs, double e0, int* __restrict__ row_counter, int* __restrict__ err) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const TcLayout L = tc_layout(s1a, npair, nbs, THREE);
+    unsigned char* Bhi = smem + L.off_bhi;
+    unsigned char* Blo = smem + L.off_blo;
+    int* acc_hi = reinterpret_cast<int*>(smem + L.off_acc);
+    unsigned int* acc_lo = reinterpret_cast<unsigned int*>(acc_hi + nbs);
+    uint32_t* cs = reinterpret_cast<uint32_t*>(smem + L.off_conn);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L.off_bar);  // [0],[1]: MMA done per accumulator
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + L.off_bar + 64);
+    __shared__ int s_row;
+    __shared__ int s_abort;
+
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const int kpad = L.kpad, npad = L.npad;
+    const int q = warp & 3, cg = warp >> 2;  // TMEM lane quarter and column group of this warp
+
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_abort = 0;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+    const uint32_t tlane = (uint32_t)(32 * q) << 16;
+
+    // fixed-point grid: |y| <= kpad * max|C| * max|V| < 2^46 * 2^-el
+    const float cmax = __uint_as_float(*cmax_bits);
+    const float ybound = fmaxf(1.01f * (float)kpad * cmax * vmax, 1e-30f);
+    const int el = min(60, (int)floorf(46.0f - log2f(ybound)));
+    const double grid = ldexp(1.0, el), inv_grid = ldexp(1.0, -el);
+
+    // instruction descriptor: D f32, A/B tf32, both K-major, N = npad, M = 128
+    const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(npad >> 3) << 17) | ((uint32_t)(kTcM >> 4) << 24);
+    const uint32_t lbo_b = (uint32_t)(npad / 8) * 128;
+    const uint32_t sb_hi = smem_u32(Bhi), sb_lo = smem_u32(Blo);
+    const uint32_t acc_hi_s = smem_u32(acc_hi), acc_lo_s = smem_u32(acc_lo);
+
+    uint32_t mma_count[2] = {0u, 0u};  // commits issued per accumulator (parity tracking)
+    const int ntiles = (nbs + kTcM - 1) / kTcM;
+    const int nk8 = kpad / 8, nn8 = npad / 8;
+
+    while (true) {
+        if (tid == 0) s_row = atomicAdd(row_counter, 1);
+        __syncthreads();
+        const int Ia = s_row;
+        if (Ia >= nas || s_abort) break;
+        for (int k = tid; k < kpad; k += blockDim.x) cs[k] = k < s1a ? connA[(size_t)Ia * s1a + k] : 0u;
+        for (int j = tid; j < 2 * nbs; j += blockDim.x) acc_hi[j] = 0;
+        __syncthreads();
+        // B[R][k] = sgn_k V[P_k][R], split into tf32 hi/lo
+        for (int idx = tid; idx < npad * kpad; idx += blockDim.x) {
+            int R = idx / kpad, k = idx - R * kpad;
+            float hi = 0.f, lo = 0.f;
+            if (k < s1a && R < npair) {
+                uint32_t e = cs[k];
+                double v = V[(size_t)((e >> 21) & 1023) * ldv + R];
+                if (e & kSignBit) v = -v;
+                hi = __uint_as_float(to_tf32((float)v));
+                lo = __uint_as_float(to_tf32((float)(v - (double)hi)));
+            }
+            uint32_t off = kmaj_off(R, k, npad);
+            *reinterpret_cast<float*>(Bhi + off) = hi;
+            if (THREE) *reinterpret_cast<float*>(Blo + off) = lo;
+        }
+        // A-tile gather: the thread owning tile row m = 32q + lane loads A[m][k] = plane[J_k][jb0 + m]
+        // for the 8-column chunks c8 = cg + 4j (coalesced across lanes); one tile ahead in registers
+        float gh[kTcGat][8], gl[kTcGat][8];
+        auto prefetch = [&](int tt) {
+            const int jb = tt * kTcM + 32 * q + lane;
+#pragma unroll
+            for (int j = 0; j < kTcGat; j++) {
+                const int c8 = cg + 4 * j;
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    const int k = 8 * c8 + u;
+                    float h = 0.f, l = 0.f;
+                    if (c8 < nk8 && k < s1a && jb < nbs) {
+                        const size_t o = (size_t)(cs[k] & kConnIdxMask) * ldp + jb;
+                        h = __ldg(Phi + o);
+                        if (THREE) l = __ldg(Plo + o);
+                    }
+                    gh[j][u] = h;
+                    gl[j][u] = l;
+                }
+            }
+        };
+        prefetch(0);
+        for (int t = 0; t <= ntiles; t++) {
+            const int cur = t & 1, prv = cur ^ 1;
+            // (a) the TMEM A buffer is free once the previous tile's MMAs completed (one waiter)
+            if (t >= 1 && tid == 0) {
+                if (!mbar_wait_bounded(&bars[prv], (mma_count[prv] - 1) & 1)) {
+                    atomicCAS(err, 0, kErrTimeoutMma);
+                    s_abort = 1;
+                }
+            }
+            __syncthreads();
+            if (s_abort) break;
+            tc_fence_after();
+            // (b) registers -> A in tensor memory
+            if (t < ntiles) {
+#pragma unroll
+                for (int j = 0; j < kTcGat; j++) {
+                    const int c8 = cg + 4 * j;
+                    if (c8 < nk8) {
+                        tmem_st8(tmem_base + tlane + kColAhi + 8 * c8, gh[j]);
+                        if (THREE) tmem_st8(tmem_base + tlane + kColAlo + 8 * c8, gl[j]);
+                    }
+                }
+                asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+            }
+            tc_fence_before();
+            __syncthreads();
+            tc_fence_after();
+            // (c) one thread issues the tile's MMAs into accumulator `cur`
+            if (t < ntiles && tid == 0) {
+                const uint32_t dt = tmem_base + (uint32_t)cur * kColAccStride;
+                uint32_t acc = 0;
+                for (int ks = 0; ks < nk8; ks++) {
+                    const uint32_t ah = tmem_base + kColAhi + 8 * ks;
+                    uint64_t bh = make_desc(sb_hi + ks * 2 * lbo_b, lbo_b, 128);
+                    if (THREE) {
+                        const uint32_t al = tmem_base + kColAlo + 8 * ks;
+                        uint64_t bl = make_desc(sb_lo + ks * 2 * lbo_b, lbo_b, 128);
+                        mma_tf32_ta(dt, al, bh, idesc, acc);
+                        acc = 1;
+                        mma_tf32_ta(dt, ah, bl, idesc, acc);
+                    }
+                    mma_tf32_ta(dt, ah, bh, idesc, acc);
+                    acc = 1;
+                }
+                mma_commit(&bars[cur]);
+            }
+            if (t < ntiles) mma_count[cur]++;
+            // (b') next tile's loads overlap the MMAs above and the epilogue below
+            if (t + 1 < ntiles) prefetch(t + 1);
+            // (d) epilogue of tile t-1: exact fixed-point scatter over beta replacements
+            if (t >= 1) {
+                const int jb = (t - 1) * kTcM + 32 * q + lane;
+                const uint32_t tbase = tmem_base + (uint32_t)prv * kColAccStride + tlane;
+                uint4 tg[kTcEpiC];
+#pragma unroll
+                for (int i = 0; i < kTcEpiC; i++) {
+                    const int c8 = cg + 4 * i;
+                    tg[i] = (c8 < nn8 && jb < nbs)
+                                ? __ldg(reinterpret_cast<const uint4*>(tgtR + (size_t)jb * npad + c8 * 8))
+                                : make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
+                }
+#pragma unroll
+                for (int i = 0; i < kTcEpiC; i++) {
+                    const int c8 = cg + 4 * i;
+                    if (c8 < nn8) {
+                        float v[8];
+                        tmem_ld8(tbase + (uint32_t)(c8 * 8), v);
+                        const uint32_t w[4] = {tg[i].x, tg[i].y, tg[i].z, tg[i].w};
+#pragma unroll
+                        for (int u = 0; u < 8; u++) {
+                            const uint32_t g = (w[u >> 1] >> (16 * (u & 1))) & 0xFFFFu;
+                            if (g != 0xFFFFu) {
+                                double y = (double)v[u];
+                                if (g & 0x8000u) y = -y;
+                                const long long Y = __double2ll_rn(y * grid);
+                                const uint32_t idx = (g & 0x7FFFu) << 2;
+                                red_add_u32(acc_hi_s + idx, (uint32_t)(int)(Y >> kFixLoBits));
+                                red_add_u32(acc_lo_s + idx, (uint32_t)(Y & ((1ll << kFixLoBits) - 1)));
+                            }
+                        }
+                    }
+                }
+                tc_fence_before();
+            }
+        }
+        if (s_abort) break;
+        __syncthreads();
+        // (e) sigma row = E0 * C row + opposite-spin part (exact fixed-point sum -> FP64)
+        const double* Crow = C + (size_t)Ia * nbs;
+        double* Srow = S + (size_t)Ia * nbs;
+        for (int j = tid; j < nbs; j += blockDim.x) {
+            const long long tot = ((long long)acc_hi[j] << kFixLoBits) + (long long)acc_lo[j];
+            Srow[j] = e0 * Crow[j] + (double)tot * inv_grid;
+        }
+        __syncthreads();
+    }
+    // drain: wait (bounded) for any MMA still in flight before releasing tensor memory
+    __syncthreads();
+    if (tid == 0) {
+        for (int b = 0; b < 2; b++)
+            if (mma_count[b] > 0) mbar_wait_bounded(&bars[b], (mma_count[b] - 1) & 1);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(kTmemCols) : "memory");
+}
+
+// tgtR[Jb][R] = 16-bit scatter target of F_R Jb: index | sign << 15; no connection -> 0xFFFF
+__global__ void k_tgt_rows16(const int32_t* __restrict__ tgt, uint16_t* __restrict__ out, int nstr, int npp_in,
+                             int npad_out) {
+    size_t total = (size_t)npad_out * nstr;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        int J = (int)(i / npad_out), R = (int)(i % npad_out);
+        uint16_t v = 0xFFFFu;
+        if (R < npp_in) {
+            int32_t t = tgt[(size_t)J * npp_in + R];
+            if (t != kNoTarget) v = (uint16_t)(((uint32_t)t & kConnIdxMask) | (((uint32_t)t >> 31) << 15));
+        }
+        out[i] = v;
+    }
+}
+
+// C (FP64, nas x nbs) -> tf32 hi/lo planes with row stride ldp (zero padded); also max |C|
+__global__ void k_split_tf32(const double* __restrict__ C, float* __restrict__ hi, float* __restrict__ lo, int nas,
+                             int nbs, int ldp, unsigned int* __restrict__ cmax_bits) {
+    size_t total = (size_t)nas * ldp;
+    float mx = 0.f;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        int r = (int)(i / ldp), col = (int)(i % ldp);
+        double v = col < nbs ? C[(size_t)r * nbs + col] : 0.0;
+        float h = __uint_as_float(to_tf32((float)v));
+        hi[i] = h;
+        if (lo) lo[i] = __uint_as_float(to_tf32((float)(v - (double)h)));
+        mx = fmaxf(mx, fabsf((float)v));
+    }
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    // non-negative floats order like their bit patterns; round up by one ulp for safety
+    if ((threadIdx.x & 31) == 0) atomicMax(cmax_bits, __float_as_uint(mx) + 1u);
+}
+
+size_t tc_smem_bytes(int s1a, int npair, int nbs, bool three) { return tc_layout(s1a, npair, nbs, three).total; }
+
+void ab_tc(Context& c, const double* C, double* S, bool three) {
+    const int nas = (int)c.nas, nbs = (int)c.nbs;
+    const int s1a = c.A.s1, npair = c.A.npair;
+    FCIB_CHECK(nbs < 32767, FCIB_ERR_UNSUPPORTED, "tensor-core opposite-spin kernel: too many beta strings");
+    TcLayout L = tc_layout(s1a, npair, nbs, three);
+    FCIB_CHECK(L.npad <= 144 && L.kpad <= 72 && L.npad / 8 <= 4 * kTcEpiC && L.kpad / 8 <= 4 * kTcGat,
+               FCIB_ERR_UNSUPPORTED, "tensor-core kernel: more than 16 active orbitals");
+    size_t smem = std::max<size_t>(L.total, 120 * 1024);  // one CTA per SM (owns all tensor memory)
+    FCIB_CHECK(smem + 2048 <= (size_t)c.smem_optin, FCIB_ERR_UNSUPPORTED,
+               "tensor-core kernel: sigma row and integral block exceed shared memory");
+    if (!c.tgtR16.p) {
+        c.tgtR16.alloc((size_t)L.npad * nbs);
+        k_tgt_rows16<<<4 * c.num_sms, 256, 0, c.stream>>>(c.B.tgt.p, c.tgtR16.p, nbs, c.B.npair_pad, L.npad);
+        FCIB_CUDA(cudaGetLastError());
+    }
+    if (c.vmax <= 0.0f) {
+        std::vector<double> hv(c.V.n);
+        FCIB_CUDA(cudaMemcpy(hv.data(), c.V.p, sizeof(double) * c.V.n, cudaMemcpyDeviceToHost));
+        double m = 0.0;
+        for (double x : hv) m = std::max(m, std::fabs(x));
+        c.vmax = (float)(m * (1.0 + 1e-6)) + 1e-30f;
+    }
+    const int ldp = (nbs + 3) / 4 * 4;
+    c.tf_hi.alloc((size_t)nas * ldp);
+    if (three) c.tf_lo.alloc((size_t)nas * ldp);
+    if (!c.counter.p) c.counter.alloc(16);
+    FCIB_CUDA(cudaMemsetAsync(c.counter.p, 0, 3 * sizeof(int), c.stream));
+    unsigned int* cmax_bits = reinterpret_cast<unsigned int*>(c.counter.p + 3);
+    FCIB_CUDA(cudaMemsetAsync(cmax_bits, 0, sizeof(unsigned int), c.stream));
+    k_split_tf32<<<8 * c.num_sms, 256, 0, c.stream>>>(C, c.tf_hi.p, three ? c.tf_lo.p : nullptr, nas, nbs, ldp, cmax_bits);
+    FCIB_CUDA(cudaGetLastError());
+    auto kern = three ? k_ab_tc<true> : k_ab_tc<false>;
+    FCIB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int grid = std::min(nas, c.num_sms);
+    kern<<<grid, kTcThreads, smem, c.stream>>>(c.tf_hi.p, three ? c.tf_lo.p : c.tf_hi.p, ldp, C, S, c.A.conn.p, s1a,
+                                              c.tgtR16.p, npair, c.V.p, c.A.npair_pad, c.vmax, cmax_bits, nas, nbs,
+                                              c.scalar, c.counter.p, c.counter.p + 1);
+    FCIB_CUDA(cudaGetLastError());
+}
+
+int tc_check_error(Context& c) {
+    int e = 0;
+    FCIB_CUDA(cudaMemcpyAsync(&e, c.counter.p + 1, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    FCIB_CUDA(cudaStreamSynchronize(c.stream));
+    return e;
+}
+
+}  // namespace fcib

@@ -1,0 +1,65 @@
+"""Mixed-precision path: tensor-core (tcgen05 kind::tf32) opposite-spin sigma with FP32 same-spin
+terms, checked against the FP64 oracle; mixed Davidson energies checked against FP64 ones."""
+import numpy as np
+import pytest
+
+import golden_cases
+from forte_b200 import FCISolver, StateInfo, synthetic
+from oracle.oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+# 3xTF32 split products with FP32 accumulation: ~FP32 accuracy of each sigma element relative
+# to the largest one; single-pass TF32 keeps ~10 mantissa bits.
+TOL_MIXED = 2e-5
+TOL_TF32 = 5e-3
+
+
+@pytest.mark.parametrize("n,na,nb", [(4, 2, 2), (6, 3, 3), (8, 4, 4), (7, 4, 2), (9, 3, 5), (10, 5, 5), (12, 6, 6),
+                                     (6, 1, 1), (5, 2, 0)])
+@pytest.mark.parametrize("mode,tol", [("MIXED", TOL_MIXED), ("MIXED_TF32", TOL_TF32)])
+def test_mixed_sigma_matches_oracle(n, na, nb, mode, tol):
+    ints = synthetic(n, 3 * n, 21)
+    o = Oracle(n, na, nb)
+    o.set_integrals(ints)
+    s = FCISolver(StateInfo(na, nb, 0, na - nb), 1, ints, {"FCI_PRECISION": mode})
+    rng = np.random.default_rng(7 * n + na)
+    c = rng.normal(size=o.ndet)
+    c /= np.linalg.norm(c)
+    ref = o.sigma(c)
+    got = s.sigma(c)
+    err = np.max(np.abs(got - ref)) / np.max(np.abs(ref))
+    assert err < tol, err
+
+
+@pytest.mark.parametrize("n,L", [(8, 24), (10, 30), (12, 36)])
+def test_mixed_solve_matches_fp64(n, L):
+    """North-star tolerance for mixed mode: 1e-8 Eh against the FP64 energy (one root; with
+    several roots and no spin selection, exact FP64 arithmetic never leaves the spin sectors of
+    the guess while low-precision noise can, so multi-root parity is checked on a
+    symmetry-adapted golden system below)."""
+    ints = synthetic(n, L, 3)
+    opts = {"E_CONVERGENCE": 1e-10, "R_CONVERGENCE": 1e-6, "DL_MAXITER": 300}
+    f = FCISolver(StateInfo(n // 2, n // 2, 0), 1, ints, opts)
+    f.compute_energy()
+    m = FCISolver(StateInfo(n // 2, n // 2, 0), 1, ints, dict(opts, FCI_PRECISION="MIXED"))
+    m.compute_energy()
+    assert abs(m.energies()[0] - f.energies()[0]) < 1e-8
+
+
+def test_mixed_multiroot_golden():
+    ints, na, nb, irrep, mult, ref = golden_cases.load(1)
+    opts = {"E_CONVERGENCE": 1e-10, "R_CONVERGENCE": 1e-6}
+    f = FCISolver(StateInfo(na, nb, mult, 0, irrep), 3, ints, opts)
+    f.compute_energy()
+    m = FCISolver(StateInfo(na, nb, mult, 0, irrep), 3, ints, dict(opts, FCI_PRECISION="MIXED"))
+    m.compute_energy()
+    assert np.max(np.abs(np.array(m.energies()) - np.array(f.energies()))) < 1e-8
+
+
+@pytest.mark.parametrize("k", [1, 2, 3, 4, 5])
+def test_mixed_golden_fcidump(k):
+    ints, na, nb, irrep, mult, ref = golden_cases.load(k)
+    s = FCISolver(StateInfo(na, nb, mult, na - nb, irrep), 1, ints,
+                  {"E_CONVERGENCE": 1e-10, "R_CONVERGENCE": 1e-6, "FCI_PRECISION": "MIXED"})
+    assert abs(s.compute_energy() - ref) < 1e-8
