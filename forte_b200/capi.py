@@ -47,6 +47,15 @@ class FcibOptions(C.Structure):
     ]
 
 
+class FcibProfile(C.Structure):
+    _fields_ = [
+        ("total_ms", C.c_double), ("sigma_ms", C.c_double), ("ab_ms", C.c_double), ("same_ms", C.c_double),
+        ("ab64_ms", C.c_double), ("same64_ms", C.c_double),
+        ("guess_ms", C.c_double), ("iterations", C.c_int), ("n_sigma", C.c_int), ("n_sigma_fp64", C.c_int),
+        ("n_ab", C.c_int), ("n_ab64", C.c_int), ("launches", C.c_ulonglong),
+    ]
+
+
 class FcibError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"fcib error {code}: {msg}")
@@ -79,6 +88,8 @@ SIGNATURES = {
                                     C.POINTER(C.c_int64), C.POINTER(C.c_int8), C.POINTER(C.c_uint32),
                                     C.POINTER(C.c_uint32)]),
     "fcib_last_timing": (C.c_int, [_vp, _dp, C.POINTER(C.c_int), _dp]),
+    "fcib_get_profile": (C.c_int, [_vp, C.POINTER(FcibProfile)]),
+    "fcib_stream": (C.c_int, [_vp, C.POINTER(C.c_void_p)]),
 }
 
 

@@ -12,6 +12,7 @@ struct fcib_ctx {
 
 namespace fcib {
 
+unsigned long long g_launch_count = 0;
 static thread_local std::string g_last_error;
 void set_error(const std::string& msg) { g_last_error = msg; }
 
@@ -420,6 +421,31 @@ int fcib_last_timing(fcib_ctx* ctx, double* sigma_ms, int* n_sigma, double* tota
     if (sigma_ms) *sigma_ms = ctx->c.t_sigma_ms;
     if (n_sigma) *n_sigma = ctx->c.n_sigma;
     if (total_ms) *total_ms = ctx->c.t_total_ms;
+    return FCIB_OK;
+}
+
+int fcib_get_profile(fcib_ctx* ctx, fcib_profile* o) {
+    if (!ctx || !o) { set_error("null argument"); return FCIB_ERR_ARG; }
+    const Context& c = ctx->c;
+    o->total_ms = c.t_total_ms;
+    o->sigma_ms = c.t_sigma_ms;
+    o->ab_ms = c.t_ab_ms;
+    o->same_ms = c.t_same_ms;
+    o->ab64_ms = c.t_ab64_ms;
+    o->same64_ms = c.t_same64_ms;
+    o->n_ab64 = c.n_ab64;
+    o->guess_ms = c.t_guess_ms;
+    o->iterations = c.iterations;
+    o->n_sigma = c.n_sigma;
+    o->n_sigma_fp64 = c.n_sigma_fp64;
+    o->n_ab = c.n_ab;
+    o->launches = g_launch_count;
+    return FCIB_OK;
+}
+
+int fcib_stream(fcib_ctx* ctx, void** stream) {
+    if (!ctx || !stream) { set_error("null argument"); return FCIB_ERR_ARG; }
+    *stream = (void*)ctx->c.stream;
     return FCIB_OK;
 }
 

@@ -341,7 +341,7 @@ struct Ops {
     }
     void fetch(int nslots) {
         k_final_reduce<<<nslots, 256, 0, c.stream>>>(partial.p, nblk, out.p);
-        FCIB_CUDA(cudaGetLastError());
+        FCIB_KCHECK();
         FCIB_CUDA(cudaMemcpyAsync(hout.data(), out.p, sizeof(double) * nslots, cudaMemcpyDeviceToHost, c.stream));
         FCIB_CUDA(cudaStreamSynchronize(c.stream));
     }
@@ -367,7 +367,7 @@ struct Ops {
             else if (nv <= 16) k_dots<16><<<nblk, kRedThreads, 0, c.stream>>>(a, N, partial.p);
             else if (nv <= 32) k_dots<32><<<nblk, kRedThreads, 0, c.stream>>>(a, N, partial.p);
             else k_dots<64><<<nblk, kRedThreads, 0, c.stream>>>(a, N, partial.p);
-            FCIB_CUDA(cudaGetLastError());
+            FCIB_KCHECK();
             fetch(kMaxIn + 1);
             for (int j = 0; j < nv; j++) d[done + j] = hout[j];
             if (a.self) *self = hout[kMaxIn];
@@ -419,7 +419,7 @@ struct Ops {
                     else if (nv <= 32) FCIB_COMBO(32, 4); else FCIB_COMBO(64, 4);
                 }
 #undef FCIB_COMBO
-                FCIB_CUDA(cudaGetLastError());
+                FCIB_KCHECK();
                 done += nv;
                 if (last) {
                     fetch(2 * nout);
@@ -431,7 +431,7 @@ struct Ops {
     }
     void scale(double* v, double a) {
         k_scale<<<nblk, kRedThreads, 0, c.stream>>>(v, a, N);
-        FCIB_CUDA(cudaGetLastError());
+        FCIB_KCHECK();
     }
     void copy(double* dst, const double* src) {
         FCIB_CUDA(cudaMemcpyAsync(dst, src, N * sizeof(double), cudaMemcpyDeviceToDevice, c.stream));
@@ -489,14 +489,14 @@ static void project_out(Context& c, std::vector<SparseDev>& bad, std::vector<dou
     for (int k = 0; k < nvec; k++)
         for (auto& b : bad) {
             k_project_sparse<<<1, 256, 0, c.stream>>>(V[k], b.idx.p, b.val.p, b.cnt);
-            FCIB_CUDA(cudaGetLastError());
+            FCIB_KCHECK();
         }
 }
 
 double spin2_device(Context& c, const double* C) {
     Ops ops(c);
     k_spin2<<<ops.nblk, kRedThreads, 0, c.stream>>>(C, c.A.str.p, c.B.str.p, (int)c.nas, (int)c.nbs, c.n, ops.partial.p);
-    FCIB_CUDA(cudaGetLastError());
+    FCIB_KCHECK();
     ops.fetch(1);
     double s = ops.hout[0];
     double na = c.na, nb = c.nb;
@@ -516,7 +516,7 @@ static std::vector<std::pair<double, int64_t>> lowest_diagonal(Context& c, int c
     for (int shift = 56; shift >= 0; shift -= 8) {
         FCIB_CUDA(cudaMemsetAsync(hist.p, 0, 256 * sizeof(unsigned int), c.stream));
         k_radix_hist<<<grid, 256, 0, c.stream>>>(c.hdiag.p, mask, N, prefix, pmask, shift, hist.p);
-        FCIB_CUDA(cudaGetLastError());
+        FCIB_KCHECK();
         unsigned int h[256];
         FCIB_CUDA(cudaMemcpyAsync(h, hist.p, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
         FCIB_CUDA(cudaStreamSynchronize(c.stream));
@@ -540,7 +540,7 @@ static std::vector<std::pair<double, int64_t>> lowest_diagonal(Context& c, int c
     ei.alloc(cap);
     FCIB_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(int), c.stream));
     k_collect_le<<<grid, 256, 0, c.stream>>>(c.hdiag.p, mask, N, prefix, cap, cnt.p, ev.p, ei.p);
-    FCIB_CUDA(cudaGetLastError());
+    FCIB_KCHECK();
     int hc = 0;
     FCIB_CUDA(cudaMemcpyAsync(&hc, cnt.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
     FCIB_CUDA(cudaStreamSynchronize(c.stream));
@@ -606,6 +606,10 @@ void dl_solve(Context& c) {
     c.t_sigma_ms = 0.0;
     c.n_sigma = 0;
     c.n_sigma_fp64 = 0;
+    c.t_ab_ms = c.t_same_ms = 0.0;
+    c.n_ab = 0;
+    c.t_ab64_ms = c.t_same64_ms = 0.0;
+    c.n_ab64 = 0;
     c.trace.clear();
 
     // ---- initial guess ----
@@ -653,7 +657,7 @@ void dl_solve(Context& c) {
         sd.idx.upload(ix, c.stream);
         sd.val.upload(vv, c.stream);
         k_fill_sparse<<<((int)ix.size() + 255) / 256, 256, 0, c.stream>>>(tmp[g], sd.idx.p, sd.val.p, (int)ix.size());
-        FCIB_CUDA(cudaGetLastError());
+        FCIB_KCHECK();
         FCIB_CUDA(cudaStreamSynchronize(c.stream));
     }
     if (gr.perturb) {
@@ -663,7 +667,7 @@ void dl_solve(Context& c) {
         for (int k = 0; k < nguess; k++) {
             k_add_random<<<ops.nblk, kRedThreads, 0, c.stream>>>(tmp[k], N, 0x9E3779B97F4A7C15ull * (k + 1),
                                                                  1.0e-3 * std::sqrt(3.0 / (double)N));
-            FCIB_CUDA(cudaGetLastError());
+            FCIB_KCHECK();
             apply_mask(c, tmp[k]);
         }
     }
@@ -840,7 +844,7 @@ void dl_solve(Context& c) {
             for (int k = 0; k < missing; k++) {
                 FCIB_CUDA(cudaMemsetAsync(tmp[m - 1], 0, sizeof(double) * N, c.stream));
                 k_add_random<<<ops.nblk, kRedThreads, 0, c.stream>>>(tmp[m - 1], N, 0xD1B54A32D192ED03ull + rng(), 1.0);
-                FCIB_CUDA(cudaGetLastError());
+                FCIB_KCHECK();
                 apply_mask(c, tmp[m - 1]);
                 std::vector<double*> one{tmp[m - 1]};
                 project_out(c, bad, one, 1);

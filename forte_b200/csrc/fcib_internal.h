@@ -29,6 +29,14 @@ void set_error(const std::string& msg);
             throw fcib::Error{FCIB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)}; \
     } while (0)
 
+// counts this engine's kernel launches (reported by fcib_profile) and checks the launch
+extern unsigned long long g_launch_count;
+#define FCIB_KCHECK()                           \
+    do {                                        \
+        ++fcib::g_launch_count;                 \
+        FCIB_CUDA(cudaGetLastError());          \
+    } while (0)
+
 #define FCIB_CHECK(cond, code, msg)                   \
     do {                                              \
         if (!(cond)) throw fcib::Error{(code), (msg)}; \
@@ -151,6 +159,10 @@ struct Context {
     double t_total_ms = 0.0;
     int n_sigma_fp64 = 0;
     double t_guess_ms = 0.0;
+    double t_ab_ms = 0.0, t_same_ms = 0.0;  // tensor-core opposite-spin / same-spin kernels (mixed sigma)
+    int n_ab = 0;
+    double t_ab64_ms = 0.0, t_same64_ms = 0.0;  // the same for FP64 sigma builds
+    int n_ab64 = 0;
     int guess_dets = 0;
     bool converged = false;
     std::vector<std::array<double, 5>> trace;  // iteration, ms, lambda_0, max residual, fp64 basis

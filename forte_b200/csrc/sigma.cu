@@ -310,7 +310,7 @@ static void launch_group_t(Context& c, const double* C, double* S, int ncols, in
     if (!c.counter.p) c.counter.alloc(16);
     FCIB_CUDA(cudaMemsetAsync(c.counter.p + 2, 0, sizeof(int), c.stream));
     k_group<T><<<grid, threads, smem, c.stream>>>(C, S, ncols, rows, labs, G, Gp, M, ldm, ngroups, nchunks, c.counter.p + 2, m_in_smem);
-    FCIB_CUDA(cudaGetLastError());
+    FCIB_KCHECK();
 }
 
 static void launch_group(Context& c, const double* C, double* S, int ncols, int ngroups, int G,
@@ -368,19 +368,19 @@ __global__ void k_apply_mask(double* __restrict__ v, const uint8_t* __restrict__
 static void transpose(Context& c, const double* in, double* out, int rows, int cols) {
     dim3 grid((cols + 31) / 32, (rows + 31) / 32), block(32, 8);
     k_transpose<<<grid, block, 0, c.stream>>>(in, out, rows, cols);
-    FCIB_CUDA(cudaGetLastError());
+    FCIB_KCHECK();
 }
 // out[rows][cols] += transpose(in[cols][rows])
 static void transpose_add(Context& c, const double* in, double* out, int rows, int cols) {
     dim3 grid((rows + 31) / 32, (cols + 31) / 32), block(32, 8);
     k_transpose_add<<<grid, block, 0, c.stream>>>(in, out, rows, cols);
-    FCIB_CUDA(cudaGetLastError());
+    FCIB_KCHECK();
 }
 
 void apply_mask(Context& c, double* v) {
     if (c.nirrep <= 1 || !c.mask.p) return;
     k_apply_mask<<<4 * c.num_sms, 256, 0, c.stream>>>(v, c.mask.p, (size_t)c.ndet);
-    FCIB_CUDA(cudaGetLastError());
+    FCIB_KCHECK();
 }
 
 // ------------------------------------------------------------------------------------------
@@ -406,10 +406,34 @@ static void sigma_same_spin(Context& c, const double* C, double* S, bool fp32) {
     }
 }
 
+// events bracketing the opposite-spin and same-spin parts of a sigma build
+struct SigmaEvents {
+    cudaEvent_t e[3];
+    SigmaEvents() { for (auto& x : e) cudaEventCreate(&x); }
+    ~SigmaEvents() { for (auto& x : e) cudaEventDestroy(x); }
+};
+static void sigma_timing(Context& c, SigmaEvents& ev, bool fp64) {
+    FCIB_CUDA(cudaEventSynchronize(ev.e[2]));
+    float a = 0.f, b = 0.f;
+    cudaEventElapsedTime(&a, ev.e[0], ev.e[1]);
+    cudaEventElapsedTime(&b, ev.e[1], ev.e[2]);
+    if (fp64) {
+        c.t_ab64_ms += a;
+        c.t_same64_ms += b;
+        c.n_ab64++;
+    } else {
+        c.t_ab_ms += a;
+        c.t_same_ms += b;
+        c.n_ab++;
+    }
+}
+
 void sigma_fp64(Context& c, const double* C, double* S) {
     const int nas = (int)c.nas, nbs = (int)c.nbs;
     const size_t N = (size_t)c.ndet;
     if (!c.counter.p) c.counter.alloc(16);
+    SigmaEvents ev;
+    FCIB_CUDA(cudaEventRecord(ev.e[0], c.stream));
     if (c.fold_h) {
         const int s1a = c.A.s1, npp = c.A.npair_pad;
         size_t smem = ab_fp64_smem(nbs, s1a, npp);
@@ -425,12 +449,15 @@ void sigma_fp64(Context& c, const double* C, double* S) {
         FCIB_CUDA(cudaMemsetAsync(c.counter.p, 0, sizeof(int), c.stream));
         k_ab_fp64<<<grid, threads, smem, c.stream>>>(C, S, c.A.conn.p, s1a, c.B.tgt.p, npp, c.V.p,
                                                      nas, nbs, c.scalar, c.counter.p);
-        FCIB_CUDA(cudaGetLastError());
+        FCIB_KCHECK();
     } else {
         k_scale_copy<<<4 * c.num_sms, 256, 0, c.stream>>>(C, S, c.scalar, N);
-        FCIB_CUDA(cudaGetLastError());
+        FCIB_KCHECK();
     }
+    FCIB_CUDA(cudaEventRecord(ev.e[1], c.stream));
     sigma_same_spin(c, C, S, false);
+    FCIB_CUDA(cudaEventRecord(ev.e[2], c.stream));
+    sigma_timing(c, ev, true);
     apply_mask(c, S);
 }
 
@@ -439,13 +466,18 @@ int tc_check_error(Context& c);
 
 void sigma_mixed(Context& c, const double* C, double* S, bool three) {
     const size_t N = (size_t)c.ndet;
+    SigmaEvents ev;
+    FCIB_CUDA(cudaEventRecord(ev.e[0], c.stream));
     if (c.fold_h) {
         ab_tc(c, C, S, three);
     } else {
         k_scale_copy<<<4 * c.num_sms, 256, 0, c.stream>>>(C, S, c.scalar, N);
-        FCIB_CUDA(cudaGetLastError());
+        FCIB_KCHECK();
     }
+    FCIB_CUDA(cudaEventRecord(ev.e[1], c.stream));
     sigma_same_spin(c, C, S, true);
+    FCIB_CUDA(cudaEventRecord(ev.e[2], c.stream));
+    sigma_timing(c, ev, false);
     apply_mask(c, S);
     if (c.fold_h) {
         int e = tc_check_error(c);
@@ -520,7 +552,7 @@ void compute_hdiag(Context& c, double* out) {
     FCIB_CUDA(cudaMemcpyToSymbolAsync(d_diag, &d, sizeof(d), 0, cudaMemcpyHostToDevice, c.stream));
     k_hdiag<<<8 * c.num_sms, 256, 0, c.stream>>>(c.A.str.p, c.B.str.p, (int)c.nas, (int)c.nbs, n,
                                                 c.scalar, out, (size_t)c.ndet);
-    FCIB_CUDA(cudaGetLastError());
+    FCIB_KCHECK();
 }
 
 }  // namespace fcib

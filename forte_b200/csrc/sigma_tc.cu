@@ -415,7 +415,7 @@ void ab_tc(Context& c, const double* C, double* S, bool three) {
     if (!c.tgtR16.p) {
         c.tgtR16.alloc((size_t)L.npad * nbs);
         k_tgt_rows16<<<4 * c.num_sms, 256, 0, c.stream>>>(c.B.tgt.p, c.tgtR16.p, nbs, c.B.npair_pad, L.npad);
-        FCIB_CUDA(cudaGetLastError());
+        FCIB_KCHECK();
     }
     if (c.vmax <= 0.0f) {
         std::vector<double> hv(c.V.n);
@@ -432,14 +432,14 @@ void ab_tc(Context& c, const double* C, double* S, bool three) {
     unsigned int* cmax_bits = reinterpret_cast<unsigned int*>(c.counter.p + 3);
     FCIB_CUDA(cudaMemsetAsync(cmax_bits, 0, sizeof(unsigned int), c.stream));
     k_split_tf32<<<8 * c.num_sms, 256, 0, c.stream>>>(C, c.tf_hi.p, three ? c.tf_lo.p : nullptr, nas, nbs, ldp, cmax_bits);
-    FCIB_CUDA(cudaGetLastError());
+    FCIB_KCHECK();
     auto kern = three ? k_ab_tc<true> : k_ab_tc<false>;
     FCIB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int grid = std::min(nas, c.num_sms);
     kern<<<grid, kTcThreads, smem, c.stream>>>(c.tf_hi.p, three ? c.tf_lo.p : c.tf_hi.p, ldp, C, S, c.A.conn.p, s1a,
                                               c.tgtR16.p, npair, c.V.p, c.A.npair_pad, c.vmax, cmax_bits, nas, nbs,
                                               c.scalar, c.counter.p, c.counter.p + 1);
-    FCIB_CUDA(cudaGetLastError());
+    FCIB_KCHECK();
 }
 
 int tc_check_error(Context& c) {

@@ -198,15 +198,15 @@ void build_spin_tables(SpinTables& t, int n, int k, bool need_g1, cudaStream_t s
     t.npair_pad = (t.npair + 7) / 8 * 8;
     t.str.alloc(t.nstr);
     k_unrank<<<(t.nstr + 255) / 256, 256, 0, s>>>(t.str.p, t.nstr, n, k);
-    FCIB_CUDA(cudaGetLastError());
+    FCIB_KCHECK();
     if (t.s1 > 0) {
         t.conn.alloc((size_t)t.nstr * t.s1);
         k_conn<<<(t.nstr + 127) / 128, 128, 0, s>>>(t.str.p, t.conn.p, t.nstr, n, t.s1);
-        FCIB_CUDA(cudaGetLastError());
+        FCIB_KCHECK();
     }
     t.tgt.alloc((size_t)t.nstr * t.npair_pad);
     k_tgt<<<t.nstr, 128, 0, s>>>(t.str.p, t.tgt.p, t.nstr, n, t.npair_pad);
-    FCIB_CUDA(cudaGetLastError());
+    FCIB_KCHECK();
     t.ng2 = t.g2 = 0;
     if (k >= 2) {
         t.ng2 = (int)B.c[n][k - 2];
@@ -214,7 +214,7 @@ void build_spin_tables(SpinTables& t, int n, int k, bool need_g1, cudaStream_t s
         t.g2row.alloc((size_t)t.ng2 * t.g2);
         t.g2lab.alloc((size_t)t.ng2 * t.g2);
         k_groups<<<(t.ng2 + 127) / 128, 128, 0, s>>>(t.g2row.p, t.g2lab.p, t.ng2, t.g2, n, k, 2);
-        FCIB_CUDA(cudaGetLastError());
+        FCIB_KCHECK();
     }
     t.ng1 = t.g1 = 0;
     if (need_g1 && k >= 1) {
@@ -223,7 +223,7 @@ void build_spin_tables(SpinTables& t, int n, int k, bool need_g1, cudaStream_t s
         t.g1row.alloc((size_t)t.ng1 * t.g1);
         t.g1lab.alloc((size_t)t.ng1 * t.g1);
         k_groups<<<(t.ng1 + 127) / 128, 128, 0, s>>>(t.g1row.p, t.g1lab.p, t.ng1, t.g1, n, k, 1);
-        FCIB_CUDA(cudaGetLastError());
+        FCIB_KCHECK();
     }
 }
 
@@ -347,7 +347,7 @@ void export_list(int n, int k, int kind, int p, int q, int r, int s, std::vector
         DBuf<int8_t> ds; DBuf<uint32_t> dI, dJ;
         ds.alloc(len); dI.alloc(len); dJ.alloc(len);
         launch(ds.p, dI.p, dJ.p);
-        FCIB_CUDA(cudaGetLastError());
+        FCIB_KCHECK();
         sign.resize(len); I.resize(len); J.resize(len);
         FCIB_CUDA(cudaMemcpyAsync(sign.data(), ds.p, len, cudaMemcpyDeviceToHost, st));
         FCIB_CUDA(cudaMemcpyAsync(I.data(), dI.p, 4 * len, cudaMemcpyDeviceToHost, st));
@@ -385,7 +385,7 @@ void export_list(int n, int k, int kind, int p, int q, int r, int s, std::vector
         DBuf<int8_t> ds; DBuf<uint32_t> dI, dJ;
         ds.alloc(npat); dI.alloc(npat); dJ.alloc(npat);
         k_vvoo_list<<<(npat + 127) / 128, 128, 0, st>>>(n, k, p, q, r, s, npat, cnt.p, pat.p, ds.p, dI.p, dJ.p);
-        FCIB_CUDA(cudaGetLastError());
+        FCIB_KCHECK();
         int len = 0;
         FCIB_CUDA(cudaMemcpyAsync(&len, cnt.p, sizeof(int), cudaMemcpyDeviceToHost, st));
         FCIB_CUDA(cudaStreamSynchronize(st));

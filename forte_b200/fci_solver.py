@@ -205,6 +205,16 @@ class FCISolver:
         capi.check(capi.lib().fcib_spin2(self._h, capi.dptr(c), C.byref(s)))
         return s.value
 
+    def profile(self) -> dict:
+        p = capi.FcibProfile()
+        capi.check(capi.lib().fcib_get_profile(self._h, C.byref(p)))
+        return {k: getattr(p, k) for k, _ in capi.FcibProfile._fields_}
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        capi.check(capi.lib().fcib_stream(self._h, C.byref(s)))
+        return s.value or 0
+
     def timing(self):
         sm = C.c_double()
         ns = C.c_int()

@@ -125,6 +125,26 @@ int fcib_string_list(fcib_ctx* ctx, int spin, int kind, int p, int q, int r, int
 /* timing of the last solve: total sigma milliseconds and number of sigma builds */
 int fcib_last_timing(fcib_ctx* ctx, double* sigma_ms, int* n_sigma, double* total_ms);
 
+/* Device-timed breakdown of the last solve (CUDA events on the engine's stream). */
+typedef struct fcib_profile {
+    double total_ms;        /* whole Davidson-Liu solve */
+    double sigma_ms;        /* all sigma builds */
+    double ab_ms;           /* tensor-core opposite-spin kernel inside mixed sigma builds */
+    double same_ms;         /* same-spin kernels inside mixed sigma builds */
+    double ab64_ms;         /* FP64 opposite-spin kernel inside FP64 sigma builds */
+    double same64_ms;       /* same-spin kernels inside FP64 sigma builds */
+    double guess_ms;        /* initial guess (host wall time) */
+    int iterations;
+    int n_sigma;            /* sigma builds */
+    int n_sigma_fp64;       /* of which in FP64 */
+    int n_ab;               /* launches timed in ab_ms */
+    int n_ab64;             /* launches timed in ab64_ms */
+    unsigned long long launches; /* kernel launches of this library since it was loaded */
+} fcib_profile;
+int fcib_get_profile(fcib_ctx* ctx, fcib_profile* out);
+/* the CUDA stream (cudaStream_t as void*) the engine launches on */
+int fcib_stream(fcib_ctx* ctx, void** stream);
+
 #ifdef __cplusplus
 }
 #endif
