@@ -90,6 +90,7 @@ SIGNATURES = {
     "fcib_last_timing": (C.c_int, [_vp, _dp, C.POINTER(C.c_int), _dp]),
     "fcib_get_profile": (C.c_int, [_vp, C.POINTER(FcibProfile)]),
     "fcib_stream": (C.c_int, [_vp, C.POINTER(C.c_void_p)]),
+    "fcib_spin2_device_noalloc": (C.c_int, [_vp, C.c_void_p, _dp, C.c_void_p]),
 }
 
 

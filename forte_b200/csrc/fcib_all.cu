@@ -5,3 +5,4 @@
 #include "sigma_tc.cu"
 #include "davidson.cu"
 #include "capi.cu"
+#include "noalloc.cu"

@@ -1,0 +1,71 @@
+// fcib_spin2_device_noalloc: <S^2> of a device vector with no allocation of any kind.
+//
+// The same k_spin2 / k_final_reduce kernels and the same grid as fcib_spin2, but the per-block
+// partial sums and the reduced result live in a file-scope device array instead of buffers
+// allocated per call.  The array's address is taken once per device with cudaGetSymbolAddress.
+//
+// Scratch limits: kNoAllocMaxBlocks partial-sum blocks of kSlots doubles plus one result row,
+// (1024 + 1) * 73 * 8 B = 598,600 B per device.  The grid is min(4 * SMs, ceil(ndet / 256)), so a
+// launch that would need more than kNoAllocMaxBlocks blocks is rejected with FCIB_ERR_UNSUPPORTED.
+// Every partial slot read by k_final_reduce is written by k_spin2 first in the same call, so
+// nothing in the scratch has to start at zero.
+//
+// The scratch is shared by every context on a device: calls that overlap in time (concurrent
+// host threads, or work still in flight on another stream) race on it; callers serialise them.
+#include <mutex>
+
+#include "fcib_internal.h"
+
+namespace fcib {
+
+constexpr int kNoAllocMaxBlocks = 1024;
+constexpr int kNoAllocMaxDevices = 64;
+constexpr size_t kNoAllocDoubles = (size_t)(kNoAllocMaxBlocks + 1) * kSlots;
+
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
+
+static double* noalloc_scratch(int device) {
+    static std::mutex mu;
+    static double* addr[kNoAllocMaxDevices] = {};
+    FCIB_CHECK(device >= 0 && device < kNoAllocMaxDevices, FCIB_ERR_UNSUPPORTED,
+               "fcib_spin2_device_noalloc: device ordinal above the scratch table size (64)");
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[device]) {
+        int cur = -1;
+        FCIB_CUDA(cudaGetDevice(&cur));
+        FCIB_CHECK(cur == device, FCIB_ERR_STATE, "fcib_spin2_device_noalloc: context device is not current");
+        void* p = nullptr;
+        FCIB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        addr[device] = static_cast<double*>(p);
+    }
+    return addr[device];
+}
+
+}  // namespace fcib
+
+extern "C" int fcib_spin2_device_noalloc(fcib_ctx* ctx, const double* d_c, double* s2, void* stream) {
+    if (!ctx || !d_c || !s2) { set_error("null argument"); return FCIB_ERR_ARG; }
+    return guarded(ctx, [&] {
+        Context& c = ctx->c;
+        FCIB_CHECK(c.has_ints && c.has_state && c.tables_ready, FCIB_ERR_STATE,
+                   "fcib_spin2_device_noalloc: string tables not built (call fcib_size, fcib_solve or "
+                   "fcib_spin2 on this context first)");
+        const size_t N = (size_t)c.ndet;
+        const int nblk = std::max(1, std::min(4 * c.num_sms, (int)((N + kRedThreads - 1) / kRedThreads)));
+        FCIB_CHECK(nblk <= kNoAllocMaxBlocks, FCIB_ERR_UNSUPPORTED,
+                   "fcib_spin2_device_noalloc: launch needs more partial-sum blocks than the static "
+                   "scratch holds (1024)");
+        double* partial = noalloc_scratch(c.device);
+        double* out = partial + (size_t)kNoAllocMaxBlocks * kSlots;
+        cudaStream_t st = stream ? (cudaStream_t)stream : c.stream;
+        k_spin2<<<nblk, kRedThreads, 0, st>>>(d_c, c.A.str.p, c.B.str.p, (int)c.nas, (int)c.nbs, c.n, partial);
+        FCIB_KCHECK();
+        k_final_reduce<<<1, 256, 0, st>>>(partial, nblk, out);
+        FCIB_KCHECK();
+        double s = 0.0;
+        FCIB_CUDA(cudaMemcpyAsync(&s, out, sizeof(double), cudaMemcpyDeviceToHost, st));
+        FCIB_CUDA(cudaStreamSynchronize(st));
+        const double na = c.na, nb = c.nb;
+        *s2 = -s + 0.25 * (na - nb) * (na - nb) + 0.5 * (na + nb);
+    });
+}
