@@ -12,6 +12,7 @@ engine's stream.  The CI vectors (1.3 GB each) are far larger than L2, so no flu
 One FP64 solve of the same problem gives the reference energy (|dE| check) and the FP64 time.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+  python bench.py --mode sigma --n 15 [--precision MIXED|MIXED_TF32|FP64]   (sigma builds/s)
 
 N > 1 runs independent replicas (the solve does not shard across GPUs), one per rank.
 """
@@ -191,6 +192,76 @@ def run_reference(args, world, rank):
     _ = barrier_free
 
 
+def run_sigma(args, world, rank, local):
+    """Sigma builds per second at CAS(n,n) (Ms = 0, C1) on device vectors, through fcib_sigma_device."""
+    import ctypes as C
+    import torch
+    from forte_b200 import FCISolver, StateInfo, build, capi, synthetic
+    build.build()
+    torch.cuda.set_device(local)
+    n, k = args.n, args.n // 2
+    ints = synthetic(n, 3 * n, SEED, gap=GAP)
+    s = FCISolver(StateInfo(k, k, 0), 1, ints, device=local)
+    N = s.size()
+    g = torch.Generator(device="cuda").manual_seed(0)
+    b = torch.randn(N, dtype=torch.float64, device="cuda", generator=g)
+    b /= b.norm()
+    out = torch.empty_like(b)
+    torch.cuda.synchronize()
+    prec = {"FP64": capi.PREC_FP64, "MIXED": capi.PREC_MIXED, "MIXED_TF32": capi.PREC_MIXED_TF32}[args.precision]
+    L = capi.lib()
+    stream = torch.cuda.ExternalStream(s.stream())
+
+    def one():
+        capi.check(L.fcib_sigma_device(s._h, C.c_void_p(b.data_ptr()), C.c_void_p(out.data_ptr()), prec, None))
+
+    for _ in range(args.warmup):
+        one()
+    barrier(world)
+    torch.cuda.synchronize()
+    p0 = s.profile()
+    st = torch.cuda.Event(enable_timing=True)
+    en = torch.cuda.Event(enable_timing=True)
+    st.record(stream)
+    for _ in range(args.steps):
+        one()
+    en.record(stream)
+    en.synchronize()
+    p1 = s.profile()
+    sec = allmax(world, st.elapsed_time(en) / 1e3)
+    launches = p1["launches"] - p0["launches"]
+    npair = n * (n + 1) // 2
+    s1 = k * (n - k) + k
+    flops = 2.0 * N * s1 * npair
+    hbm, bf16, bf16s, peak_kind = peaks()
+    roofline = None
+    if prec != capi.PREC_FP64:
+        tc_ms = (p1["tc_kernel_ms"] - p0["tc_kernel_ms"]) / args.steps
+        ach = flops / (tc_ms * 1e-3) / 1e12
+        roofline = {"bound": "tensor", "kernel": "k_ab_tc<3xTF32>" if prec == capi.PREC_MIXED else "k_ab_tc<TF32>",
+                    "achieved": ach, "peak": bf16, "unit": "TFLOP/s", "frac": ach / bf16,
+                    "peak_kind": f"bf16 burst ({peak_kind}); the TF32 tensor rate is half of bf16",
+                    "frac_vs_tf32": 2 * ach / bf16, "flops_per_launch": flops, "launch_ms": tc_ms,
+                    "traffic": None}
+    if rank == 0:
+        print(json.dumps({
+            "metric": f"sigma builds/s @CAS({n},{n})", "value": world * args.steps / sec, "unit": "sigma/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": {"FP64": "f64", "MIXED": "tf32x3/f32", "MIXED_TF32": "tf32/f32"}[args.precision],
+            "data": "synthetic",
+            "config": {"workload": f"sigma of a random unit vector, CAS({n},{n}) synthetic L={3 * n} Ms=0",
+                       "n_det": N, "precision": args.precision,
+                       "l2": f"vectors of {N * 8 / 1e9:.2f} GB" + (" (> L2)" if N * 8 > 126e6 else " (fit in L2)")},
+            "roofline": roofline, "gpu_launches": int(launches / args.steps),
+            "sigma_profile_ms": {"opposite_spin": ((p1["ab_ms"] - p0["ab_ms"]) + (p1["ab64_ms"] - p0["ab64_ms"])) / args.steps,
+                                 "same_spin": ((p1["same_ms"] - p0["same_ms"]) + (p1["same64_ms"] - p0["same64_ms"])) / args.steps},
+        }), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -202,10 +273,16 @@ def main():
     ap.add_argument("--ref-iterations", type=int, default=53, help="FP64 iteration count used by the CPU arm")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparator solve")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--mode", default="solve", choices=["solve", "sigma"],
+                    help="solve: the Davidson time-to-solution metric; sigma: sigma builds/s at CAS(n,n)")
+    ap.add_argument("--n", type=int, default=16, help="active orbitals of the sigma mode")
     args = ap.parse_args()
     world, rank, local = dist_init(args)
     if args.impl == "reference":
         run_reference(args, world, rank)
+        return
+    if args.mode == "sigma":
+        run_sigma(args, world, rank, local)
         return
 
     import torch
@@ -264,7 +341,7 @@ def main():
     s1 = k * (n - k) + k
     ndet = (len(s.strings(0))) * (len(s.strings(1)))
     flops_per_launch = 2.0 * ndet * s1 * npair  # one TF32 pass of the connected-pair contraction
-    ab_ms = sum(p["ab_ms"] for p in profs) / max(1, sum(p["n_ab"] for p in profs))
+    ab_ms = sum(p["tc_kernel_ms"] for p in profs) / max(1, sum(p["n_ab"] for p in profs))
     achieved = flops_per_launch / (ab_ms * 1e-3) / 1e12 if ab_ms > 0 else None
     traffic = NCU_TRAFFIC_CAS15 * (ndet * s1) / NCU_UNITS_CAS15
     roofline = {"bound": "tensor", "kernel": "k_ab_tc<3xTF32>", "achieved": achieved, "peak": bf16s,

@@ -52,7 +52,7 @@ class FcibProfile(C.Structure):
         ("total_ms", C.c_double), ("sigma_ms", C.c_double), ("ab_ms", C.c_double), ("same_ms", C.c_double),
         ("ab64_ms", C.c_double), ("same64_ms", C.c_double),
         ("guess_ms", C.c_double), ("iterations", C.c_int), ("n_sigma", C.c_int), ("n_sigma_fp64", C.c_int),
-        ("n_ab", C.c_int), ("n_ab64", C.c_int), ("launches", C.c_ulonglong),
+        ("n_ab", C.c_int), ("n_ab64", C.c_int), ("launches", C.c_ulonglong), ("tc_kernel_ms", C.c_double),
     ]
 
 

@@ -440,6 +440,7 @@ int fcib_get_profile(fcib_ctx* ctx, fcib_profile* o) {
     o->n_sigma_fp64 = c.n_sigma_fp64;
     o->n_ab = c.n_ab;
     o->launches = g_launch_count;
+    o->tc_kernel_ms = c.t_tc_ms;
     return FCIB_OK;
 }
 

@@ -606,7 +606,7 @@ void dl_solve(Context& c) {
     c.t_sigma_ms = 0.0;
     c.n_sigma = 0;
     c.n_sigma_fp64 = 0;
-    c.t_ab_ms = c.t_same_ms = 0.0;
+    c.t_ab_ms = c.t_same_ms = c.t_tc_ms = 0.0;
     c.n_ab = 0;
     c.t_ab64_ms = c.t_same64_ms = 0.0;
     c.n_ab64 = 0;

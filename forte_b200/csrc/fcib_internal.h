@@ -110,6 +110,19 @@ struct SpinTables {
 };
 void build_spin_tables(SpinTables& t, int n, int k, bool need_g1, cudaStream_t s);
 
+// a pair of CUDA events owned by the context (created on first use)
+struct EventPair {
+    cudaEvent_t e[2] = {nullptr, nullptr};
+    void ensure() {
+        for (auto& x : e)
+            if (!x) cudaEventCreate(&x);
+    }
+    ~EventPair() {
+        for (auto& x : e)
+            if (x) cudaEventDestroy(x);
+    }
+};
+
 // ------------------------------------------------------------------------------------------
 // engine context
 // ------------------------------------------------------------------------------------------
@@ -163,6 +176,9 @@ struct Context {
     int n_ab = 0;
     double t_ab64_ms = 0.0, t_same64_ms = 0.0;  // the same for FP64 sigma builds
     int n_ab64 = 0;
+    EventPair tc_ev;      // brackets the last tensor-core contraction launch
+    bool tc_recorded = false;
+    double t_tc_ms = 0.0;  // tensor-core contraction kernel alone (mixed sigma)
     int guess_dets = 0;
     bool converged = false;
     std::vector<std::array<double, 5>> trace;  // iteration, ms, lambda_0, max residual, fp64 basis

@@ -425,6 +425,12 @@ static void sigma_timing(Context& c, SigmaEvents& ev, bool fp64) {
         c.t_ab_ms += a;
         c.t_same_ms += b;
         c.n_ab++;
+        if (c.tc_recorded) {
+            float t = 0.f;
+            cudaEventElapsedTime(&t, c.tc_ev.e[0], c.tc_ev.e[1]);
+            c.t_tc_ms += t;
+            c.tc_recorded = false;
+        }
     }
 }
 

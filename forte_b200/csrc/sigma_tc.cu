@@ -436,10 +436,14 @@ void ab_tc(Context& c, const double* C, double* S, bool three) {
     auto kern = three ? k_ab_tc<true> : k_ab_tc<false>;
     FCIB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int grid = std::min(nas, c.num_sms);
+    c.tc_ev.ensure();
+    FCIB_CUDA(cudaEventRecord(c.tc_ev.e[0], c.stream));
     kern<<<grid, kTcThreads, smem, c.stream>>>(c.tf_hi.p, three ? c.tf_lo.p : c.tf_hi.p, ldp, C, S, c.A.conn.p, s1a,
                                               c.tgtR16.p, npair, c.V.p, c.A.npair_pad, c.vmax, cmax_bits, nas, nbs,
                                               c.scalar, c.counter.p, c.counter.p + 1);
     FCIB_KCHECK();
+    FCIB_CUDA(cudaEventRecord(c.tc_ev.e[1], c.stream));
+    c.tc_recorded = true;
 }
 
 int tc_check_error(Context& c) {

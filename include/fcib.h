@@ -140,6 +140,7 @@ typedef struct fcib_profile {
     int n_ab;               /* launches timed in ab_ms */
     int n_ab64;             /* launches timed in ab64_ms */
     unsigned long long launches; /* kernel launches of this library since it was loaded */
+    double tc_kernel_ms;    /* tensor-core contraction kernel alone (part of ab_ms) */
 } fcib_profile;
 int fcib_get_profile(fcib_ctx* ctx, fcib_profile* out);
 /* the CUDA stream (cudaStream_t as void*) the engine launches on */
