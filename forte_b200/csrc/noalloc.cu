@@ -1,8 +1,17 @@
 // fcib_spin2_device_noalloc: <S^2> of a device vector with no allocation of any kind.
 //
+// For callers that cannot allocate device memory: a host program whose memory pool owns the
+// whole GPU (a framework caching allocator, a fixed arena sized at start-up), or a loop that
+// must not pay for cudaMalloc/cudaFree, which can synchronise the device and fail when memory
+// is fragmented.  fcib_spin2 allocates a copy of the vector and its reduction buffers on
+// every call; this entry point takes the vector already on the device and allocates nothing.
+//
 // The same k_spin2 / k_final_reduce kernels and the same grid as fcib_spin2, but the per-block
 // partial sums and the reduced result live in a file-scope device array instead of buffers
-// allocated per call.  The array's address is taken once per device with cudaGetSymbolAddress.
+// allocated per call.  Host code cannot use that array's name as a device address, so the
+// first call on each device, with that device current, takes the address with
+// cudaGetSymbolAddress (return code checked) and keeps it; later calls reuse it.  Make that
+// first call before any stream capture that might include the entry point.
 //
 // Scratch limits: kNoAllocMaxBlocks partial-sum blocks of kSlots doubles plus one result row,
 // (1024 + 1) * 73 * 8 B = 598,600 B per device.  The grid is min(4 * SMs, ceil(ndet / 256)), so a

@@ -146,13 +146,17 @@ int fcib_get_profile(fcib_ctx* ctx, fcib_profile* out);
 /* the CUDA stream (cudaStream_t as void*) the engine launches on */
 int fcib_stream(fcib_ctx* ctx, void** stream);
 
-/* <S^2> of a device vector in the engine's C1 layout, allocating nothing: no device or host
+/* <S^2> of a device vector in the engine's C1 layout, allocating nothing.  For callers that
+ * cannot call cudaMalloc: a host whose memory pool already owns the GPU, or a loop that must
+ * not pay for an allocation's device synchronisation or risk its failure.  No device or host
  * buffers are created; the reduction scratch is a static per-device array of 598,600 bytes
- * (1024 partial-sum blocks).  Same kernels and grid as fcib_spin2, so the value matches it
- * bit for bit.  The context's string tables must already exist (FCIB_ERR_STATE otherwise);
- * a launch needing more than 1024 blocks returns FCIB_ERR_UNSUPPORTED.  Calls on one device
- * must not overlap in time: they share the scratch.  stream: cudaStream_t as void*, NULL =
- * the context's stream; the call synchronizes it.  No reference counterpart. */
+ * (1024 partial-sum blocks) that every call shares.  Same kernels and grid as fcib_spin2, so
+ * the value matches it bit for bit.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress); make it before any stream capture.  The context's string
+ * tables must already exist (FCIB_ERR_STATE otherwise); a launch needing more than 1024
+ * blocks returns FCIB_ERR_UNSUPPORTED.  Calls on one device that overlap on the GPU race on
+ * the shared scratch: serialise them.  stream: cudaStream_t as void*, NULL = the context's
+ * stream; the call synchronizes it.  No counterpart in the reference. */
 int fcib_spin2_device_noalloc(fcib_ctx* ctx, const double* d_c, double* s2, void* stream);
 
 #ifdef __cplusplus

@@ -1,5 +1,8 @@
 """fcib_spin2_device_noalloc against fcib_spin2 (same kernels, static scratch instead of buffers).
 
+The no-alloc entry point serves callers that cannot allocate device memory (their own pool owns
+the GPU, or an allocation's device sync is not acceptable); its scratch is one static array per
+device that every call reuses, so two calls in a row must both match the allocating entry point.
 Collected last (file name) so it also runs after every other GPU test in the same process.
 """
 import ctypes as C
