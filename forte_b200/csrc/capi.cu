@@ -114,6 +114,36 @@ static void download_flat(Context& c, const double* dev, double* flat) {
     FCIB_CUDA(cudaStreamSynchronize(c.stream));
     for (size_t i = 0; i < c.block_to_c1.size(); i++) flat[i] = full[c.block_to_c1[i]];
 }
+// RDM blocks -> caller buffers; spin-free sums follow FCIVector::compute_rdms
+// (fci_vector_rdm.cc:120-126): G1 = g1a + g1b, G2 = (g2aa + (g2ab(pqrs) + g2ab(qpsr))) + g2bb.
+static void rdms_to_outputs(const RdmBlocks& b, int level, int spin_free, double* g1a, double* g1b, double* g2aa,
+                            double* g2ab, double* g2bb) {
+    const int n = b.n;
+    const size_t nn = (size_t)n * n, n4 = nn * nn;
+    if (!spin_free) {
+        if (g1a) std::copy(b.g1a.begin(), b.g1a.end(), g1a);
+        if (g1b) std::copy(b.g1b.begin(), b.g1b.end(), g1b);
+        if (level >= 2) {
+            if (g2aa) std::copy(b.g2aa.begin(), b.g2aa.end(), g2aa);
+            if (g2ab) std::copy(b.g2ab.begin(), b.g2ab.end(), g2ab);
+            if (g2bb) std::copy(b.g2bb.begin(), b.g2bb.end(), g2bb);
+        }
+        return;
+    }
+    if (g1a)
+        for (size_t i = 0; i < nn; i++) g1a[i] = b.g1a[i] + b.g1b[i];
+    if (level >= 2 && g2aa) {
+        for (int p = 0; p < n; p++)
+            for (int q = 0; q < n; q++)
+                for (int r = 0; r < n; r++)
+                    for (int s = 0; s < n; s++) {
+                        const size_t x = (((size_t)p * n + q) * n + r) * n + s;
+                        const size_t y = (((size_t)q * n + p) * n + s) * n + r;
+                        g2aa[x] = (b.g2aa[x] + (b.g2ab[x] + b.g2ab[y])) + b.g2bb[x];
+                    }
+    }
+    (void)n4;
+}
 static int64_t flat_size(const Context& c) {
     return c.nirrep <= 1 ? c.ndet : (int64_t)c.block_to_c1.size();
 }
@@ -365,11 +395,44 @@ int fcib_spin2(fcib_ctx* ctx, const double* cvec, double* s2) {
 
 int fcib_rdms(fcib_ctx* ctx, int root_left, int root_right, int level, int spin_free, double* g1a,
               double* g1b, double* g2aa, double* g2ab, double* g2bb) {
-    (void)root_left; (void)root_right; (void)level; (void)spin_free;
-    (void)g1a; (void)g1b; (void)g2aa; (void)g2ab; (void)g2bb;
     if (!ctx) { set_error("null context"); return FCIB_ERR_ARG; }
-    set_error("fcib_rdms: not available in this build");
-    return FCIB_ERR_UNSUPPORTED;
+    return guarded(ctx, [&] {
+        Context& c = ctx->c;
+        FCIB_CHECK(c.solved, FCIB_ERR_STATE, "FCIVector is not assigned. Cannot compute RDMs.");
+        FCIB_CHECK(root_left >= 0 && root_right >= 0, FCIB_ERR_ARG, "negative root index");
+        if (std::max(root_left, root_right) >= c.nroot)
+            throw Error{FCIB_ERR_ARG, "Cannot compute RDMs <" + std::to_string(root_left) + "| ... |" +
+                                          std::to_string(root_right) + "> (0-based) because nroot = " +
+                                          std::to_string(c.nroot)};
+        FCIB_CHECK(level <= 2, FCIB_ERR_UNSUPPORTED, "RDMs of order 3 or higher are not available in this engine");
+        if (level <= 0) return;
+        RdmBlocks blk;
+        compute_rdms(c, c.b.p + (size_t)root_left * c.ndet, c.b.p + (size_t)root_right * c.ndet, level, blk);
+        rdms_to_outputs(blk, level, spin_free, g1a, g1b, g2aa, g2ab, g2bb);
+    });
+}
+
+int fcib_compute_rdms(fcib_ctx* ctx, const double* left, const double* right, int level, int spin_free,
+                      double* g1a, double* g1b, double* g2aa, double* g2ab, double* g2bb) {
+    if (!ctx || !left) { set_error("null argument"); return FCIB_ERR_ARG; }
+    return guarded(ctx, [&] {
+        Context& c = ctx->c;
+        ensure_setup(c);
+        FCIB_CHECK(level <= 2, FCIB_ERR_UNSUPPORTED, "RDMs of order 3 or higher are not available in this engine");
+        if (level <= 0) return;
+        DBuf<double> dl, dr;
+        dl.alloc(c.ndet);
+        upload_flat(c, left, dl.p);
+        const double* R = dl.p;
+        if (right && right != left) {
+            dr.alloc(c.ndet);
+            upload_flat(c, right, dr.p);
+            R = dr.p;
+        }
+        RdmBlocks blk;
+        compute_rdms(c, dl.p, R, level, blk);
+        rdms_to_outputs(blk, level, spin_free, g1a, g1b, g2aa, g2ab, g2bb);
+    });
 }
 
 int fcib_num_strings(fcib_ctx* ctx, int spin, int64_t* count) {

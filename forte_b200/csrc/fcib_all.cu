@@ -4,5 +4,6 @@
 #include "sigma.cu"
 #include "sigma_tc.cu"
 #include "davidson.cu"
+#include "rdms.cu"
 #include "capi.cu"
 #include "noalloc.cu"

@@ -194,6 +194,12 @@ void export_list(int n, int k, int kind, int p, int q, int r, int s, std::vector
 void compute_hdiag(Context& c, double* out);
 void sigma_dispatch(Context& c, const double* b, double* s, int precision);
 void ensure_setup(Context& c);
+// rdms.cu: host copies of the RDM blocks (row-major, n^2 and n^4)
+struct RdmBlocks {
+    int n = 0;
+    std::vector<double> g1a, g1b, g2aa, g2ab, g2bb;
+};
+void compute_rdms(Context& c, const double* L, const double* R, int level, RdmBlocks& out);
 // davidson.cu
 void dl_solve(Context& c);
 double spin2_device(Context& c, const double* C);

@@ -223,26 +223,41 @@ class FCISolver:
         return {"sigma_ms": sm.value, "n_sigma": ns.value, "total_ms": tt.value}
 
     def rdms(self, root_list, max_rdm_level=2, rdm_type="spin_dependent"):
-        """FCISolver::rdms (forte/fci/fci_solver_rdms.cc:40-64)."""
+        """FCISolver::rdms (forte/fci/fci_solver_rdms.cc:40-104): one RDMs object per (left, right)
+        root pair of the last solve; max_rdm_level <= 0 gives empty objects."""
         if max_rdm_level > 2:
             raise RuntimeError("RDMs of order 3 or higher are not implemented in this engine")
-        n = self.ints.n
         out = []
-        sf = rdm_type in ("spin_free", 1)
         for (rl, rr) in root_list:
-            if rl >= self.nroot or rr >= self.nroot:
-                raise RuntimeError(f"FCISolver::rdms: root {max(rl, rr)} is larger than the number of "
-                                   f"computed roots ({self.nroot})")
-            g1a = np.zeros((n, n)); g1b = np.zeros((n, n))
-            g2aa = np.zeros((n,) * 4); g2ab = np.zeros((n,) * 4); g2bb = np.zeros((n,) * 4)
-            capi.check(capi.lib().fcib_rdms(self._h, rl, rr, max_rdm_level, 1 if sf else 0,
-                                            capi.dptr(g1a), capi.dptr(g1b), capi.dptr(g2aa),
-                                            capi.dptr(g2ab), capi.dptr(g2bb)))
-            if sf:
-                out.append(RDMs(True, g1=g1a, g2=g2aa if max_rdm_level > 1 else None))
-            else:
-                out.append(RDMs(False, g1a=g1a, g1b=g1b, g2aa=g2aa, g2ab=g2ab, g2bb=g2bb))
+            if max(rl, rr) >= self.nroot:
+                raise RuntimeError(f"Cannot compute RDMs <{rl}| ... |{rr}> (0-based) because nroot = {self.nroot}")
+            out.append(self._rdm_call(lambda *a, rl=rl, rr=rr: capi.lib().fcib_rdms(self._h, rl, rr, *a),
+                                      max_rdm_level, rdm_type))
         return out
+
+    def compute_rdms(self, left, right=None, max_rdm_level=2, rdm_type="spin_dependent"):
+        """FCIVector::compute_rdms (forte/fci/fci_vector_rdm.cc:43-145) between two vectors in
+        FCIVector flat order (right defaults to left)."""
+        if max_rdm_level > 2:
+            raise RuntimeError("RDMs of order 3 or higher are not implemented in this engine")
+        left = np.ascontiguousarray(left, dtype=np.float64)
+        right = left if right is None else np.ascontiguousarray(right, dtype=np.float64)
+        return self._rdm_call(lambda *a: capi.lib().fcib_compute_rdms(self._h, capi.dptr(left), capi.dptr(right), *a),
+                              max_rdm_level, rdm_type)
+
+    def _rdm_call(self, fn, level, rdm_type):
+        n = self.ints.n
+        sf = rdm_type in ("spin_free", 1)
+        if level <= 0:
+            return RDMs(sf)
+        g1a = np.zeros((n, n))
+        g1b = np.zeros((n, n))
+        g2 = [np.zeros((n,) * 4) for _ in range(3)] if level > 1 else [None] * 3
+        ptr = [capi.dptr(x) if x is not None else None for x in (g1a, g1b, *g2)]
+        capi.check(fn(level, 1 if sf else 0, *ptr))
+        if sf:
+            return RDMs(True, g1=g1a, g2=g2[0])
+        return RDMs(False, g1a=g1a, g1b=g1b, g2aa=g2[0], g2ab=g2[1], g2bb=g2[2])
 
     # ---- string tables (parity checks) ----------------------------------------------------
     def strings(self, spin):

@@ -113,6 +113,10 @@ int fcib_spin2(fcib_ctx* ctx, const double* c, double* s2);
  * spin_free = 1: g1a <- g1a + g1b and g2aa <- g2aa + g2ab + g2ab(qpsr) + g2bb. */
 int fcib_rdms(fcib_ctx* ctx, int root_left, int root_right, int level, int spin_free,
               double* g1a, double* g1b, double* g2aa, double* g2ab, double* g2bb);
+/* The same RDMs between two host vectors in FCIVector flat order (right == NULL: right = left);
+ * replaces FCIVector::compute_rdms(C_left, C_right, max_rdm_level, type) (fci_vector_rdm.cc:43-145). */
+int fcib_compute_rdms(fcib_ctx* ctx, const double* left, const double* right, int level, int spin_free,
+                      double* g1a, double* g1b, double* g2aa, double* g2ab, double* g2bb);
 
 /* String tables for parity checks.  spin 0 = alpha, 1 = beta. */
 int fcib_num_strings(fcib_ctx* ctx, int spin, int64_t* count);
