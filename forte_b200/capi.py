@@ -64,6 +64,8 @@ class FcibError(RuntimeError):
 
 #: exported symbols and their (restype, argtypes)
 _dp = C.POINTER(C.c_double)
+_fp = C.POINTER(C.c_float)
+_up = C.POINTER(C.c_uint32)
 _vp = C.c_void_p
 SIGNATURES = {
     "fcib_default_options": (None, [C.POINTER(FcibOptions)]),
@@ -92,7 +94,16 @@ SIGNATURES = {
     "fcib_get_profile": (C.c_int, [_vp, C.POINTER(FcibProfile)]),
     "fcib_stream": (C.c_int, [_vp, C.POINTER(C.c_void_p)]),
     "fcib_spin2_device_noalloc": (C.c_int, [_vp, C.c_void_p, _dp, C.c_void_p]),
+    "fcib_set_mlp": (C.c_int, [_vp, _fp, C.c_int]),
+    "fcib_mlp_eval": (C.c_int, [C.c_int, C.c_int64, _up, _up, _fp, _fp, _fp, _fp]),
+    "fcib_mlp_grad": (C.c_int, [C.c_int, C.c_int64, _up, _up, _fp, _fp, _fp, _fp, _fp, _fp, _dp]),
+    "fcib_mlp_train": (C.c_int, [C.c_int, C.c_int64, _up, _up, _fp, _fp, _fp, _fp, C.c_int, C.c_int, C.c_float,
+                                 C.c_uint64, C.c_int, _fp, _dp]),
+    "fcib_precondition": (C.c_int, [_vp, _dp, C.c_double, _dp]),
+    "fcib_set_residual_capture": (C.c_int, [_vp, C.c_int]),
+    "fcib_captured_residual": (C.c_int, [_vp, C.c_int, _dp, _dp, C.POINTER(C.c_int)]),
 }
+MLP_NWEIGHTS = 10689
 
 
 def lib():
@@ -117,6 +128,16 @@ def check(rc):
 
 def dptr(a: np.ndarray):
     return a.ctypes.data_as(_dp)
+
+
+def fptr(a: np.ndarray):
+    assert a.dtype == np.float32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_fp)
+
+
+def uptr(a: np.ndarray):
+    assert a.dtype == np.uint32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_up)
 
 
 def default_options() -> FcibOptions:

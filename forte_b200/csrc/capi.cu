@@ -435,6 +435,25 @@ int fcib_compute_rdms(fcib_ctx* ctx, const double* left, const double* right, in
     });
 }
 
+int fcib_set_residual_capture(fcib_ctx* ctx, int max_vectors) {
+    if (!ctx || max_vectors < 0) { set_error("bad argument"); return FCIB_ERR_ARG; }
+    ctx->c.capture_max = max_vectors;
+    ctx->c.cap_r.clear();
+    ctx->c.cap_lambda.clear();
+    return FCIB_OK;
+}
+
+int fcib_captured_residual(fcib_ctx* ctx, int index, double* r, double* lambda, int* count) {
+    if (!ctx) { set_error("null context"); return FCIB_ERR_ARG; }
+    const Context& c = ctx->c;
+    if (count) *count = (int)c.cap_r.size();
+    if (index < 0) return FCIB_OK;
+    if (index >= (int)c.cap_r.size()) { set_error("captured residual index out of range"); return FCIB_ERR_ARG; }
+    if (r) std::copy(c.cap_r[index].begin(), c.cap_r[index].end(), r);
+    if (lambda) *lambda = c.cap_lambda[index];
+    return FCIB_OK;
+}
+
 int fcib_num_strings(fcib_ctx* ctx, int spin, int64_t* count) {
     if (!ctx || !count) { set_error("null argument"); return FCIB_ERR_ARG; }
     return guarded(ctx, [&] {

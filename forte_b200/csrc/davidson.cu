@@ -766,6 +766,23 @@ void dl_solve(Context& c) {
                 rnorm[k] = std::sqrt(rc[k].first);
                 cnorm[k] = std::sqrt(rc[k].second);
             }
+            if (c.capture_max > (int)c.cap_r.size()) {
+                // raw residual of root 0 (training data of the learned preconditioner)
+                std::vector<std::vector<double>> c0(1, coef[0]);
+                ops.combo(V, c0, {tmp[0]}, 0.0);
+                std::vector<double> h(N);
+                FCIB_CUDA(cudaMemcpyAsync(h.data(), tmp[0], sizeof(double) * N, cudaMemcpyDeviceToHost, c.stream));
+                FCIB_CUDA(cudaStreamSynchronize(c.stream));
+                c.cap_r.push_back(std::move(h));
+                c.cap_lambda.push_back(lambda[0]);
+            }
+            if (o.preconditioner == FCIB_PRECOND_MLP) {
+                // learned per-determinant rescaling of the diagonal corrections
+                for (int k = 0; k < nroot; k++) {
+                    mlp_apply(c, r[k], lambda[k], rnorm[k]);
+                    cnorm[k] = std::sqrt(ops.norm2(r[k]));
+                }
+            }
         }
         // 4. project out undesired roots; normalisation is folded into Gram-Schmidt
         project_out(c, bad, r, nroot);

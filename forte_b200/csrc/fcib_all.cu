@@ -6,4 +6,5 @@
 #include "davidson.cu"
 #include "rdms.cu"
 #include "capi.cu"
+#include "mlp.cu"
 #include "noalloc.cu"

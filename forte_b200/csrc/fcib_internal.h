@@ -181,7 +181,13 @@ struct Context {
     double t_tc_ms = 0.0;  // tensor-core contraction kernel alone (mixed sigma)
     int guess_dets = 0;
     bool converged = false;
-    std::vector<std::array<double, 5>> trace;  // iteration, ms, lambda_0, max residual, fp64 basis
+    std::vector<std::array<double, 5>> trace;
+    // learned preconditioner weights (FP32 master copy, BF16-rounded at use)
+    DBuf<float> mlp_w;
+    // residual capture of root 0 during solves (training data of the learned preconditioner)
+    int capture_max = 0;
+    std::vector<std::vector<double>> cap_r;
+    std::vector<double> cap_lambda;  // iteration, ms, lambda_0, max residual, fp64 basis
 };
 
 // kernels / launchers (sigma.cu)
@@ -200,6 +206,8 @@ struct RdmBlocks {
     std::vector<double> g1a, g1b, g2aa, g2ab, g2bb;
 };
 void compute_rdms(Context& c, const double* L, const double* R, int level, RdmBlocks& out);
+// mlp.cu: learned preconditioner, in place on a diagonal correction t
+void mlp_apply(Context& c, double* t, double lambda, double rnorm);
 // davidson.cu
 void dl_solve(Context& c);
 double spin2_device(Context& c, const double* C);

@@ -117,6 +117,9 @@ class FCISolver:
                        "MIXED_TF32": capi.PREC_MIXED_TF32}[str(d["FCI_PRECISION"]).upper()]
         o.preconditioner = {"DIAG": capi.PRECOND_DIAG, "MLP": capi.PRECOND_MLP}[str(d["FCI_PRECONDITIONER"]).upper()]
         o.mixed_switch = float(d["FCI_MIXED_SWITCH"])
+        if o.preconditioner == capi.PRECOND_MLP and getattr(self, "_mlp", None) is None:
+            from .learned_precond import load_weights
+            self.set_mlp_weights(load_weights())
         capi.check(capi.lib().fcib_set_options(self._h, C.byref(o)))
 
     def set_options(self, options: dict):
@@ -145,6 +148,16 @@ class FCISolver:
 
     def set_print(self, v):
         self.set_options({"PRINT": v})
+
+    def set_mlp_weights(self, weights):
+        """Weights of the learned preconditioner (FCIB_MLP_NWEIGHTS floats); None unloads.  With
+        FCI_PRECONDITIONER = MLP and no weights set, the committed default weights are used."""
+        if weights is None:
+            self._mlp = None
+            capi.check(capi.lib().fcib_set_mlp(self._h, None, 0))
+            return
+        self._mlp = np.ascontiguousarray(weights, dtype=np.float32)
+        capi.check(capi.lib().fcib_set_mlp(self._h, capi.fptr(self._mlp), len(self._mlp)))
 
     def set_die_if_not_converged(self, v: bool):
         self._die = bool(v)

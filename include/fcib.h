@@ -118,6 +118,38 @@ int fcib_rdms(fcib_ctx* ctx, int root_left, int root_right, int level, int spin_
 int fcib_compute_rdms(fcib_ctx* ctx, const double* left, const double* right, int level, int spin_free,
                       double* g1a, double* g1b, double* g2aa, double* g2ab, double* g2bb);
 
+/* ---- learned preconditioner (no counterpart in the reference) ------------------------------
+ * With preconditioner = FCIB_PRECOND_MLP each diagonal correction t_I = r_I / (lambda - H_II)
+ * is rescaled by 1 + 0.25 tanh(m(x_I)), m a 35-64-64-64-1 ReLU network with BF16 weights; inputs
+ * are the alpha/beta excitation bits of determinant I in a 16-orbital window around the Fermi
+ * level, H_II - lambda and |r_I| / ||r||.  Weight vector (floats): W1[64][35], b1[64], W2[64][64],
+ * b2[64], W3[64][64], b3[64], w4[64], b4.  Samples for eval/grad/train: ea/eb = excitation
+ * window bits (16 each), u = H_II - lambda, r = r_I / ||r||, tgt = target correction element on
+ * the scale of -r/u, wgt = per-sample loss weight. */
+#define FCIB_MLP_NWEIGHTS 10689
+/* load weights into a context (NULL unloads) */
+int fcib_set_mlp(fcib_ctx* ctx, const float* weights, int nweights);
+/* inference kernel on samples: factor[i] = 1 + 0.25 tanh(m(x_i)) */
+int fcib_mlp_eval(int device, int64_t n, const uint32_t* ea, const uint32_t* eb, const float* u, const float* r,
+                  const float* weights, float* factor);
+/* loss = mean over samples of wgt (t (1 + 0.25 tanh m) - tgt)^2, t = -r/u (0 when |u| <= 1e-6), wgt
+ * NULL = 1, and its gradient */
+int fcib_mlp_grad(int device, int64_t n, const uint32_t* ea, const uint32_t* eb, const float* u, const float* r,
+                  const float* tgt, const float* wgt, const float* weights, float* grad, double* loss);
+/* Adam training on the GPU (init != 0: seeded Xavier init, zero output layer); weights in/out,
+ * epoch_loss[epochs] (may be NULL) = mean minibatch loss of each epoch */
+int fcib_mlp_train(int device, int64_t n, const uint32_t* ea, const uint32_t* eb, const float* u, const float* r,
+                   const float* tgt, const float* wgt, int epochs, int batch, float lr, uint64_t seed, int init,
+                   float* weights, double* epoch_loss);
+/* the correction-vector step of DavidsonLiuSolver (davidson_liu_solver.cc:432-448) with the
+ * context's preconditioner option: out = r / (lambda - H_II) (0 when |lambda - H_II| <= 1e-6),
+ * rescaled by the network when preconditioner = FCIB_PRECOND_MLP; host vectors in flat order */
+int fcib_precondition(fcib_ctx* ctx, const double* r, double lambda, double* out);
+/* keep the raw residual of root 0 (C1 layout) and its Ritz value at every Davidson iteration of
+ * later solves, up to max_vectors (0 = off); read them back by index (index < 0: count only) */
+int fcib_set_residual_capture(fcib_ctx* ctx, int max_vectors);
+int fcib_captured_residual(fcib_ctx* ctx, int index, double* r, double* lambda, int* count);
+
 /* String tables for parity checks.  spin 0 = alpha, 1 = beta. */
 int fcib_num_strings(fcib_ctx* ctx, int spin, int64_t* count);
 int fcib_strings(fcib_ctx* ctx, int spin, uint32_t* out);
