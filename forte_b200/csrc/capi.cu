@@ -67,6 +67,7 @@ void ensure_setup(Context& c) {
     FCIB_CHECK(c.has_ints, FCIB_ERR_STATE, "integrals have not been set");
     FCIB_CHECK(c.has_state, FCIB_ERR_STATE, "state has not been set");
     if (c.tables_ready) return;
+    c.mlp_tables_ready = false;
     FCIB_CHECK(c.na <= c.n && c.nb <= c.n, FCIB_ERR_ARG, "more electrons than orbitals");
     bool fold = (c.na >= 1 && c.nb >= 1);
     c.tgtR16.release();

@@ -779,7 +779,7 @@ void dl_solve(Context& c) {
             if (o.preconditioner == FCIB_PRECOND_MLP) {
                 // learned per-determinant rescaling of the diagonal corrections
                 for (int k = 0; k < nroot; k++) {
-                    mlp_apply(c, r[k], lambda[k], rnorm[k]);
+                    mlp_apply(c, r[k], lambda[k], rnorm[k], cnorm[k]);
                     cnorm[k] = std::sqrt(ops.norm2(r[k]));
                 }
             }

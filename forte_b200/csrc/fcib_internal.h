@@ -184,6 +184,8 @@ struct Context {
     std::vector<std::array<double, 5>> trace;
     // learned preconditioner weights (FP32 master copy, BF16-rounded at use)
     DBuf<float> mlp_w;
+    DBuf<float> mlp_tabA, mlp_tabB;  // per-string layer-1 sums of the loaded weights
+    bool mlp_tables_ready = false;
     // residual capture of root 0 during solves (training data of the learned preconditioner)
     int capture_max = 0;
     std::vector<std::vector<double>> cap_r;
@@ -207,7 +209,7 @@ struct RdmBlocks {
 };
 void compute_rdms(Context& c, const double* L, const double* R, int level, RdmBlocks& out);
 // mlp.cu: learned preconditioner, in place on a diagonal correction t
-void mlp_apply(Context& c, double* t, double lambda, double rnorm);
+void mlp_apply(Context& c, double* t, double lambda, double rnorm, double tnorm);
 // davidson.cu
 void dl_solve(Context& c);
 double spin2_device(Context& c, const double* C);

@@ -44,7 +44,10 @@ static_assert(kMlpNW == FCIB_MLP_NWEIGHTS, "weight layout");
 #define FCIB_MLP_RANGE 0.25f
 #endif
 constexpr float kMlpRange = FCIB_MLP_RANGE;  // factor = 1 + kMlpRange * tanh(m)
-constexpr int kW2Ld = 72;  // padded bf16 row stride of W2/W3 in shared memory (conflict-free B fragments)
+constexpr int kW2Ld = 72;
+// Tiles of 16 determinants whose diagonal corrections are all below kMlpSkip * ||t|| keep the
+// diagonal rule (their elements change the correction by less than 1e-4 ||t|| each).
+constexpr double kMlpSkip = 1.0e-4;  // padded bf16 row stride of W2/W3 in shared memory (conflict-free B fragments)
 
 __device__ __forceinline__ float bf16r(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
 
@@ -67,23 +70,50 @@ struct MlpDevice {
 };
 
 // ---- inference --------------------------------------------------------------------------
-struct EngineSource {  // determinant I of a C1 vector: correction t in place
+// Per-string layer-1 tables: tab[s][c] = sum over the excitation bits b of string s of
+// W1[c][off + b] (BF16-rounded weights), so that layer 1 of determinant (Ia, Ib) is
+// b1 + tabA[Ia] + tabB[Ib] + W1[:, 32..34] x[32..34].
+__global__ void k_mlp_tables(const uint32_t* __restrict__ str, int nstr, int k, int off, const float* __restrict__ w,
+                             float* __restrict__ tab) {
+    const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i >= (size_t)nstr * kMlpH) return;
+    const int s = (int)(i / kMlpH), c = (int)(i - (size_t)s * kMlpH);
+    float acc = 0.0f;
+    for (uint32_t e = excitation_window(str[s], k); e; e &= e - 1) acc += bf16r(w[kOffW1 + c * kMlpIn + off + __ffs(e) - 1]);
+    tab[i] = acc;
+}
+
+struct MlpSmem {
+    float w1[kMlpH][kMlpIn];
+    float b1[kMlpH], b2[kMlpH], b3[kMlpH], w4[kMlpH];
+    float b4;
+    __nv_bfloat16 w2[kMlpH * kW2Ld];
+    __nv_bfloat16 w3[kMlpH * kW2Ld];
+};
+
+struct EngineSource {  // determinant I of a C1 vector: diagonal correction t rescaled in place
     double* t;
     const double* hd;
-    const uint32_t* sa;
-    const uint32_t* sb;
-    long long nbs;
+    const float* tabA;  // [nas][64]
+    const float* tabB;  // [nbs][64]
+    unsigned nbs;
     double lambda;
     float inv_rnorm;
-    int na, nb;
-    __device__ void load(size_t I, uint32_t& ea, uint32_t& eb, float& u, float& rr, double& tv) const {
-        const size_t ia = I / (size_t)nbs, ib = I - ia * (size_t)nbs;
-        ea = excitation_window(sa[ia], na);
-        eb = excitation_window(sb[ib], nb);
+    float skip;  // tiles whose |t_I| are all below this keep the diagonal rule
+    __device__ bool load(size_t I, uint32_t& a, uint32_t& b, float& u, float& rr, double& tv) const {
+        const unsigned Iu = (unsigned)I;
+        a = Iu / nbs;
+        b = Iu - a * nbs;
         const double h = hd[I];
         tv = t[I];
         u = (float)(h - lambda);
         rr = (float)fabs(tv * (lambda - h)) * inv_rnorm;
+        return fabs(tv) >= (double)skip;
+    }
+    __device__ float2 excite(uint32_t a, uint32_t b, int col, const MlpSmem&) const {
+        const float2 x = *reinterpret_cast<const float2*>(tabA + (size_t)a * kMlpH + col);
+        const float2 y = *reinterpret_cast<const float2*>(tabB + (size_t)b * kMlpH + col);
+        return make_float2(x.x + y.x, x.y + y.y);
     }
     __device__ void store(size_t I, double tv, float f) const { t[I] = tv * (double)f; }
 };
@@ -94,12 +124,22 @@ struct SampleSource {  // training-style samples: factor out
     const float* u;
     const float* r;
     float* factor;
-    __device__ void load(size_t I, uint32_t& a, uint32_t& b, float& uu, float& rr, double& tv) const {
-        a = ea[I];
-        b = eb[I];
+    __device__ bool load(size_t I, uint32_t& a, uint32_t& b, float& uu, float& rr, double& tv) const {
+        a = ea[I] | (eb[I] << 16);
+        b = 0;
         uu = u[I];
         rr = fabsf(r[I]);
         tv = 0.0;
+        return true;
+    }
+    __device__ float2 excite(uint32_t a, uint32_t, int col, const MlpSmem& S) const {
+        float x = 0.0f, y = 0.0f;
+        for (uint32_t e = a; e; e &= e - 1) {
+            const int bit = __ffs(e) - 1;
+            x += S.w1[col][bit];
+            y += S.w1[col + 1][bit];
+        }
+        return make_float2(x, y);
     }
     __device__ void store(size_t I, double, float f) const { factor[I] = f; }
 };
@@ -117,15 +157,7 @@ __device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], 
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-struct MlpSmem {
-    float w1[kMlpH][kMlpIn];
-    float b1[kMlpH], b2[kMlpH], b3[kMlpH], w4[kMlpH];
-    float b4;
-    __nv_bfloat16 w2[kMlpH * kW2Ld];
-    __nv_bfloat16 w3[kMlpH * kW2Ld];
-};
-
-// one hidden layer on the tensor cores: A fragments in, relu(A W^T + b) re-packed as A fragments
+// one hidden layer on the tensor cores: A fragments in, relu(A W^T + b) as FP32 C fragments
 __device__ __forceinline__ void mma_layer(uint32_t (&a)[4][4], const __nv_bfloat16* W, const float* b, int g, int t4,
                                           float (&out)[8][4]) {
 #pragma unroll
@@ -146,6 +178,9 @@ __device__ __forceinline__ void mma_layer(uint32_t (&a)[4][4], const __nv_bfloat
     }
 }
 
+// One warp per tile of 16 consecutive determinants.  Lanes 0..15 load one determinant each and
+// compute its scalar inputs; mma fragment lane (g, t4) works on rows g and g + 8, whose inputs
+// arrive by shuffles; the factor goes back to the loading lane by a shuffle.
 template <class Src>
 __global__ void __launch_bounds__(256) k_mlp_apply(Src src, size_t N, MlpDevice P) {
     extern __shared__ __align__(16) unsigned char mlp_smem_raw[];
@@ -169,20 +204,25 @@ __global__ void __launch_bounds__(256) k_mlp_apply(Src src, size_t N, MlpDevice 
     const size_t nwarps = (gridDim.x * (size_t)blockDim.x) >> 5;
     const size_t ntiles = (N + 15) / 16;
     for (size_t tile = warp; tile < ntiles; tile += nwarps) {
-        size_t Irow[2];
-        double tv[2];
+        const size_t I = tile * 16 + (lane & 15);
+        const bool mine = lane < 16 && I < N;
+        uint32_t ka = 0, kb = 0;
+        float u = 0.0f, rr = 0.0f;
+        double tv = 0.0;
+        bool big = src.load(mine ? I : N - 1, ka, kb, u, rr, tv);
+        if (!__any_sync(0xffffffffu, mine && big)) continue;
+        float f0, f1, f2;
+        scalar_features(u, rr, f0, f1, f2);
+        uint32_t ra[2], rb[2];
         float x[2][3];
-        uint32_t ex[2];
 #pragma unroll
         for (int h = 0; h < 2; h++) {
-            size_t I = tile * 16 + g + 8 * h;
-            Irow[h] = I;
-            if (I >= N) I = N - 1;
-            uint32_t ea, eb;
-            float u, rr;
-            src.load(I, ea, eb, u, rr, tv[h]);
-            ex[h] = ea | (eb << 16);
-            scalar_features(u, rr, x[h][0], x[h][1], x[h][2]);
+            const int srcl = g + 8 * h;
+            ra[h] = __shfl_sync(0xffffffffu, ka, srcl);
+            rb[h] = __shfl_sync(0xffffffffu, kb, srcl);
+            x[h][0] = __shfl_sync(0xffffffffu, f0, srcl);
+            x[h][1] = __shfl_sync(0xffffffffu, f1, srcl);
+            x[h][2] = __shfl_sync(0xffffffffu, f2, srcl);
         }
         // layer 1 (FP32): columns 16kt + 2t4 + {0,1} and 16kt + 8 + 2t4 + {0,1} of rows g, g+8
         uint32_t a[4][4];
@@ -190,14 +230,17 @@ __global__ void __launch_bounds__(256) k_mlp_apply(Src src, size_t N, MlpDevice 
         for (int kt = 0; kt < 4; kt++) {
             float z[2][4];
 #pragma unroll
-            for (int cc = 0; cc < 4; cc++) {
-                const int col = 16 * kt + 2 * t4 + (cc & 1) + 8 * (cc >> 1);
-                const float* wr = S.w1[col];
+            for (int half = 0; half < 2; half++) {
+                const int col = 16 * kt + 8 * half + 2 * t4;
+                const float* w0 = S.w1[col];
+                const float* w1 = S.w1[col + 1];
 #pragma unroll
                 for (int h = 0; h < 2; h++) {
-                    float acc = S.b1[col] + wr[32] * x[h][0] + wr[33] * x[h][1] + wr[34] * x[h][2];
-                    for (uint32_t e = ex[h]; e; e &= e - 1) acc += wr[__ffs(e) - 1];
-                    z[h][cc] = fmaxf(acc, 0.0f);
+                    const float2 e = src.excite(ra[h], rb[h], col, S);
+                    const float z0 = S.b1[col] + w0[32] * x[h][0] + w0[33] * x[h][1] + w0[34] * x[h][2] + e.x;
+                    const float z1 = S.b1[col + 1] + w1[32] * x[h][0] + w1[33] * x[h][1] + w1[34] * x[h][2] + e.y;
+                    z[h][2 * half] = fmaxf(z0, 0.0f);
+                    z[h][2 * half + 1] = fmaxf(z1, 0.0f);
                 }
             }
             a[kt][0] = pack_bf16(z[0][0], z[0][1]);
@@ -226,10 +269,11 @@ __global__ void __launch_bounds__(256) k_mlp_apply(Src src, size_t N, MlpDevice 
         m0 += __shfl_xor_sync(0xffffffffu, m0, 2);
         m1 += __shfl_xor_sync(0xffffffffu, m1, 1);
         m1 += __shfl_xor_sync(0xffffffffu, m1, 2);
-        if (t4 < 2) {
-            const int h = t4;
-            if (Irow[h] < N) src.store(Irow[h], tv[h], 1.0f + kMlpRange * tanhf((h ? m1 : m0) + S.b4));
-        }
+        // lane (g, t4): t4 == 0 holds row g, t4 == 1 row g + 8; the loader of row r is lane r
+        const float fm = 1.0f + kMlpRange * tanhf((t4 ? m1 : m0) + S.b4);
+        const int r = lane & 15;
+        const float fr = __shfl_sync(0xffffffffu, fm, ((r & 7) << 2) | (r >> 3));
+        if (mine) src.store(I, tv, fr);
     }
 }
 
@@ -416,16 +460,27 @@ __global__ void k_diag_correction(double* __restrict__ t, const double* __restri
 }
 
 // ---- host -------------------------------------------------------------------------------
-static size_t mlp_apply_smem() { return sizeof(MlpSmem); }
 
-void mlp_apply(Context& c, double* t, double lambda, double rnorm) {
+void mlp_apply(Context& c, double* t, double lambda, double rnorm, double tnorm) {
     FCIB_CHECK(c.mlp_w.p, FCIB_ERR_STATE, "learned preconditioner selected but no MLP weights are loaded (fcib_set_mlp)");
-    EngineSource src{t, c.hdiag.p, c.A.str.p, c.B.str.p, (long long)c.nbs, lambda,
-                     (float)(rnorm > 0.0 ? 1.0 / rnorm : 0.0), c.na, c.nb};
-    const size_t smem = mlp_apply_smem();
+    FCIB_CHECK(c.ndet < ((int64_t)1 << 32), FCIB_ERR_UNSUPPORTED, "learned preconditioner: determinant index above 2^32");
+    if (!c.mlp_tables_ready) {
+        c.mlp_tabA.alloc((size_t)c.nas * kMlpH);
+        c.mlp_tabB.alloc((size_t)c.nbs * kMlpH);
+        k_mlp_tables<<<(unsigned)((c.nas * kMlpH + 255) / 256), 256, 0, c.stream>>>(c.A.str.p, (int)c.nas, c.na, 0,
+                                                                                  c.mlp_w.p, c.mlp_tabA.p);
+        FCIB_KCHECK();
+        k_mlp_tables<<<(unsigned)((c.nbs * kMlpH + 255) / 256), 256, 0, c.stream>>>(c.B.str.p, (int)c.nbs, c.nb, 16,
+                                                                                  c.mlp_w.p, c.mlp_tabB.p);
+        FCIB_KCHECK();
+        c.mlp_tables_ready = true;
+    }
+    EngineSource src{t, c.hdiag.p, c.mlp_tabA.p, c.mlp_tabB.p, (unsigned)c.nbs, lambda,
+                     (float)(rnorm > 0.0 ? 1.0 / rnorm : 0.0), (float)(kMlpSkip * tnorm)};
+    const size_t smem = sizeof(MlpSmem);
     FCIB_CUDA(cudaFuncSetAttribute(k_mlp_apply<EngineSource>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const size_t N = (size_t)c.ndet;
-    const int grid = (int)std::min<size_t>((size_t)4 * c.num_sms, (N + 127) / 128);
+    const int grid = (int)std::min<size_t>((size_t)6 * c.num_sms, (N + 127) / 128);
     k_mlp_apply<EngineSource><<<grid, 256, smem, c.stream>>>(src, N, MlpDevice{c.mlp_w.p});
     FCIB_KCHECK();
 }
@@ -484,6 +539,7 @@ extern "C" {
 int fcib_set_mlp(fcib_ctx* ctx, const float* weights, int nweights) {
     if (!ctx) { set_error("null context"); return FCIB_ERR_ARG; }
     return guarded(ctx, [&] {
+        ctx->c.mlp_tables_ready = false;
         if (!weights) {
             ctx->c.mlp_w.release();
             return;
@@ -492,6 +548,7 @@ int fcib_set_mlp(fcib_ctx* ctx, const float* weights, int nweights) {
         std::vector<float> w(weights, weights + nweights);
         for (float x : w) FCIB_CHECK(std::isfinite(x), FCIB_ERR_ARG, "fcib_set_mlp: non-finite weight");
         ctx->c.mlp_w.upload(w, ctx->c.stream);
+        ctx->c.mlp_tables_ready = false;
         FCIB_CUDA(cudaStreamSynchronize(ctx->c.stream));
     });
 }
@@ -511,7 +568,14 @@ int fcib_precondition(fcib_ctx* ctx, const double* r, double lambda, double* out
         upload_flat(c, r, d.p);
         k_diag_correction<<<4 * c.num_sms, 256, 0, c.stream>>>(d.p, c.hdiag.p, lambda, (size_t)c.ndet);
         FCIB_KCHECK();
-        if (c.opt.preconditioner == FCIB_PRECOND_MLP) mlp_apply(c, d.p, lambda, rn);
+        if (c.opt.preconditioner == FCIB_PRECOND_MLP) {
+            std::vector<double> h((size_t)c.ndet);
+            FCIB_CUDA(cudaMemcpyAsync(h.data(), d.p, sizeof(double) * c.ndet, cudaMemcpyDeviceToHost, c.stream));
+            FCIB_CUDA(cudaStreamSynchronize(c.stream));
+            double tn = 0.0;
+            for (double x : h) tn += x * x;
+            mlp_apply(c, d.p, lambda, rn, std::sqrt(tn));
+        }
         download_flat(c, d.p, out);
     });
 }
@@ -532,7 +596,7 @@ int fcib_mlp_eval(int device, int64_t n, const uint32_t* ea, const uint32_t* eb,
             f.alloc(n);
             FCIB_CUDA(cudaMemcpyAsync(w.p, weights, 4 * kMlpNW, cudaMemcpyHostToDevice, s));
             SampleSource src{ds.ea.p, ds.eb.p, ds.u.p, ds.r.p, f.p};
-            const size_t smem = mlp_apply_smem();
+            const size_t smem = sizeof(MlpSmem);
             FCIB_CUDA(cudaFuncSetAttribute(k_mlp_apply<SampleSource>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             const int grid = (int)std::min<int64_t>(1184, (n + 127) / 128);
             k_mlp_apply<SampleSource><<<grid, 256, smem, s>>>(src, (size_t)n, MlpDevice{w.p});
