@@ -295,6 +295,100 @@ def run_precond(args, world, rank, local):
         }), flush=True)
 
 
+BATCH_OPTS = {"E_CONVERGENCE": 1e-9, "R_CONVERGENCE": 1e-5, "DL_SUBSPACE_PER_ROOT": 8, "DL_COLLAPSE_PER_ROOT": 2,
+              "DL_MAXITER": 200}
+
+
+def batch_instances(count, sizes, seed):
+    """Seeded CAS instances: n drawn uniformly from `sizes`, integrals synthetic(n, 3n, seed_i)."""
+    from forte_b200 import synthetic
+    rng = np.random.default_rng(seed)
+    ns = rng.choice(sizes, size=count)
+    return [(synthetic(int(n), 3 * int(n), seed * 100003 + i), (int(n) + 1) // 2, int(n) // 2) for i, n in enumerate(ns)]
+
+
+def cpu_batch_sample(instances, nroot, budget_s=20.0):
+    """The oracle's Davidson on host cores (one process per core) over the smallest instances of the
+    batch until about budget_s of CPU time is used; returns instances/s and the sample description."""
+    import multiprocessing as mp
+    small = sorted(instances, key=lambda x: x[0].n)
+    cores = max(1, min(os.cpu_count() or 1, 16))
+    t0 = time.perf_counter()
+    done = 0
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        chunk = small[:cores * 4]
+        res = pool.map(_oracle_solve, [(x[0], x[1], x[2], nroot) for x in chunk])
+        done = len(res)
+    wall = time.perf_counter() - t0
+    sizes = sorted({x[0].n for x in chunk})
+    return done / wall, cores, f"{done} instances of CAS({sizes[0]},{sizes[0]})..CAS({sizes[-1]},{sizes[-1]}), the smallest of the batch, oracle Davidson, {cores} processes"
+
+
+def _oracle_solve(args):
+    ints, na, nb, nroot = args
+    sys.path.insert(0, ROOT)
+    from oracle.oracle import Oracle
+    o = Oracle(ints.n, na, nb)
+    o.set_integrals(ints)
+    return o.solve(nroot=nroot, multiplicity=0, e_conv=BATCH_OPTS["E_CONVERGENCE"], r_conv=BATCH_OPTS["R_CONVERGENCE"],
+                   maxiter=BATCH_OPTS["DL_MAXITER"])["energies"]
+
+
+def run_batch(args, world, rank, local):
+    """Batched CASCI: instances/s of one persistent launch over seeded CAS instances."""
+    import torch
+    from forte_b200 import build
+    from forte_b200.batch import BatchSolver
+    build.build()
+    torch.cuda.set_device(local)
+    sizes = [int(x) for x in args.batch_sizes.split(",")]
+    inst = batch_instances(args.batch_count, sizes, SEED + rank)
+    opts = dict(BATCH_OPTS)
+    if args.maxiter:
+        opts["DL_MAXITER"] = args.maxiter
+    t0 = time.perf_counter()
+    b = BatchSolver(inst, nroot=4, options=opts, device=local)
+    setup_s = time.perf_counter() - t0
+    tuned = b.tune() if args.warmup > 0 else None
+    for _ in range(max(0, args.warmup - 1)):
+        b.solve()
+    barrier(world)
+    ms = []
+    for _ in range(args.steps):
+        e, it, cv, d = b.solve()
+        ms.append(d)
+    step_s = allmax(world, statistics.mean(ms) / 1e3)
+    # end to end: integrals from host memory to energies back, through the public API
+    t1 = time.perf_counter()
+    b2 = BatchSolver(inst, nroot=4, options=opts, device=local)
+    e2, it2, cv2, _ = b2.solve()
+    e2e_s = allmax(world, time.perf_counter() - t1)
+    h2d = sum(sum(getattr(x[0], k).nbytes for k in ("oei_a", "oei_b", "tei_aa", "tei_ab", "tei_bb")) for x in inst)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, cores, sample = cpu_batch_sample(inst, 4)
+        cpu = {"value": v, "unit": "instances/s", "cores": cores, "kind": "port", "sample": sample}
+    if rank == 0:
+        ndets = [x[0].n for x in inst]
+        print(json.dumps({
+            "metric": f"batched CASCI instances/s ({args.batch_count} instances CAS({min(sizes)},{min(sizes)})-"
+                      f"CAS({max(sizes)},{max(sizes)}), 4 roots, one persistent launch)",
+            "value": world * args.batch_count / step_s, "unit": "instances/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{args.batch_count} seeded instances, n uniform in {sizes}, L=3n, 4 roots, "
+                                   "subspace 8/root", "e_convergence": opts["E_CONVERGENCE"],
+                       "r_convergence": opts["R_CONVERGENCE"], "parallelism": f"replicas x{world}"},
+            "iterations_mean": float(np.mean(it)), "iterations_max": int(np.max(it)),
+            "converged_fraction": float(np.mean(cv)), "autotune": tuned, "setup_seconds": setup_s,
+            "e2e": {"value": world * args.batch_count / e2e_s, "unit": "instances/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(e2.nbytes + it2.nbytes + cv2.nbytes)},
+            "cpu_baseline": cpu, "gpu_launches": 1,
+            "instances_by_orbitals": {str(n): int(ndets.count(n)) for n in sorted(set(ndets))},
+        }), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -306,9 +400,14 @@ def main():
     ap.add_argument("--ref-iterations", type=int, default=53, help="FP64 iteration count used by the CPU arm")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparator solve")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--mode", default="solve", choices=["solve", "sigma", "precond"],
+    ap.add_argument("--batch-count", type=int, default=256)
+    ap.add_argument("--batch-sizes", default="6,7,8,9,10")
+    ap.add_argument("--maxiter", type=int, default=0, help="batch mode: Davidson iteration cap (0 = 200)")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--mode", default="solve", choices=["solve", "sigma", "precond", "batch"],
                     help="solve: the Davidson time-to-solution metric; sigma: sigma builds/s at CAS(n,n); "
-                         "precond: learned vs diagonal preconditioner at CAS(14,14), 2 roots")
+                         "precond: learned vs diagonal preconditioner at CAS(14,14), 2 roots; "
+                         "batch: batched CASCI instances/s")
     ap.add_argument("--n", type=int, default=16, help="active orbitals of the sigma mode")
     args = ap.parse_args()
     world, rank, local = dist_init(args)
@@ -320,6 +419,9 @@ def main():
         return
     if args.mode == "precond":
         run_precond(args, world, rank, local)
+        return
+    if args.mode == "batch":
+        run_batch(args, world, rank, local)
         return
 
     import torch

@@ -101,6 +101,12 @@ SIGNATURES = {
                                  C.c_uint64, C.c_int, _fp, _dp]),
     "fcib_precondition": (C.c_int, [_vp, _dp, C.c_double, _dp]),
     "fcib_set_residual_capture": (C.c_int, [_vp, C.c_int]),
+    "fcib_batch_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                    C.POINTER(C.c_int), _dp, C.POINTER(_dp), C.POINTER(_dp), C.POINTER(_dp),
+                                    C.POINTER(_dp), C.POINTER(_dp), C.c_int, C.POINTER(FcibOptions)]),
+    "fcib_batch_destroy": (C.c_int, [_vp]),
+    "fcib_batch_solve": (C.c_int, [_vp, _dp, C.POINTER(C.c_int), C.POINTER(C.c_int), _dp]),
+    "fcib_batch_tune": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int), _dp]),
     "fcib_captured_residual": (C.c_int, [_vp, C.c_int, _dp, _dp, C.POINTER(C.c_int)]),
 }
 MLP_NWEIGHTS = 10689

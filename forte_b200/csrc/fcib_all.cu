@@ -7,4 +7,5 @@
 #include "rdms.cu"
 #include "capi.cu"
 #include "mlp.cu"
+#include "batch.cu"
 #include "noalloc.cu"
