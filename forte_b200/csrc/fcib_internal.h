@@ -154,6 +154,9 @@ struct Context {
     DBuf<double> ct, st;  // transposed C and sigma for beta same-spin terms
     DBuf<uint16_t> tgtR16; // beta replacement targets [string][pair] for the tensor-core kernel
     DBuf<float> tf_hi, tf_lo; // tf32 split planes of the sigma input (mixed path)
+    DBuf<float> c32, ct32;    // FP32 copy of the sigma input and its transpose (mixed same-spin)
+    DBuf<float> s32a, st32;   // FP32 same-spin sigma parts: alpha (row-major), beta (transposed)
+    bool c32_ready = false;   // c32 holds the current sigma input (written by the tensor-core split)
     float vmax = 0.0f;    // max |V| (fixed-point grid of the tensor-core scatter)
     DBuf<double> hdiag;
     // solver storage

@@ -180,12 +180,13 @@ constexpr int kGrRows = 8;   // rows per thread
 // Persistent CTAs take (group, column chunk) work items in chunk-major order, so the columns of
 // C and sigma a chunk touches stay L2-resident while every group of that chunk is processed.
 // The pair-pair block M stays in shared memory; W = M[lab_i][lab_j] is rebuilt per item from it.
-// T = double (FP64 path) or float (mixed path: FP32 operands and accumulation, FP64 atomics).
+// T = double (FP64 path: FP64 in, FP64 atomics) or float (mixed path: an FP32 copy of C in, FP32
+// accumulation, float2 vector atomics into an FP32 sigma buffer that is added to FP64 sigma later).
 constexpr int kGrLoads = 16;  // X elements per thread per item (G*kGrTN/threads <= 16 by construction)
 
 template <typename T>
 __global__ void __launch_bounds__(1024) k_group(
-    const double* __restrict__ C, double* __restrict__ S, int ncols,
+    const T* __restrict__ C, T* __restrict__ S, int ncols,
     const uint32_t* __restrict__ rows, const uint16_t* __restrict__ labs, int G, int Gp,
     const double* __restrict__ M, int ldm, int ngroups, int nchunks, int* __restrict__ counter, int m_in_smem) {
     using T2 = typename std::conditional<std::is_same<T, double>::value, double2, float2>::type;
@@ -219,11 +220,11 @@ __global__ void __launch_bounds__(1024) k_group(
         }
         __syncthreads();
         // gather the G rows (this chunk's columns) with all loads in flight at once
-        double xv[kGrLoads];
+        T xv[kGrLoads];
 #pragma unroll
         for (int r = 0; r < kGrLoads; r++) {
             const int idx = tid + r * nth;
-            double v = 0.0;
+            T v = (T)0;
             if (idx < G * kGrTN) {
                 const int j = idx / kGrTN, col = c0 + (idx - j * kGrTN);
                 if (col < ncols) v = C[(size_t)(rs[j] & kConnIdxMask) * ncols + col];
@@ -279,10 +280,16 @@ __global__ void __launch_bounds__(1024) k_group(
                 int ii = i0 + i;
                 if (ii < G) {
                     uint32_t e = rs[ii];
-                    double* dst = S + (size_t)(e & kConnIdxMask) * ncols + col;
-                    double sg = (e & kSignBit) ? -1.0 : 1.0;
-                    if (col < ncols) atomicAdd(dst, sg * (double)acc[i][0]);
-                    if (col + 1 < ncols) atomicAdd(dst + 1, sg * (double)acc[i][1]);
+                    const size_t off = (size_t)(e & kConnIdxMask) * ncols + col;
+                    T* dst = S + off;
+                    const T a0 = (e & kSignBit) ? -acc[i][0] : acc[i][0];
+                    const T a1 = (e & kSignBit) ? -acc[i][1] : acc[i][1];
+                    if (!std::is_same<T, double>::value && col + 1 < ncols && (off & 1) == 0) {
+                        atomicAdd(reinterpret_cast<float2*>(dst), make_float2((float)a0, (float)a1));
+                    } else {
+                        if (col < ncols) atomicAdd(dst, a0);
+                        if (col + 1 < ncols) atomicAdd(dst + 1, a1);
+                    }
                 }
             }
         }
@@ -290,7 +297,7 @@ __global__ void __launch_bounds__(1024) k_group(
 }
 
 template <typename T>
-static void launch_group_t(Context& c, const double* C, double* S, int ncols, int ngroups, int G,
+static void launch_group_t(Context& c, const T* C, T* S, int ncols, int ngroups, int G,
                            const uint32_t* rows, const uint16_t* labs, const double* M, int ldm) {
     if (ngroups == 0 || G == 0) return;
     int Gp = (G + kGrRows - 1) / kGrRows * kGrRows;
@@ -314,9 +321,12 @@ static void launch_group_t(Context& c, const double* C, double* S, int ncols, in
 }
 
 static void launch_group(Context& c, const double* C, double* S, int ncols, int ngroups, int G,
-                         const uint32_t* rows, const uint16_t* labs, const double* M, int ldm, bool fp32 = false) {
-    if (fp32) launch_group_t<float>(c, C, S, ncols, ngroups, G, rows, labs, M, ldm);
-    else launch_group_t<double>(c, C, S, ncols, ngroups, G, rows, labs, M, ldm);
+                         const uint32_t* rows, const uint16_t* labs, const double* M, int ldm) {
+    launch_group_t<double>(c, C, S, ncols, ngroups, G, rows, labs, M, ldm);
+}
+static void launch_group(Context& c, const float* C, float* S, int ncols, int ngroups, int G,
+                         const uint32_t* rows, const uint16_t* labs, const double* M, int ldm) {
+    launch_group_t<float>(c, C, S, ncols, ngroups, G, rows, labs, M, ldm);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -355,6 +365,48 @@ __global__ void k_transpose_add(const double* __restrict__ in, double* __restric
     }
 }
 
+__global__ void k_transpose_f32(const float* __restrict__ in, float* __restrict__ out, int rows, int cols) {
+    __shared__ float tile[32][33];
+    int x = blockIdx.x * 32 + threadIdx.x;
+    int y0 = blockIdx.y * 32;
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        int y = y0 + j;
+        if (x < cols && y < rows) tile[j][threadIdx.x] = in[(size_t)y * cols + x];
+    }
+    __syncthreads();
+    int ox = y0 + threadIdx.x;
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        int oy = blockIdx.x * 32 + j;
+        if (ox < rows && oy < cols) out[(size_t)oy * rows + ox] = tile[threadIdx.x][j];
+    }
+}
+
+// S[r][c] += A[r][c] + Bt[c][r]: the alpha (row-major) and beta (transposed) FP32 same-spin parts
+__global__ void k_add_same_f32(double* __restrict__ S, const float* __restrict__ A, const float* __restrict__ Bt,
+                               int rows, int cols) {
+    __shared__ float tile[32][33];
+    int x = blockIdx.x * 32 + threadIdx.x;  // Bt column = S row
+    int y0 = blockIdx.y * 32;               // Bt row = S column
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        int y = y0 + j;
+        if (x < rows && y < cols) tile[j][threadIdx.x] = Bt[(size_t)y * rows + x];
+    }
+    __syncthreads();
+    int oc = y0 + threadIdx.x;
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        int orow = blockIdx.x * 32 + j;
+        if (orow < rows && oc < cols) {
+            const size_t o = (size_t)orow * cols + oc;
+            S[o] += (double)A[o] + (double)tile[threadIdx.x][j];
+        }
+    }
+}
+
+__global__ void k_to_f32(const double* __restrict__ in, float* __restrict__ out, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = (float)in[i];
+}
+
 __global__ void k_scale_copy(const double* __restrict__ in, double* __restrict__ out, double a, size_t n) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
         out[i] = a * in[i];
@@ -390,20 +442,48 @@ void apply_mask(Context& c, double* v) {
 static void sigma_same_spin(Context& c, const double* C, double* S, bool fp32) {
     const int nas = (int)c.nas, nbs = (int)c.nbs;
     const size_t N = (size_t)c.ndet;
-    if (!c.fold_h && c.A.ng1)
-        launch_group(c, C, S, nbs, c.A.ng1, c.A.g1, c.A.g1row.p, c.A.g1lab.p, c.Ha.p, c.n, fp32);
     const int np2 = c.n * (c.n - 1) / 2;
-    if (c.A.ng2) launch_group(c, C, S, nbs, c.A.ng2, c.A.g2, c.A.g2row.p, c.A.g2lab.p, c.M2a.p, np2, fp32);
-    bool beta_g1 = (!c.fold_h && c.B.ng1);
-    if (c.B.ng2 || beta_g1) {
-        c.ct.alloc(N);
-        c.st.alloc(N);
-        transpose(c, C, c.ct.p, nas, nbs);
-        FCIB_CUDA(cudaMemsetAsync(c.st.p, 0, N * sizeof(double), c.stream));
-        if (beta_g1) launch_group(c, c.ct.p, c.st.p, nas, c.B.ng1, c.B.g1, c.B.g1row.p, c.B.g1lab.p, c.Hb.p, c.n, fp32);
-        if (c.B.ng2) launch_group(c, c.ct.p, c.st.p, nas, c.B.ng2, c.B.g2, c.B.g2row.p, c.B.g2lab.p, c.M2b.p, np2, fp32);
-        transpose_add(c, c.st.p, S, nas, nbs);
+    const bool a_g1 = !c.fold_h && c.A.ng1, b_g1 = !c.fold_h && c.B.ng1;
+    if (!fp32) {
+        if (a_g1) launch_group(c, C, S, nbs, c.A.ng1, c.A.g1, c.A.g1row.p, c.A.g1lab.p, c.Ha.p, c.n);
+        if (c.A.ng2) launch_group(c, C, S, nbs, c.A.ng2, c.A.g2, c.A.g2row.p, c.A.g2lab.p, c.M2a.p, np2);
+        if (c.B.ng2 || b_g1) {
+            c.ct.alloc(N);
+            c.st.alloc(N);
+            transpose(c, C, c.ct.p, nas, nbs);
+            FCIB_CUDA(cudaMemsetAsync(c.st.p, 0, N * sizeof(double), c.stream));
+            if (b_g1) launch_group(c, c.ct.p, c.st.p, nas, c.B.ng1, c.B.g1, c.B.g1row.p, c.B.g1lab.p, c.Hb.p, c.n);
+            if (c.B.ng2) launch_group(c, c.ct.p, c.st.p, nas, c.B.ng2, c.B.g2, c.B.g2row.p, c.B.g2lab.p, c.M2b.p, np2);
+            transpose_add(c, c.st.p, S, nas, nbs);
+        }
+        return;
     }
+    // mixed: FP32 copy of C (written by the tensor-core split when it ran), FP32 accumulation
+    const bool any_a = a_g1 || c.A.ng2, any_b = b_g1 || c.B.ng2;
+    if (!any_a && !any_b) return;
+    if (!c.c32_ready) {
+        c.c32.alloc(N);
+        k_to_f32<<<4 * c.num_sms, 256, 0, c.stream>>>(C, c.c32.p, N);
+        FCIB_KCHECK();
+    }
+    c.c32_ready = false;
+    c.s32a.alloc(N);
+    c.st32.alloc(N);
+    FCIB_CUDA(cudaMemsetAsync(c.s32a.p, 0, N * sizeof(float), c.stream));
+    FCIB_CUDA(cudaMemsetAsync(c.st32.p, 0, N * sizeof(float), c.stream));
+    if (a_g1) launch_group(c, c.c32.p, c.s32a.p, nbs, c.A.ng1, c.A.g1, c.A.g1row.p, c.A.g1lab.p, c.Ha.p, c.n);
+    if (c.A.ng2) launch_group(c, c.c32.p, c.s32a.p, nbs, c.A.ng2, c.A.g2, c.A.g2row.p, c.A.g2lab.p, c.M2a.p, np2);
+    if (any_b) {
+        c.ct32.alloc(N);
+        dim3 grid((nbs + 31) / 32, (nas + 31) / 32), block(32, 8);
+        k_transpose_f32<<<grid, block, 0, c.stream>>>(c.c32.p, c.ct32.p, nas, nbs);
+        FCIB_KCHECK();
+        if (b_g1) launch_group(c, c.ct32.p, c.st32.p, nas, c.B.ng1, c.B.g1, c.B.g1row.p, c.B.g1lab.p, c.Hb.p, c.n);
+        if (c.B.ng2) launch_group(c, c.ct32.p, c.st32.p, nas, c.B.ng2, c.B.g2, c.B.g2row.p, c.B.g2lab.p, c.M2b.p, np2);
+    }
+    dim3 grid2((nas + 31) / 32, (nbs + 31) / 32), block2(32, 8);
+    k_add_same_f32<<<grid2, block2, 0, c.stream>>>(S, c.s32a.p, c.st32.p, nas, nbs);
+    FCIB_KCHECK();
 }
 
 // events bracketing the opposite-spin and same-spin parts of a sigma build

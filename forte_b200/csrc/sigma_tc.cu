@@ -14,11 +14,12 @@
 // * two 144-column accumulators in TMEM are double buffered, so the MMAs of tile t overlap the
 //   epilogue of tile t-1;
 // * the epilogue accumulates the sigma row exactly in two-word fixed point with native 32-bit
-//   shared-memory integer atomics: each contribution y is scaled to a 64-bit integer on a grid
-//   2^-el chosen per sigma from max|C| * max|V| (so |y| 2^el < 2^46), split into a signed high
-//   part (bits >= 22) and an unsigned 22-bit low part; every sigma element receives at most
-//   s1 (<= 72) contributions, so neither word can overflow.  The row is converted back to FP64
-//   and added to E0*C when it is written.
+//   shared-memory integer atomics: each contribution y is scaled, exactly and in FP32, to the
+//   grid 2^-el chosen per sigma from max|C| * max|V| (so |y| 2^el < 2^44) and rounded to the
+//   integer X = hi 2^22 + lo with |hi| < 2^22 and |lo| <= 2^21 (FP32 adds of 1.5 * 2^23 do the
+//   rounding; no FP64 or conversion instructions); every sigma element receives at most
+//   s1 (<= 72) contributions, so neither 32-bit word can overflow.  The row is converted back to
+//   FP64 and added to E0*C when it is written.
 //
 // Every mbarrier wait is bounded; on timeout the kernel records an error code, waits (bounded)
 // for its outstanding MMAs, frees tensor memory and exits.
@@ -154,6 +155,8 @@ constexpr int kTcWarps = kTcThreads / 32;
 constexpr int kTcGat = 3;    // 8-column A chunks per warp per tile: 9 chunks over 4 column groups
 constexpr int kTcEpiC = 5;   // 8-column accumulator chunks per warp: 18 chunks over 4 column groups
 constexpr int kFixLoBits = 22;
+constexpr float kMagic = 12582912.0f;       // 1.5 * 2^23: x + kMagic rounds |x| < 2^22 to an integer
+constexpr int kMagicBits = 0x4B400000;      // bit pattern of kMagic
 
 template <bool THREE>
 __global__ void __launch_bounds__(kTcThreads, 1)
@@ -196,11 +199,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const uint32_t tmem_base = *tmem_slot;
     const uint32_t tlane = (uint32_t)(32 * q) << 16;
 
-    // fixed-point grid: |y| <= kpad * max|C| * max|V| < 2^46 * 2^-el
+    // fixed-point grid: |y| <= kpad * max|C| * max|V| < 2^44 * 2^-el
     const float cmax = __uint_as_float(*cmax_bits);
     const float ybound = fmaxf(1.01f * (float)kpad * cmax * vmax, 1e-30f);
-    const int el = min(60, (int)floorf(46.0f - log2f(ybound)));
-    const double grid = ldexp(1.0, el), inv_grid = ldexp(1.0, -el);
+    const int el = min(60, (int)floorf(44.0f - log2f(ybound)));
+    const double inv_grid = ldexp(1.0, -el);
+    const float gridf = ldexpf(1.0f, el);  // exact power of two (el <= 60 is within float range)
 
     // instruction descriptor: D f32, A/B tf32, both K-major, N = npad, M = 128
     const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(npad >> 3) << 17) | ((uint32_t)(kTcM >> 4) << 24);
@@ -330,12 +334,17 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                         for (int u = 0; u < 8; u++) {
                             const uint32_t g = (w[u >> 1] >> (16 * (u & 1))) & 0xFFFFu;
                             if (g != 0xFFFFu) {
-                                double y = (double)v[u];
-                                if (g & 0x8000u) y = -y;
-                                const long long Y = __double2ll_rn(y * grid);
+                                // y 2^el exactly in FP32 (|.| < 2^44), split as hi 2^22 + lo with
+                                // hi = round(y 2^(el-22)) and lo = round(y 2^el - hi 2^22), |lo| <= 2^21;
+                                // both rounded to integers by adding 1.5 * 2^23
+                                const float ys = v[u] * ((g & 0x8000u) ? -gridf : gridf);
+                                const float hf = fmaf(ys, 2.38418579e-7f, kMagic) - kMagic;
+                                const float lf = fmaf(-hf, 4194304.0f, ys);
+                                const int hi = __float_as_int(hf + kMagic) - kMagicBits;
+                                const int lo = __float_as_int(lf + kMagic) - kMagicBits;
                                 const uint32_t idx = (g & 0x7FFFu) << 2;
-                                red_add_u32(acc_hi_s + idx, (uint32_t)(int)(Y >> kFixLoBits));
-                                red_add_u32(acc_lo_s + idx, (uint32_t)(Y & ((1ll << kFixLoBits) - 1)));
+                                red_add_u32(acc_hi_s + idx, (uint32_t)hi);
+                                red_add_u32(acc_lo_s + idx, (uint32_t)lo);
                             }
                         }
                     }
@@ -349,7 +358,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         const double* Crow = C + (size_t)Ia * nbs;
         double* Srow = S + (size_t)Ia * nbs;
         for (int j = tid; j < nbs; j += blockDim.x) {
-            const long long tot = ((long long)acc_hi[j] << kFixLoBits) + (long long)acc_lo[j];
+            const long long tot = ((long long)acc_hi[j] << kFixLoBits) + (long long)(int)acc_lo[j];
             Srow[j] = e0 * Crow[j] + (double)tot * inv_grid;
         }
         __syncthreads();
@@ -383,8 +392,8 @@ __global__ void k_tgt_rows16(const int32_t* __restrict__ tgt, uint16_t* __restri
 }
 
 // C (FP64, nas x nbs) -> tf32 hi/lo planes with row stride ldp (zero padded); also max |C|
-__global__ void k_split_tf32(const double* __restrict__ C, float* __restrict__ hi, float* __restrict__ lo, int nas,
-                             int nbs, int ldp, unsigned int* __restrict__ cmax_bits) {
+__global__ void k_split_tf32(const double* __restrict__ C, float* __restrict__ hi, float* __restrict__ lo,
+                             float* __restrict__ c32, int nas, int nbs, int ldp, unsigned int* __restrict__ cmax_bits) {
     size_t total = (size_t)nas * ldp;
     float mx = 0.f;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
@@ -393,6 +402,7 @@ __global__ void k_split_tf32(const double* __restrict__ C, float* __restrict__ h
         float h = __uint_as_float(to_tf32((float)v));
         hi[i] = h;
         if (lo) lo[i] = __uint_as_float(to_tf32((float)(v - (double)h)));
+        if (col < nbs) c32[(size_t)r * nbs + col] = (float)v;
         mx = fmaxf(mx, fabsf((float)v));
     }
     for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
@@ -431,8 +441,11 @@ void ab_tc(Context& c, const double* C, double* S, bool three) {
     FCIB_CUDA(cudaMemsetAsync(c.counter.p, 0, 3 * sizeof(int), c.stream));
     unsigned int* cmax_bits = reinterpret_cast<unsigned int*>(c.counter.p + 3);
     FCIB_CUDA(cudaMemsetAsync(cmax_bits, 0, sizeof(unsigned int), c.stream));
-    k_split_tf32<<<8 * c.num_sms, 256, 0, c.stream>>>(C, c.tf_hi.p, three ? c.tf_lo.p : nullptr, nas, nbs, ldp, cmax_bits);
+    c.c32.alloc((size_t)nas * nbs);
+    k_split_tf32<<<8 * c.num_sms, 256, 0, c.stream>>>(C, c.tf_hi.p, three ? c.tf_lo.p : nullptr, c.c32.p, nas, nbs, ldp,
+                                                     cmax_bits);
     FCIB_KCHECK();
+    c.c32_ready = true;
     auto kern = three ? k_ab_tc<true> : k_ab_tc<false>;
     FCIB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int grid = std::min(nas, c.num_sms);
