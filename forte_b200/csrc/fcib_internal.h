@@ -152,8 +152,8 @@ struct Context {
     DBuf<uint8_t> mask;   // determinant in target irrep (only when nirrep > 1)
     // work vectors
     DBuf<double> ct, st;  // transposed C and sigma for beta same-spin terms
-    DBuf<uint16_t> tgtR16; // beta replacement targets [string][pair] for the tensor-core kernel
-    DBuf<float> tf_hi, tf_lo; // tf32 split planes of the sigma input (mixed path)
+    DBuf<uint16_t> tgtR16; // beta replacement targets [pair/8][string][pair%8] for the tensor-core kernel
+    DBuf<float> tf_hi;        // interleaved (tf32 hi, tf32 lo) pairs of the sigma input (mixed path)
     DBuf<float> c32, ct32;    // FP32 copy of the sigma input and its transpose (mixed same-spin)
     DBuf<float> s32a, st32;   // FP32 same-spin sigma parts: alpha (row-major), beta (transposed)
     bool c32_ready = false;   // c32 holds the current sigma input (written by the tensor-core split)

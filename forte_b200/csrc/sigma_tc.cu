@@ -89,14 +89,23 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
                  : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
-    uint32_t r0, r1, r2, r3, r4, r5, r6, r7;
+// 8 columns of the accumulator without waiting; tmem_wait_ld8 must follow before any use
+__device__ __forceinline__ void tmem_ld8_async(uint32_t taddr, uint32_t (&r)[8]) {
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3), "=r"(r4), "=r"(r5), "=r"(r6), "=r"(r7)
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
                  : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-    v[0] = __uint_as_float(r0); v[1] = __uint_as_float(r1); v[2] = __uint_as_float(r2); v[3] = __uint_as_float(r3);
-    v[4] = __uint_as_float(r4); v[5] = __uint_as_float(r5); v[6] = __uint_as_float(r6); v[7] = __uint_as_float(r7);
+}
+// waits for every outstanding tcgen05.ld of the thread; the "+r" operands keep the compiler from
+// moving uses of those registers above the wait
+__device__ __forceinline__ void tmem_wait_ld8(uint32_t (&r)[8]) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7])
+                 :: "memory");
+}
+// orders later uses of r after a preceding volatile wait (emits no instruction)
+__device__ __forceinline__ void reg_after(uint32_t (&r)[8]) {
+    asm volatile(""
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]));
 }
 
 struct TcLayout {
@@ -125,8 +134,9 @@ __device__ __forceinline__ uint32_t kmaj_off(int row, int k, int rows) {
     return (uint32_t)((k >> 2) * (rows / 8) * 128 + (row >> 3) * 128 + (row & 7) * 16 + (k & 3) * 4);
 }
 
+// no "memory" clobber: the accumulator is read only after a __syncthreads, which orders it
 __device__ __forceinline__ void red_add_u32(uint32_t saddr, uint32_t v) {
-    asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(saddr), "r"(v) : "memory");
+    asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(saddr), "r"(v));
 }
 
 __device__ __forceinline__ void mma_tf32_ta(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc, uint32_t idesc,
@@ -160,10 +170,10 @@ constexpr int kMagicBits = 0x4B400000;      // bit pattern of kMagic
 
 template <bool THREE>
 __global__ void __launch_bounds__(kTcThreads, 1)
-    k_ab_tc(const float* __restrict__ Phi, const float* __restrict__ Plo, int ldp, const double* __restrict__ C,
+    k_ab_tc(const float2* __restrict__ Phl, int ldp, const double* __restrict__ C,
             double* __restrict__ S, const uint32_t* __restrict__ connA, int s1a, const uint16_t* __restrict__ tgtR,
             int npair, const double* __restrict__ V, int ldv, float vmax, const unsigned int* __restrict__ cmax_bits,
-            int nas, int nbs, double e0, int* __restrict__ row_counter, int* __restrict__ err) {
+            int nas, int nbs, int s1b, double e0, int* __restrict__ row_counter, int* __restrict__ err) {
     extern __shared__ __align__(128) unsigned char smem[];
     const TcLayout L = tc_layout(s1a, npair, nbs, THREE);
     unsigned char* Bhi = smem + L.off_bhi;
@@ -205,6 +215,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const int el = min(60, (int)floorf(44.0f - log2f(ybound)));
     const double inv_grid = ldexp(1.0, -el);
     const float gridf = ldexpf(1.0f, el);  // exact power of two (el <= 60 is within float range)
+    const unsigned magic_total = (unsigned)s1b * (unsigned)kMagicBits;  // removed once per element (mod 2^32)
 
     // instruction descriptor: D f32, A/B tf32, both K-major, N = npad, M = 128
     const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(npad >> 3) << 17) | ((uint32_t)(kTcM >> 4) << 24);
@@ -253,8 +264,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     float h = 0.f, l = 0.f;
                     if (c8 < nk8 && k < s1a && jb < nbs) {
                         const size_t o = (size_t)(cs[k] & kConnIdxMask) * ldp + jb;
-                        h = __ldg(Phi + o);
-                        if (THREE) l = __ldg(Plo + o);
+                        const float2 x = __ldg(Phl + o);  // interleaved (hi, lo) TF32 pair
+                        h = x.x;
+                        if (THREE) l = x.y;
                     }
                     gh[j][u] = h;
                     gl[j][u] = l;
@@ -286,6 +298,18 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 }
                 asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
             }
+            // targets of the epilogue tile t-1, loaded early (consumed in (d))
+            uint4 tg[kTcEpiC];
+            {
+                const int jb = (t - 1) * kTcM + 32 * q + lane;
+#pragma unroll
+                for (int i = 0; i < kTcEpiC; i++) {
+                    const int c8 = cg + 4 * i;
+                    tg[i] = (t >= 1 && c8 < nn8 && jb < nbs)
+                                ? __ldg(reinterpret_cast<const uint4*>(tgtR + ((size_t)c8 * nbs + jb) * 8))
+                                : make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
+                }
+            }
             tc_fence_before();
             __syncthreads();
             tc_fence_after();
@@ -313,38 +337,37 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             if (t + 1 < ntiles) prefetch(t + 1);
             // (d) epilogue of tile t-1: exact fixed-point scatter over beta replacements
             if (t >= 1) {
-                const int jb = (t - 1) * kTcM + 32 * q + lane;
                 const uint32_t tbase = tmem_base + (uint32_t)prv * kColAccStride + tlane;
-                uint4 tg[kTcEpiC];
+                // all of this warp's accumulator chunks are loaded before a single wait
+                uint32_t rv[kTcEpiC][8];
 #pragma unroll
                 for (int i = 0; i < kTcEpiC; i++) {
                     const int c8 = cg + 4 * i;
-                    tg[i] = (c8 < nn8 && jb < nbs)
-                                ? __ldg(reinterpret_cast<const uint4*>(tgtR + (size_t)jb * npad + c8 * 8))
-                                : make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
+                    if (c8 < nn8) tmem_ld8_async(tbase + (uint32_t)(c8 * 8), rv[i]);
                 }
+                tmem_wait_ld8(rv[0]);
+#pragma unroll
+                for (int i = 1; i < kTcEpiC; i++) reg_after(rv[i]);
 #pragma unroll
                 for (int i = 0; i < kTcEpiC; i++) {
                     const int c8 = cg + 4 * i;
                     if (c8 < nn8) {
-                        float v[8];
-                        tmem_ld8(tbase + (uint32_t)(c8 * 8), v);
                         const uint32_t w[4] = {tg[i].x, tg[i].y, tg[i].z, tg[i].w};
 #pragma unroll
                         for (int u = 0; u < 8; u++) {
                             const uint32_t g = (w[u >> 1] >> (16 * (u & 1))) & 0xFFFFu;
                             if (g != 0xFFFFu) {
                                 // y 2^el exactly in FP32 (|.| < 2^44), split as hi 2^22 + lo with
-                                // hi = round(y 2^(el-22)) and lo = round(y 2^el - hi 2^22), |lo| <= 2^21;
-                                // both rounded to integers by adding 1.5 * 2^23
-                                const float ys = v[u] * ((g & 0x8000u) ? -gridf : gridf);
-                                const float hf = fmaf(ys, 2.38418579e-7f, kMagic) - kMagic;
-                                const float lf = fmaf(-hf, 4194304.0f, ys);
-                                const int hi = __float_as_int(hf + kMagic) - kMagicBits;
-                                const int lo = __float_as_int(lf + kMagic) - kMagicBits;
+                                // hi = round(y 2^(el-22)) and lo = round(y 2^el - hi 2^22), |lo| <= 2^21,
+                                // both rounded by adding 1.5 * 2^23; the raw bit patterns (integer +
+                                // kMagicBits) are accumulated and s1b * kMagicBits is removed per element
+                                // when the row is written (every element gets exactly s1b contributions)
+                                const float ys = __uint_as_float(rv[i][u]) * ((g & 0x8000u) ? -gridf : gridf);
+                                const float t1 = fmaf(ys, 2.38418579e-7f, kMagic);
+                                const float lf = fmaf(kMagic - t1, 4194304.0f, ys);
                                 const uint32_t idx = (g & 0x7FFFu) << 2;
-                                red_add_u32(acc_hi_s + idx, (uint32_t)hi);
-                                red_add_u32(acc_lo_s + idx, (uint32_t)lo);
+                                red_add_u32(acc_hi_s + idx, __float_as_uint(t1));
+                                red_add_u32(acc_lo_s + idx, __float_as_uint(lf + kMagic));
                             }
                         }
                     }
@@ -358,7 +381,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         const double* Crow = C + (size_t)Ia * nbs;
         double* Srow = S + (size_t)Ia * nbs;
         for (int j = tid; j < nbs; j += blockDim.x) {
-            const long long tot = ((long long)acc_hi[j] << kFixLoBits) + (long long)(int)acc_lo[j];
+            const int hi = (int)((unsigned)acc_hi[j] - magic_total), lo = (int)(acc_lo[j] - magic_total);
+            const long long tot = ((long long)hi << kFixLoBits) + (long long)lo;
             Srow[j] = e0 * Crow[j] + (double)tot * inv_grid;
         }
         __syncthreads();
@@ -376,12 +400,17 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(kTmemCols) : "memory");
 }
 
-// tgtR[Jb][R] = 16-bit scatter target of F_R Jb: index | sign << 15; no connection -> 0xFFFF
+// tgtR[R/8][Jb][R%8] = 16-bit scatter target of F_R Jb: index | sign << 15; no connection -> 0xFFFF.
+// Chunk-major: the 8 targets of one 8-pair chunk of consecutive Jb sit in consecutive 16-byte words,
+// so a warp (32 consecutive Jb) reads one chunk with fully coalesced loads.
 __global__ void k_tgt_rows16(const int32_t* __restrict__ tgt, uint16_t* __restrict__ out, int nstr, int npp_in,
                              int npad_out) {
     size_t total = (size_t)npad_out * nstr;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
-        int J = (int)(i / npad_out), R = (int)(i % npad_out);
+        const int u = (int)(i & 7);
+        const size_t cj = i >> 3;
+        const int c8 = (int)(cj / nstr), J = (int)(cj - (size_t)c8 * nstr);
+        const int R = 8 * c8 + u;
         uint16_t v = 0xFFFFu;
         if (R < npp_in) {
             int32_t t = tgt[(size_t)J * npp_in + R];
@@ -392,16 +421,17 @@ __global__ void k_tgt_rows16(const int32_t* __restrict__ tgt, uint16_t* __restri
 }
 
 // C (FP64, nas x nbs) -> tf32 hi/lo planes with row stride ldp (zero padded); also max |C|
-__global__ void k_split_tf32(const double* __restrict__ C, float* __restrict__ hi, float* __restrict__ lo,
-                             float* __restrict__ c32, int nas, int nbs, int ldp, unsigned int* __restrict__ cmax_bits) {
+// hl[r][col] = (tf32 hi, tf32 lo) of C[r][col] (interleaved, row stride ldp), c32 = FP32 copy of C,
+// cmax_bits = bits of max|C| rounded up
+__global__ void k_split_tf32(const double* __restrict__ C, float2* __restrict__ hl, float* __restrict__ c32, int nas,
+                             int nbs, int ldp, unsigned int* __restrict__ cmax_bits) {
     size_t total = (size_t)nas * ldp;
     float mx = 0.f;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
         int r = (int)(i / ldp), col = (int)(i % ldp);
         double v = col < nbs ? C[(size_t)r * nbs + col] : 0.0;
-        float h = __uint_as_float(to_tf32((float)v));
-        hi[i] = h;
-        if (lo) lo[i] = __uint_as_float(to_tf32((float)(v - (double)h)));
+        const float h = __uint_as_float(to_tf32((float)v));
+        hl[i] = make_float2(h, __uint_as_float(to_tf32((float)(v - (double)h))));
         if (col < nbs) c32[(size_t)r * nbs + col] = (float)v;
         mx = fmaxf(mx, fabsf((float)v));
     }
@@ -435,14 +465,14 @@ void ab_tc(Context& c, const double* C, double* S, bool three) {
         c.vmax = (float)(m * (1.0 + 1e-6)) + 1e-30f;
     }
     const int ldp = (nbs + 3) / 4 * 4;
-    c.tf_hi.alloc((size_t)nas * ldp);
-    if (three) c.tf_lo.alloc((size_t)nas * ldp);
+    c.tf_hi.alloc(2 * (size_t)nas * ldp);  // interleaved hi/lo pairs
     if (!c.counter.p) c.counter.alloc(16);
     FCIB_CUDA(cudaMemsetAsync(c.counter.p, 0, 3 * sizeof(int), c.stream));
     unsigned int* cmax_bits = reinterpret_cast<unsigned int*>(c.counter.p + 3);
     FCIB_CUDA(cudaMemsetAsync(cmax_bits, 0, sizeof(unsigned int), c.stream));
     c.c32.alloc((size_t)nas * nbs);
-    k_split_tf32<<<8 * c.num_sms, 256, 0, c.stream>>>(C, c.tf_hi.p, three ? c.tf_lo.p : nullptr, c.c32.p, nas, nbs, ldp,
+    float2* hl = reinterpret_cast<float2*>(c.tf_hi.p);
+    k_split_tf32<<<8 * c.num_sms, 256, 0, c.stream>>>(C, hl, c.c32.p, nas, nbs, ldp,
                                                      cmax_bits);
     FCIB_KCHECK();
     c.c32_ready = true;
@@ -451,9 +481,9 @@ void ab_tc(Context& c, const double* C, double* S, bool three) {
     int grid = std::min(nas, c.num_sms);
     c.tc_ev.ensure();
     FCIB_CUDA(cudaEventRecord(c.tc_ev.e[0], c.stream));
-    kern<<<grid, kTcThreads, smem, c.stream>>>(c.tf_hi.p, three ? c.tf_lo.p : c.tf_hi.p, ldp, C, S, c.A.conn.p, s1a,
-                                              c.tgtR16.p, npair, c.V.p, c.A.npair_pad, c.vmax, cmax_bits, nas, nbs,
-                                              c.scalar, c.counter.p, c.counter.p + 1);
+    kern<<<grid, kTcThreads, smem, c.stream>>>(hl, ldp, C, S, c.A.conn.p, s1a, c.tgtR16.p, npair, c.V.p,
+                                              c.A.npair_pad, c.vmax, cmax_bits, nas, nbs, c.B.s1, c.scalar,
+                                              c.counter.p, c.counter.p + 1);
     FCIB_KCHECK();
     FCIB_CUDA(cudaEventRecord(c.tc_ev.e[1], c.stream));
     c.tc_recorded = true;
