@@ -186,6 +186,78 @@ __global__ void __launch_bounds__(kRedThreads) k_combo(ComboArgs a, size_t N, do
     }
 }
 
+// Fused projection + check: out = rho * (a * x - sum_j coef_j V_j) and, in the same pass,
+// partial sums of V_j . out (slots j < nv) and out . out (slot kMaxIn).  out may alias x.
+struct OrthArgs {
+    const double* v[kMaxIn];
+    double coef[kMaxIn];
+    const double* x;
+    double* out;
+    double a, rho;
+    int nv;
+};
+
+template <int NV>
+__global__ void __launch_bounds__(kRedThreads) k_orth(OrthArgs a, size_t N, double* __restrict__ partial) {
+    double acc[NV + 1];
+#pragma unroll
+    for (int j = 0; j <= NV; j++) acc[j] = 0.0;
+    const size_t G = (size_t)gridDim.x * blockDim.x;
+    size_t I = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    for (; I + G < N; I += 2 * G) {
+        double o[2];
+#pragma unroll
+        for (int u = 0; u < 2; u++) o[u] = a.a * a.x[I + u * G];
+#pragma unroll
+        for (int j = 0; j < NV; j++)
+            if (j < a.nv)
+#pragma unroll
+                for (int u = 0; u < 2; u++) o[u] = fma(-a.coef[j], a.v[j][I + u * G], o[u]);
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            o[u] *= a.rho;
+            a.out[I + u * G] = o[u];
+            acc[NV] = fma(o[u], o[u], acc[NV]);
+        }
+        // the V_j elements were just read: these loads hit L1
+#pragma unroll
+        for (int j = 0; j < NV; j++)
+            if (j < a.nv)
+#pragma unroll
+                for (int u = 0; u < 2; u++) acc[j] = fma(a.v[j][I + u * G], o[u], acc[j]);
+    }
+    for (; I < N; I += G) {
+        double o = a.a * a.x[I];
+#pragma unroll
+        for (int j = 0; j < NV; j++)
+            if (j < a.nv) o = fma(-a.coef[j], a.v[j][I], o);
+        o *= a.rho;
+        a.out[I] = o;
+        acc[NV] = fma(o, o, acc[NV]);
+#pragma unroll
+        for (int j = 0; j < NV; j++)
+            if (j < a.nv) acc[j] = fma(a.v[j][I], o, acc[j]);
+    }
+    __shared__ double red[kRedThreads / 32][NV + 1];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j <= NV; j++) {
+        if (j < a.nv || j == NV) {
+            double v = acc[j];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) red[warp][j] = v;
+        }
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j <= NV; j += blockDim.x) {
+        if (j < a.nv || j == NV) {
+            double t = 0.0;
+            for (int w = 0; w < kRedThreads / 32; w++) t += red[w][j];
+            partial[(size_t)blockIdx.x * kSlots + (j < NV ? j : kMaxIn)] = t;
+        }
+    }
+}
+
 // out[j] = sum_b partial[b][j] for j < nslots (one block per slot, deterministic order)
 __global__ void k_final_reduce(const double* __restrict__ partial, int nblocks, double* __restrict__ out) {
     const int j = blockIdx.x;
@@ -375,6 +447,31 @@ struct Ops {
             first = false;
         }
     }
+    // out = rho * (a * x - sum_j coef[j] V[j]) with d[j] = V[j] . out and *self = out . out, one
+    // pass (V.size() <= kMaxIn)
+    void orth(const std::vector<const double*>& V, const std::vector<double>& coef, const double* x, double a_x,
+              double rho, double* out, std::vector<double>& d, double* self) {
+        FCIB_CHECK(V.size() <= (size_t)kMaxIn, FCIB_ERR_UNSUPPORTED, "subspace larger than 64 vectors");
+        OrthArgs a;
+        const int nv = (int)V.size();
+        for (int j = 0; j < nv; j++) {
+            a.v[j] = V[j];
+            a.coef[j] = coef[j];
+        }
+        a.x = x;
+        a.out = out;
+        a.a = a_x;
+        a.rho = rho;
+        a.nv = nv;
+        if (nv <= 8) k_orth<8><<<nblk, kRedThreads, 0, c.stream>>>(a, N, partial.p);
+        else if (nv <= 16) k_orth<16><<<nblk, kRedThreads, 0, c.stream>>>(a, N, partial.p);
+        else if (nv <= 32) k_orth<32><<<nblk, kRedThreads, 0, c.stream>>>(a, N, partial.p);
+        else k_orth<64><<<nblk, kRedThreads, 0, c.stream>>>(a, N, partial.p);
+        FCIB_KCHECK();
+        fetch(kMaxIn + 1);
+        d.assign(hout.begin(), hout.begin() + nv);
+        *self = hout[kMaxIn];
+    }
     double norm2(const double* x) {
         std::vector<double> d;
         double s = 0.0;
@@ -446,33 +543,44 @@ struct SparseDev {
 
 // add_row_and_orthonormalize (davidson_liu_solver.cc:634-687): A[rowsA] <- s*src Gram-Schmidt
 // orthonormalised against A[0..rowsA); false if discarded (norm < 1e-7 after projection).
-// Classical Gram-Schmidt with a re-orthogonalisation check, the same thresholds as the
-// reference's modified Gram-Schmidt loop.
+// Classical Gram-Schmidt with the reference's thresholds.  After one dots pass, each projection
+// is one fused pass that also returns the dots of the result with A and its norm (k_orth): the
+// result is scaled by the norm predicted from the dots, and the exact sums decide between
+// accept (orthogonal to 1e-12 and unit norm to 1e-12), discard (projected norm < 1e-7), a
+// corrective projection or a rescale.
 static bool add_row_orth(Ops& ops, std::vector<double*>& A, int rowsA, const double* src, double s = 1.0) {
     double* w = A[rowsA];
     std::vector<const double*> B(A.begin(), A.begin() + rowsA);
     std::vector<double> d;
     double vv = 0.0;
     ops.dots(B, {}, src, nullptr, d, &vv);
-    // first projection reads src and writes w
-    std::vector<const double*> V(B);
-    V.push_back(src);
-    std::vector<std::vector<double>> coef(1, std::vector<double>(rowsA + 1));
-    for (int i = 0; i < rowsA; i++) coef[0][i] = -s * d[i];
-    coef[0][rowsA] = s;
-    auto nn = ops.combo(V, coef, {w}, 0.0);
+    // first projection: w = rho * s * (src - sum d_i B_i), rho from the predicted norm
+    std::vector<double> coef(rowsA);
+    for (int i = 0; i < rowsA; i++) coef[i] = s * d[i];
+    double p2 = vv;
+    for (int i = 0; i < rowsA; i++) p2 -= d[i] * d[i];
+    double rho = (p2 > 0.0 && s != 0.0) ? 1.0 / (std::fabs(s) * std::sqrt(p2)) : 1.0;
+    const double* in = src;
+    double a_in = s;
     for (int cycle = 0; cycle < 10; cycle++) {
-        double nv = std::sqrt(nn[0].first);
-        if (!(nv >= 1.0e-7)) return false;  // also rejects NaN
-        ops.dots(B, {}, w, nullptr, d, &vv);
+        std::vector<double> dw;
+        double ww = 0.0;
+        ops.orth(B, coef, in, a_in, rho, w, dw, &ww);
+        const double nw = std::sqrt(ww);
+        if (!(nw / rho >= 1.0e-7)) return false;  // projected norm (also rejects NaN)
         double mo = 0.0;
-        for (int i = 0; i < rowsA; i++) mo = std::max(mo, std::fabs(d[i] / nv));
-        ops.scale(w, 1.0 / nv);
-        if (mo < 1.0e-12 && std::fabs(vv / (nv * nv) - 1.0) < 1.0e-12) return true;
-        // re-orthogonalise the normalised vector
-        std::vector<std::vector<double>> c2(1, std::vector<double>(rowsA));
-        for (int i = 0; i < rowsA; i++) c2[0][i] = -d[i] / nv;
-        nn = ops.combo(B, c2, {w}, 1.0);
+        for (int i = 0; i < rowsA; i++) mo = std::max(mo, std::fabs(dw[i] / nw));
+        if (mo < 1.0e-12) {
+            if (std::fabs(ww - 1.0) >= 1.0e-12) ops.scale(w, 1.0 / nw);
+            return true;
+        }
+        // re-orthogonalise: w <- (w - sum dw_i B_i) / ||.||, norm predicted from the sums
+        double q2 = ww;
+        for (int i = 0; i < rowsA; i++) q2 -= dw[i] * dw[i];
+        for (int i = 0; i < rowsA; i++) coef[i] = dw[i];
+        in = w;
+        a_in = 1.0;
+        rho = q2 > 0.0 ? 1.0 / std::sqrt(q2) : 1.0 / nw;
     }
     return false;
 }
