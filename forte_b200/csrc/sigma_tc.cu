@@ -250,6 +250,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             *reinterpret_cast<float*>(Bhi + off) = hi;
             if (THREE) *reinterpret_cast<float*>(Blo + off) = lo;
         }
+        fence_proxy_async();  // B (generic-proxy stores) becomes visible to the tensor core's reads
         // A-tile gather: the thread owning tile row m = 32q + lane loads A[m][k] = plane[J_k][jb0 + m]
         // for the 8-column chunks c8 = cg + 4j (coalesced across lanes); one tile ahead in registers
         float gh[kTcGat][8], gl[kTcGat][8];
