@@ -307,32 +307,40 @@ def batch_instances(count, sizes, seed):
     return [(synthetic(int(n), 3 * int(n), seed * 100003 + i), (int(n) + 1) // 2, int(n) // 2) for i, n in enumerate(ns)]
 
 
-def cpu_batch_sample(instances, nroot, budget_s=20.0):
-    """The oracle's Davidson on host cores (one process per core) over the smallest instances of the
-    batch until about budget_s of CPU time is used; returns instances/s and the sample description."""
-    import multiprocessing as mp
-    small = sorted(instances, key=lambda x: x[0].n)
-    cores = max(1, min(os.cpu_count() or 1, 16))
-    t0 = time.perf_counter()
-    done = 0
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(cores) as pool:
-        chunk = small[:cores * 4]
-        res = pool.map(_oracle_solve, [(x[0], x[1], x[2], nroot) for x in chunk])
-        done = len(res)
-    wall = time.perf_counter() - t0
-    sizes = sorted({x[0].n for x in chunk})
-    return done / wall, cores, f"{done} instances of CAS({sizes[0]},{sizes[0]})..CAS({sizes[-1]},{sizes[-1]}), the smallest of the batch, oracle Davidson, {cores} processes"
-
-
-def _oracle_solve(args):
-    ints, na, nb, nroot = args
-    sys.path.insert(0, ROOT)
+def cpu_batch_sample(instances, nroot, iterations):
+    """The oracle's CPU Davidson (numpy, BLAS threads), scaled to the batch: instances of up to 8 orbitals
+    are solved in full (one per size); for larger ones one oracle sigma is timed and multiplied by
+    the sigma builds the batch needed for that size (about nroot per iteration plus the guess).
+    Returns (instances/s for the whole size distribution, BLAS threads used, description)."""
     from oracle.oracle import Oracle
-    o = Oracle(ints.n, na, nb)
-    o.set_integrals(ints)
-    return o.solve(nroot=nroot, multiplicity=0, e_conv=BATCH_OPTS["E_CONVERGENCE"], r_conv=BATCH_OPTS["R_CONVERGENCE"],
-                   maxiter=BATCH_OPTS["DL_MAXITER"])["energies"]
+    sizes = sorted({x[0].n for x in instances})
+    per = {}
+    how = []
+    for n in sizes:
+        ints, na, nb = next(x for x in instances if x[0].n == n)
+        o = Oracle(n, na, nb)
+        o.set_integrals(ints)
+        if n <= 8:
+            t0 = time.perf_counter()
+            o.solve(nroot=nroot, multiplicity=0, e_conv=BATCH_OPTS["E_CONVERGENCE"], r_conv=BATCH_OPTS["R_CONVERGENCE"],
+                    maxiter=BATCH_OPTS["DL_MAXITER"], subspace_per_root=BATCH_OPTS["DL_SUBSPACE_PER_ROOT"],
+                    collapse_per_root=BATCH_OPTS["DL_COLLAPSE_PER_ROOT"])
+            per[n] = time.perf_counter() - t0
+            how.append(f"CAS({n},{n}) solved")
+        else:
+            c = np.random.default_rng(0).normal(size=o.ndet)
+            t0 = time.perf_counter()
+            o.sigma(c)
+            ts = time.perf_counter() - t0
+            its = [it for x, it in zip(instances, iterations) if x[0].n == n]
+            nsig = nroot * float(np.mean(its)) + 2 * nroot
+            per[n] = ts * nsig
+            how.append(f"CAS({n},{n}) one sigma x {nsig:.0f}")
+    total = sum(per[x[0].n] for x in instances)
+    from threadpoolctl import threadpool_info
+    threads = max([d.get("num_threads", 1) for d in threadpool_info()] or [1])
+    return len(instances) / total, threads, f"oracle Davidson ({threads} BLAS threads): " + ", ".join(how) + \
+        f"; summed over the {len(instances)}-instance size distribution"
 
 
 def run_batch(args, world, rank, local):
@@ -367,7 +375,7 @@ def run_batch(args, world, rank, local):
     h2d = sum(sum(getattr(x[0], k).nbytes for k in ("oei_a", "oei_b", "tei_aa", "tei_ab", "tei_bb")) for x in inst)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        v, cores, sample = cpu_batch_sample(inst, 4)
+        v, cores, sample = cpu_batch_sample(inst, 4, it)
         cpu = {"value": v, "unit": "instances/s", "cores": cores, "kind": "port", "sample": sample}
     if rank == 0:
         ndets = [x[0].n for x in inst]
