@@ -201,7 +201,7 @@ def run_sigma(args, world, rank, local):
     torch.cuda.set_device(local)
     n, k = args.n, args.n // 2
     ints = synthetic(n, 3 * n, SEED, gap=GAP)
-    s = FCISolver(StateInfo(k, k, 0), 1, ints, device=local)
+    s = FCISolver(StateInfo(k, k, 0), 1, ints, {"FCI_SAME_SPIN": args.same_spin}, device=local)
     N = s.size()
     g = torch.Generator(device="cuda").manual_seed(0)
     b = torch.randn(N, dtype=torch.float64, device="cuda", generator=g)
@@ -251,7 +251,7 @@ def run_sigma(args, world, rank, local):
             "dtype": {"FP64": "f64", "MIXED": "tf32x3/f32", "MIXED_TF32": "tf32/f32"}[args.precision],
             "data": "synthetic",
             "config": {"workload": f"sigma of a random unit vector, CAS({n},{n}) synthetic L={3 * n} Ms=0",
-                       "n_det": N, "precision": args.precision,
+                       "n_det": N, "precision": args.precision, "same_spin": args.same_spin,
                        "l2": f"vectors of {N * 8 / 1e9:.2f} GB" + (" (> L2)" if N * 8 > 126e6 else " (fit in L2)")},
             "roofline": roofline, "gpu_launches": int(launches / args.steps),
             "sigma_profile_ms": {"opposite_spin": ((p1["ab_ms"] - p0["ab_ms"]) + (p1["ab64_ms"] - p0["ab64_ms"])) / args.steps,
@@ -272,7 +272,7 @@ def run_precond(args, world, rank, local):
     n = args.n if args.n != 16 else 14
     ints = synthetic(n, 3 * n, SEED)
     opts = {"DL_SUBSPACE_PER_ROOT": 8, "DL_COLLAPSE_PER_ROOT": 2, "DL_MAXITER": 300, "E_CONVERGENCE": 1e-9,
-            "R_CONVERGENCE": 1e-5, "FCI_PRECISION": args.precision}
+            "R_CONVERGENCE": 1e-5, "FCI_PRECISION": args.precision, "FCI_SAME_SPIN": args.same_spin}
     out = {}
     for pre in ("DIAG", "MLP"):
         s = FCISolver(StateInfo(n // 2, n // 2, 0), 2, ints, dict(opts, FCI_PRECONDITIONER=pre), device=local)
@@ -308,10 +308,11 @@ def batch_instances(count, sizes, seed):
 
 
 def cpu_batch_sample(instances, nroot, iterations):
-    """The oracle's CPU Davidson (numpy, BLAS threads), scaled to the batch: instances of up to 8 orbitals
+    """The oracle's CPU Davidson (single-threaded C), scaled to the batch: instances of up to 8 orbitals
     are solved in full (one per size); for larger ones one oracle sigma is timed and multiplied by
     the sigma builds the batch needed for that size (about nroot per iteration plus the guess).
-    Returns (instances/s for the whole size distribution, BLAS threads used, description)."""
+    Returns (instances/s on one core for the whole size distribution, description).  Instances are
+    independent, so a host with P free cores would reach at most P times this."""
     from oracle.oracle import Oracle
     sizes = sorted({x[0].n for x in instances})
     per = {}
@@ -337,9 +338,7 @@ def cpu_batch_sample(instances, nroot, iterations):
             per[n] = ts * nsig
             how.append(f"CAS({n},{n}) one sigma x {nsig:.0f}")
     total = sum(per[x[0].n] for x in instances)
-    from threadpoolctl import threadpool_info
-    threads = max([d.get("num_threads", 1) for d in threadpool_info()] or [1])
-    return len(instances) / total, threads, f"oracle Davidson ({threads} BLAS threads): " + ", ".join(how) + \
+    return len(instances) / total, "oracle Davidson on 1 core: " + ", ".join(how) + \
         f"; summed over the {len(instances)}-instance size distribution"
 
 
@@ -375,8 +374,8 @@ def run_batch(args, world, rank, local):
     h2d = sum(sum(getattr(x[0], k).nbytes for k in ("oei_a", "oei_b", "tei_aa", "tei_ab", "tei_bb")) for x in inst)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        v, cores, sample = cpu_batch_sample(inst, 4, it)
-        cpu = {"value": v, "unit": "instances/s", "cores": cores, "kind": "port", "sample": sample}
+        v, sample = cpu_batch_sample(inst, 4, it)
+        cpu = {"value": v, "unit": "instances/s", "cores": 1, "kind": "port", "sample": sample}
     if rank == 0:
         ndets = [x[0].n for x in inst]
         print(json.dumps({
@@ -405,6 +404,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="MIXED", choices=["MIXED", "MIXED_TF32", "FP64"])
     ap.add_argument("--preconditioner", default="DIAG", choices=["DIAG", "MLP"])
+    ap.add_argument("--same-spin", default="TC", choices=["TC", "CUDA_CORES"],
+                    help="mixed same-spin kernel: tensor cores (3xTF32) or FP32 CUDA cores")
     ap.add_argument("--ref-iterations", type=int, default=53, help="FP64 iteration count used by the CPU arm")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparator solve")
     ap.add_argument("--no-e2e", action="store_true")
@@ -454,7 +455,8 @@ def main():
         del f
         torch.cuda.empty_cache()
 
-    opts = dict(OPTS, FCI_PRECISION=args.precision, FCI_PRECONDITIONER=args.preconditioner)
+    opts = dict(OPTS, FCI_PRECISION=args.precision, FCI_PRECONDITIONER=args.preconditioner,
+                FCI_SAME_SPIN=args.same_spin)
     s = FCISolver(state, 1, ints, opts, device=local)
     stream = torch.cuda.ExternalStream(s.stream())
     for _ in range(args.warmup):
@@ -536,6 +538,7 @@ def main():
             "data": "synthetic",
             "config": {"workload": "CAS(16,16) synthetic L=48 gap=0.3 Ms=0 1 root subspace 8", "n_orb": N_ORB,
                        "n_det": ndet, "precision": args.precision, "preconditioner": args.preconditioner,
+                       "same_spin": args.same_spin,
                        "e_convergence": OPTS["E_CONVERGENCE"], "r_convergence": OPTS["R_CONVERGENCE"],
                        "l2": "inputs larger than L2 (1.3 GB CI vectors)", "parallelism": f"replicas x{world}"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches / max(1, args.steps)),

@@ -28,6 +28,8 @@ PREC_MIXED = 1
 PREC_MIXED_TF32 = 2
 PRECOND_DIAG = 0
 PRECOND_MLP = 1
+SAME_TC = 0
+SAME_CUDA_CORES = 1
 
 
 class FcibOptions(C.Structure):
@@ -44,6 +46,7 @@ class FcibOptions(C.Structure):
         ("precision", C.c_int),
         ("preconditioner", C.c_int),
         ("mixed_switch", C.c_double),
+        ("same_spin_kernel", C.c_int),
     ]
 
 

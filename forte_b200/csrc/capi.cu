@@ -169,6 +169,7 @@ void fcib_default_options(fcib_options* o) {
     o->precision = FCIB_PREC_FP64;
     o->preconditioner = FCIB_PRECOND_DIAG;
     o->mixed_switch = 1.0e-4;
+    o->same_spin_kernel = FCIB_SAME_TC;
 }
 
 const char* fcib_last_error(void) { return g_last_error.c_str(); }
@@ -301,6 +302,8 @@ int fcib_set_options(fcib_ctx* ctx, const fcib_options* o) {
         FCIB_CHECK(o->precision >= FCIB_PREC_FP64 && o->precision <= FCIB_PREC_MIXED_TF32, FCIB_ERR_ARG, "bad precision mode");
         FCIB_CHECK(o->preconditioner == FCIB_PRECOND_DIAG || o->preconditioner == FCIB_PRECOND_MLP, FCIB_ERR_ARG,
                    "bad preconditioner");
+        FCIB_CHECK(o->same_spin_kernel == FCIB_SAME_TC || o->same_spin_kernel == FCIB_SAME_CUDA_CORES, FCIB_ERR_ARG,
+                   "bad same-spin kernel");
         ctx->c.opt = *o;
     });
 }

@@ -3,6 +3,7 @@
 #include "strings.cu"
 #include "sigma.cu"
 #include "sigma_tc.cu"
+#include "sigma_same_tc.cu"
 #include "davidson.cu"
 #include "rdms.cu"
 #include "capi.cu"

@@ -195,6 +195,13 @@ struct Context {
     std::vector<double> cap_lambda;  // iteration, ms, lambda_0, max residual, fp64 basis
 };
 
+// the work counters and error flags of the persistent kernels, zeroed when first allocated
+inline void ensure_counter(Context& c) {
+    if (c.counter.p) return;
+    c.counter.alloc(16);
+    FCIB_CUDA(cudaMemsetAsync(c.counter.p, 0, 16 * sizeof(int), c.stream));
+}
+
 // kernels / launchers (sigma.cu)
 void prepare_integrals(Context& c);
 void sigma_fp64(Context& c, const double* C, double* S);

@@ -314,7 +314,7 @@ static void launch_group_t(Context& c, const T* C, T* S, int ncols, int ngroups,
     int nchunks = (ncols + kGrTN - 1) / kGrTN;
     int per_sm = std::max(1, std::min((int)(c.smem_per_sm / (smem + 1024)), 2048 / threads));
     int grid = std::min(ngroups * nchunks, per_sm * c.num_sms);
-    if (!c.counter.p) c.counter.alloc(16);
+    ensure_counter(c);
     FCIB_CUDA(cudaMemsetAsync(c.counter.p + 2, 0, sizeof(int), c.stream));
     k_group<T><<<grid, threads, smem, c.stream>>>(C, S, ncols, rows, labs, G, Gp, M, ldm, ngroups, nchunks, c.counter.p + 2, m_in_smem);
     FCIB_KCHECK();
@@ -438,6 +438,17 @@ void apply_mask(Context& c, double* v) {
 // ------------------------------------------------------------------------------------------
 // sigma orchestration
 // ------------------------------------------------------------------------------------------
+bool launch_group_tc(Context& c, const float* C, float* S, int ncols, int ngroups, int G, const uint32_t* rows,
+                     const uint16_t* labs, const double* M, int ldm);
+
+// mixed same-spin two-body groups: tensor cores unless disabled or the groups are too large
+static void launch_group_same_f32(Context& c, const float* C, float* S, int ncols, int ngroups, int G,
+                                  const uint32_t* rows, const uint16_t* labs, const double* M, int ldm) {
+    if (c.opt.same_spin_kernel == FCIB_SAME_TC && launch_group_tc(c, C, S, ncols, ngroups, G, rows, labs, M, ldm))
+        return;
+    launch_group(c, C, S, ncols, ngroups, G, rows, labs, M, ldm);
+}
+
 // same-spin (and, when not folded into the opposite-spin block, one-body) terms added to S
 static void sigma_same_spin(Context& c, const double* C, double* S, bool fp32) {
     const int nas = (int)c.nas, nbs = (int)c.nbs;
@@ -467,19 +478,21 @@ static void sigma_same_spin(Context& c, const double* C, double* S, bool fp32) {
         FCIB_KCHECK();
     }
     c.c32_ready = false;
+    ensure_counter(c);
+    FCIB_CUDA(cudaMemsetAsync(c.counter.p + 5, 0, sizeof(int), c.stream));  // tensor-core group timeout flag
     c.s32a.alloc(N);
     c.st32.alloc(N);
     FCIB_CUDA(cudaMemsetAsync(c.s32a.p, 0, N * sizeof(float), c.stream));
     FCIB_CUDA(cudaMemsetAsync(c.st32.p, 0, N * sizeof(float), c.stream));
     if (a_g1) launch_group(c, c.c32.p, c.s32a.p, nbs, c.A.ng1, c.A.g1, c.A.g1row.p, c.A.g1lab.p, c.Ha.p, c.n);
-    if (c.A.ng2) launch_group(c, c.c32.p, c.s32a.p, nbs, c.A.ng2, c.A.g2, c.A.g2row.p, c.A.g2lab.p, c.M2a.p, np2);
+    if (c.A.ng2) launch_group_same_f32(c, c.c32.p, c.s32a.p, nbs, c.A.ng2, c.A.g2, c.A.g2row.p, c.A.g2lab.p, c.M2a.p, np2);
     if (any_b) {
         c.ct32.alloc(N);
         dim3 grid((nbs + 31) / 32, (nas + 31) / 32), block(32, 8);
         k_transpose_f32<<<grid, block, 0, c.stream>>>(c.c32.p, c.ct32.p, nas, nbs);
         FCIB_KCHECK();
         if (b_g1) launch_group(c, c.ct32.p, c.st32.p, nas, c.B.ng1, c.B.g1, c.B.g1row.p, c.B.g1lab.p, c.Hb.p, c.n);
-        if (c.B.ng2) launch_group(c, c.ct32.p, c.st32.p, nas, c.B.ng2, c.B.g2, c.B.g2row.p, c.B.g2lab.p, c.M2b.p, np2);
+        if (c.B.ng2) launch_group_same_f32(c, c.ct32.p, c.st32.p, nas, c.B.ng2, c.B.g2, c.B.g2row.p, c.B.g2lab.p, c.M2b.p, np2);
     }
     dim3 grid2((nas + 31) / 32, (nbs + 31) / 32), block2(32, 8);
     k_add_same_f32<<<grid2, block2, 0, c.stream>>>(S, c.s32a.p, c.st32.p, nas, nbs);
@@ -517,7 +530,7 @@ static void sigma_timing(Context& c, SigmaEvents& ev, bool fp64) {
 void sigma_fp64(Context& c, const double* C, double* S) {
     const int nas = (int)c.nas, nbs = (int)c.nbs;
     const size_t N = (size_t)c.ndet;
-    if (!c.counter.p) c.counter.alloc(16);
+    ensure_counter(c);
     SigmaEvents ev;
     FCIB_CUDA(cudaEventRecord(ev.e[0], c.stream));
     if (c.fold_h) {
@@ -548,7 +561,7 @@ void sigma_fp64(Context& c, const double* C, double* S) {
 }
 
 void ab_tc(Context& c, const double* C, double* S, bool three);
-int tc_check_error(Context& c);
+int tc_check_error(Context& c, bool opposite_spin);
 
 void sigma_mixed(Context& c, const double* C, double* S, bool three) {
     const size_t N = (size_t)c.ndet;
@@ -565,10 +578,8 @@ void sigma_mixed(Context& c, const double* C, double* S, bool three) {
     FCIB_CUDA(cudaEventRecord(ev.e[2], c.stream));
     sigma_timing(c, ev, false);
     apply_mask(c, S);
-    if (c.fold_h) {
-        int e = tc_check_error(c);
-        FCIB_CHECK(e == 0, FCIB_ERR_NUMERIC, "tensor-core sigma kernel reported a timeout (code " + std::to_string(e) + ")");
-    }
+    const int e = tc_check_error(c, c.fold_h);
+    FCIB_CHECK(e == 0, FCIB_ERR_NUMERIC, "tensor-core sigma kernel reported a timeout (code " + std::to_string(e) + ")");
 }
 
 // ------------------------------------------------------------------------------------------

@@ -467,7 +467,7 @@ void ab_tc(Context& c, const double* C, double* S, bool three) {
     }
     const int ldp = (nbs + 3) / 4 * 4;
     c.tf_hi.alloc(2 * (size_t)nas * ldp);  // interleaved hi/lo pairs
-    if (!c.counter.p) c.counter.alloc(16);
+    ensure_counter(c);
     FCIB_CUDA(cudaMemsetAsync(c.counter.p, 0, 3 * sizeof(int), c.stream));
     unsigned int* cmax_bits = reinterpret_cast<unsigned int*>(c.counter.p + 3);
     FCIB_CUDA(cudaMemsetAsync(cmax_bits, 0, sizeof(unsigned int), c.stream));
@@ -490,11 +490,15 @@ void ab_tc(Context& c, const double* C, double* S, bool three) {
     c.tc_recorded = true;
 }
 
-int tc_check_error(Context& c) {
-    int e = 0;
-    FCIB_CUDA(cudaMemcpyAsync(&e, c.counter.p + 1, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+// timeout flags of one mixed sigma: slot 1 (opposite-spin kernel, when it ran) and slot 5
+// (tensor-core same-spin groups, cleared at the start of every mixed same-spin term)
+int tc_check_error(Context& c, bool opposite_spin) {
+    if (!c.counter.p) return 0;
+    int h[6] = {0, 0, 0, 0, 0, 0};
+    FCIB_CUDA(cudaMemcpyAsync(h, c.counter.p, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
     FCIB_CUDA(cudaStreamSynchronize(c.stream));
-    return e;
+    if (opposite_spin && h[1]) return h[1];
+    return h[5];
 }
 
 }  // namespace fcib

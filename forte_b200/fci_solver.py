@@ -43,6 +43,7 @@ DEFAULT_OPTIONS = {
     "FCI_PRECISION": "FP64",        # FP64 | MIXED | MIXED_TF32
     "FCI_PRECONDITIONER": "DIAG",   # DIAG | MLP
     "FCI_MIXED_SWITCH": 1.0e-4,
+    "FCI_SAME_SPIN": "TC",          # TC | CUDA_CORES (mixed modes)
 }
 
 
@@ -117,6 +118,7 @@ class FCISolver:
                        "MIXED_TF32": capi.PREC_MIXED_TF32}[str(d["FCI_PRECISION"]).upper()]
         o.preconditioner = {"DIAG": capi.PRECOND_DIAG, "MLP": capi.PRECOND_MLP}[str(d["FCI_PRECONDITIONER"]).upper()]
         o.mixed_switch = float(d["FCI_MIXED_SWITCH"])
+        o.same_spin_kernel = {"TC": capi.SAME_TC, "CUDA_CORES": capi.SAME_CUDA_CORES}[str(d["FCI_SAME_SPIN"]).upper()]
         if o.preconditioner == capi.PRECOND_MLP and getattr(self, "_mlp", None) is None:
             from .learned_precond import load_weights
             self.set_mlp_weights(load_weights())

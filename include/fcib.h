@@ -51,6 +51,8 @@ extern "C" {
 /* Davidson correction-vector preconditioner */
 #define FCIB_PRECOND_DIAG 0    /* r_I / (lambda - H_II), the reference's */
 #define FCIB_PRECOND_MLP 1     /* learned per-determinant MLP correction on top of the diagonal */
+#define FCIB_SAME_TC 0         /* mixed same-spin term on the tensor cores (groups of <= 64 strings) */
+#define FCIB_SAME_CUDA_CORES 1 /* mixed same-spin term in FP32 on the CUDA cores */
 
 typedef struct fcib_options {
     int maxiter;               /* DL_MAXITER (default 100) */
@@ -65,6 +67,7 @@ typedef struct fcib_options {
     int precision;             /* FCIB_PREC_* */
     int preconditioner;        /* FCIB_PRECOND_* */
     double mixed_switch;       /* mixed modes: residual norm at which sigma switches to FP64 */
+    int same_spin_kernel;      /* mixed modes: FCIB_SAME_TC (default) or FCIB_SAME_CUDA_CORES */
 } fcib_options;
 
 typedef struct fcib_ctx fcib_ctx;

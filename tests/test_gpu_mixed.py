@@ -63,3 +63,36 @@ def test_mixed_golden_fcidump(k):
     s = FCISolver(StateInfo(na, nb, mult, na - nb, irrep), 1, ints,
                   {"E_CONVERGENCE": 1e-10, "R_CONVERGENCE": 1e-6, "FCI_PRECISION": "MIXED"})
     assert abs(s.compute_energy() - ref) < 1e-8
+
+
+@pytest.mark.parametrize("n,na,nb,oracle", [(8, 4, 4, True), (9, 3, 5, True), (12, 2, 3, True), (11, 5, 4, True),
+                                            (10, 9, 2, True), (14, 7, 7, False)])
+def test_same_spin_tensor_cores_match_cuda_cores(n, na, nb, oracle):
+    """Mixed sigma with the same-spin groups on the tensor cores (3xTF32, FCI_SAME_SPIN=TC) against
+    the FP32 CUDA-core groups and, where the oracle is quick, the FP64 oracle.  Group sizes
+    C(n-k+2, 2), alpha / beta: (8,4,4) 15; (9,3,5) 28 / 15; (11,5,4) 28 / 36; (10,9,2) 3 / 45;
+    (14,7,7) 36.  In (12,2,3)
+    the alpha groups hold C(12,2) = 66 strings, more than the tensor-core layout takes, so that
+    spin runs on the CUDA cores while beta (55 strings) runs on the tensor cores."""
+    ints = synthetic(n, 3 * n, 23)
+    rng = np.random.default_rng(11 * n + nb)
+    got = {}
+    for kern in ("TC", "CUDA_CORES"):
+        s = FCISolver(StateInfo(na, nb, 0, na - nb), 1, ints, {"FCI_PRECISION": "MIXED", "FCI_SAME_SPIN": kern})
+        if kern == "TC":
+            c = rng.normal(size=s.size())
+            c /= np.linalg.norm(c)
+        got[kern] = s.sigma(c)
+    scale = np.max(np.abs(got["CUDA_CORES"]))
+    assert np.max(np.abs(got["TC"] - got["CUDA_CORES"])) / scale < TOL_MIXED
+    if oracle:
+        o = Oracle(n, na, nb)
+        o.set_integrals(ints)
+        ref = o.sigma(c)
+        assert np.max(np.abs(got["TC"] - ref)) / np.max(np.abs(ref)) < TOL_MIXED
+
+
+def test_same_spin_kernel_option_is_checked():
+    ints = synthetic(6, 18, 1)
+    with pytest.raises(KeyError):
+        FCISolver(StateInfo(3, 3, 0), 1, ints, {"FCI_SAME_SPIN": "BOTH"})
