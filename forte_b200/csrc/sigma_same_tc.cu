@@ -5,8 +5,8 @@
 //     sigma[I_i][col] += sum_j s_i s_j M[lab_i][lab_j] C[I_j][col]      for every column col.
 // Per group this is one small dense product, mapped onto tcgen05 as
 //     D[col][i] = sum_j X[col][j] W[i][j],   X[col][j] = C[I_j][col],   W[i][j] = s_i s_j M[lab_i][lab_j]
-// with 128 columns per tile in the MMA's M dimension (one TMEM lane per column), N = G padded to 16
-// and K = G padded to 8:
+// with 128 columns per tile in the MMA's M dimension (one TMEM lane per column) and N = K = G
+// padded to a multiple of 16:
 // * a CTA takes a whole group (dynamic counter) and sweeps its 128-column tiles; W is split into
 //   TF32 hi/lo planes in shared memory once per group (K-major, no swizzle);
 // * the gathered tile X (the FP32 copy of C, coalesced across lanes) is split into TF32 hi/lo in
@@ -26,23 +26,25 @@
 namespace fcib {
 
 constexpr int kGtM = 128;             // columns per tile (MMA M, TMEM lanes)
-constexpr int kGtThreads = 256;       // 8 warps: lane quarter q = warp % 4, column group warp / 4
+constexpr int kGtThreads = 512;       // 16 warps: lane quarter q = warp % 4, column group cg = warp / 4
 constexpr uint32_t kGtTmemCols = 256; // two CTAs per SM
 constexpr uint32_t kGtColAcc = 64, kGtColAhi = 128, kGtColAlo = 192;  // accumulators at 0 and 64
 constexpr int kGtMaxG = 64;
-constexpr int kGtChunks = 4;          // 8-column chunks per thread: at most 8 chunks over 2 column groups
 constexpr int kErrTimeoutGroupMma = 2;
+constexpr uint32_t kGtNoRow = 0xFFFFFFFFu;
 
+// K (source strings) and N (target strings) are both G padded to P = 16 Q; thread (q, lane, cg)
+// owns column c0 + 32 q + lane and the Q quads of strings 4 (cg + 4 i) .. +3, i < Q, for the
+// gather and the epilogue alike
 struct GtLayout {
-    int kp, np;  // K (source strings) padded to 8, N (target strings) padded to 16
+    int P;
     uint32_t b_bytes, off_bhi, off_blo, off_rows, off_labs, off_bar, total;
 };
 
 __host__ __device__ inline GtLayout gt_layout(int G) {
     GtLayout L;
-    L.kp = (G + 7) / 8 * 8;
-    L.np = (G + 15) / 16 * 16;
-    L.b_bytes = (uint32_t)L.np * L.kp * 4;  // a multiple of 512 bytes
+    L.P = (G + 15) / 16 * 16;
+    L.b_bytes = (uint32_t)L.P * L.P * 4;  // a multiple of 1 KB
     uint32_t o = 0;
     L.off_bhi = o; o += L.b_bytes;
     L.off_blo = o; o += L.b_bytes;
@@ -54,6 +56,24 @@ __host__ __device__ inline GtLayout gt_layout(int G) {
     return L;
 }
 
+__device__ __forceinline__ void tmem_st4(uint32_t taddr, const float (&v)[4]) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1,%2,%3,%4};" ::"r"(taddr), "r"(__float_as_uint(v[0])),
+                 "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])), "r"(__float_as_uint(v[3]))
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_ld4_async(uint32_t taddr, uint32_t (&r)[4]) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld4(uint32_t (&r)[4]) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;" : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3])::"memory");
+}
+__device__ __forceinline__ void reg_after4(uint32_t (&r)[4]) {
+    asm volatile("" : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]));
+}
+
+template <int Q>
 __global__ void __launch_bounds__(kGtThreads, 2)
     k_group_tc(const float* __restrict__ C, float* __restrict__ S, int ncols, const uint32_t* __restrict__ rows,
                const uint16_t* __restrict__ labs, int G, const double* __restrict__ M, int ldm, int ngroups,
@@ -72,7 +92,7 @@ __global__ void __launch_bounds__(kGtThreads, 2)
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
     const int q = warp & 3, cg = warp >> 2;
-    const int kp = L.kp, np = L.np, nk8 = kp / 8, nn8 = np / 8;
+    constexpr int P = 16 * Q;
 
     if (tid == 0) {
         mbar_init(&bars[0], 1);
@@ -92,9 +112,9 @@ __global__ void __launch_bounds__(kGtThreads, 2)
     const uint32_t tmem_base = *tmem_slot;
     const uint32_t tlane = (uint32_t)(32 * q) << 16;
 
-    // instruction descriptor: D f32, A/B tf32, both K-major, N = np, M = 128
-    const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(np >> 3) << 17) | ((uint32_t)(kGtM >> 4) << 24);
-    const uint32_t lbo_b = (uint32_t)(np / 8) * 128;
+    // instruction descriptor: D f32, A/B tf32, both K-major, N = P, M = 128
+    const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(P >> 3) << 17) | ((uint32_t)(kGtM >> 4) << 24);
+    const uint32_t lbo_b = (uint32_t)(P / 8) * 128;
     const uint32_t sb_hi = smem_u32(Bhi), sb_lo = smem_u32(Blo);
 
     uint32_t mma_count[2] = {0u, 0u};  // commits issued per accumulator (parity tracking)
@@ -111,8 +131,8 @@ __global__ void __launch_bounds__(kGtThreads, 2)
         }
         __syncthreads();
         // W[i][j] = s_i s_j M[lab_i][lab_j], split into tf32 hi/lo (zero outside G x G)
-        for (int idx = tid; idx < np * kp; idx += blockDim.x) {
-            const int i = idx / kp, j = idx - i * kp;
+        for (int idx = tid; idx < P * P; idx += blockDim.x) {
+            const int i = idx / P, j = idx - i * P;
             float hi = 0.f, lo = 0.f;
             if (i < G && j < G) {
                 double v = M[(size_t)ls[i] * ldm + ls[j]];
@@ -120,27 +140,30 @@ __global__ void __launch_bounds__(kGtThreads, 2)
                 hi = __uint_as_float(to_tf32((float)v));
                 lo = __uint_as_float(to_tf32((float)(v - (double)hi)));
             }
-            const uint32_t off = kmaj_off(i, j, np);
+            const uint32_t off = kmaj_off(i, j, P);
             *reinterpret_cast<float*>(Bhi + off) = hi;
             *reinterpret_cast<float*>(Blo + off) = lo;
         }
         fence_proxy_async();  // W (generic-proxy stores) becomes visible to the tensor core's reads
-        // X-tile gather: the thread owning tile row m = 32q + lane (column c0 + m) loads the source
-        // strings j of its 8-column chunks c8 = cg + 2 jj; one tile ahead in registers
-        float xv[kGtChunks][8];
+        // row offsets (string index * ncols) of this thread's quads, shared by gather and epilogue
+        uint32_t off[Q][4];
+#pragma unroll
+        for (int i = 0; i < Q; i++)
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int j = 4 * (cg + 4 * i) + u;
+                off[i][u] = j < G ? (rs[j] & kConnIdxMask) * (uint32_t)ncols : kGtNoRow;
+            }
+        // X-tile gather, one tile ahead in registers (coalesced across lanes)
+        float xv[Q][4];
         auto prefetch = [&](int tt) {
             const int col = tt * kGtM + 32 * q + lane;
+            const bool in = col < ncols;
 #pragma unroll
-            for (int jj = 0; jj < kGtChunks; jj++) {
-                const int c8 = cg + 2 * jj;
+            for (int i = 0; i < Q; i++)
 #pragma unroll
-                for (int u = 0; u < 8; u++) {
-                    const int j = 8 * c8 + u;
-                    float x = 0.f;
-                    if (c8 < nk8 && j < G && col < ncols) x = __ldg(C + (size_t)(rs[j] & kConnIdxMask) * ncols + col);
-                    xv[jj][u] = x;
-                }
-            }
+                for (int u = 0; u < 4; u++)
+                    xv[i][u] = (in && off[i][u] != kGtNoRow) ? __ldg(C + (size_t)(off[i][u] + (uint32_t)col)) : 0.f;
         };
         prefetch(0);
         for (int t = 0; t <= ntiles; t++) {
@@ -158,18 +181,16 @@ __global__ void __launch_bounds__(kGtThreads, 2)
             // (b) registers -> X hi/lo in tensor memory
             if (t < ntiles) {
 #pragma unroll
-                for (int jj = 0; jj < kGtChunks; jj++) {
-                    const int c8 = cg + 2 * jj;
-                    if (c8 < nk8) {
-                        float h[8], l[8];
+                for (int i = 0; i < Q; i++) {
+                    float h[4], l[4];
 #pragma unroll
-                        for (int u = 0; u < 8; u++) {
-                            h[u] = __uint_as_float(to_tf32(xv[jj][u]));
-                            l[u] = __uint_as_float(to_tf32(xv[jj][u] - h[u]));
-                        }
-                        tmem_st8(tmem_base + tlane + kGtColAhi + 8 * c8, h);
-                        tmem_st8(tmem_base + tlane + kGtColAlo + 8 * c8, l);
+                    for (int u = 0; u < 4; u++) {
+                        h[u] = __uint_as_float(to_tf32(xv[i][u]));
+                        l[u] = __uint_as_float(to_tf32(xv[i][u] - h[u]));
                     }
+                    const uint32_t c4 = 4 * (uint32_t)(cg + 4 * i);
+                    tmem_st4(tmem_base + tlane + kGtColAhi + c4, h);
+                    tmem_st4(tmem_base + tlane + kGtColAlo + c4, l);
                 }
                 asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
             }
@@ -180,7 +201,8 @@ __global__ void __launch_bounds__(kGtThreads, 2)
             if (t < ntiles && tid == 0) {
                 const uint32_t dt = tmem_base + (uint32_t)cur * kGtColAcc;
                 uint32_t acc = 0;
-                for (int ks = 0; ks < nk8; ks++) {
+#pragma unroll
+                for (int ks = 0; ks < P / 8; ks++) {
                     const uint32_t ah = tmem_base + kGtColAhi + 8 * ks;
                     const uint32_t al = tmem_base + kGtColAlo + 8 * ks;
                     const uint64_t bh = make_desc(sb_hi + ks * 2 * lbo_b, lbo_b, 128);
@@ -198,29 +220,20 @@ __global__ void __launch_bounds__(kGtThreads, 2)
             // (d) epilogue of tile t-1: reductions into the FP32 sigma buffer
             if (t >= 1) {
                 const uint32_t tbase = tmem_base + (uint32_t)prv * kGtColAcc + tlane;
-                uint32_t rv[kGtChunks][8];
+                uint32_t rv[Q][4];
 #pragma unroll
-                for (int i = 0; i < kGtChunks; i++) {
-                    const int c8 = cg + 2 * i;
-                    if (c8 < nn8) tmem_ld8_async(tbase + (uint32_t)(c8 * 8), rv[i]);
-                }
-                tmem_wait_ld8(rv[0]);
+                for (int i = 0; i < Q; i++) tmem_ld4_async(tbase + 4 * (uint32_t)(cg + 4 * i), rv[i]);
+                tmem_wait_ld4(rv[0]);
 #pragma unroll
-                for (int i = 1; i < kGtChunks; i++) reg_after(rv[i]);
+                for (int i = 1; i < Q; i++) reg_after4(rv[i]);
                 const int col = (t - 1) * kGtM + 32 * q + lane;
                 if (col < ncols) {
 #pragma unroll
-                    for (int i = 0; i < kGtChunks; i++) {
-                        const int c8 = cg + 2 * i;
-                        if (c8 < nn8) {
+                    for (int i = 0; i < Q; i++)
 #pragma unroll
-                            for (int u = 0; u < 8; u++) {
-                                const int r = 8 * c8 + u;
-                                if (r < G)
-                                    atomicAdd(S + (size_t)(rs[r] & kConnIdxMask) * ncols + col, __uint_as_float(rv[i][u]));
-                            }
-                        }
-                    }
+                        for (int u = 0; u < 4; u++)
+                            if (off[i][u] != kGtNoRow)
+                                atomicAdd(S + (size_t)(off[i][u] + (uint32_t)col), __uint_as_float(rv[i][u]));
                 }
                 tc_fence_before();
             }
@@ -243,23 +256,25 @@ __global__ void __launch_bounds__(kGtThreads, 2)
 }
 
 // Same-spin groups of FP32 sigma on the tensor cores.  Returns false (nothing launched) when the
-// groups are too large for the kernel's tensor-memory layout; the caller then uses k_group<float>.
-// The group counter and the timeout flag live in counter slots 4 and 5; the flag is cleared by
-// the caller once per sigma and read back by tc_check_error.
+// groups are too large for the kernel's tensor-memory layout or the vectors too long for its
+// 32-bit element offsets; the caller then uses k_group<float>.  The group counter and the timeout
+// flag live in counter slots 4 and 5; the flag is cleared by the caller once per sigma and read
+// back by tc_check_error.
 bool launch_group_tc(Context& c, const float* C, float* S, int ncols, int ngroups, int G, const uint32_t* rows,
                      const uint16_t* labs, const double* M, int ldm) {
-    if (G < 1 || G > kGtMaxG) return false;
+    if (G < 1 || G > kGtMaxG || (uint64_t)c.nas * (uint64_t)c.nbs >= (1ull << 32) - kGtM) return false;
     if (ngroups == 0) return true;
     const GtLayout L = gt_layout(G);
     // at least 80 KB so that no more than two CTAs (2 x 256 TMEM columns) share an SM
     const size_t smem = std::max<size_t>(L.total, 80 * 1024);
     if (smem + 1024 > (size_t)c.smem_optin) return false;
-    FCIB_CUDA(cudaFuncSetAttribute(k_group_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    auto kern = L.P == 16 ? k_group_tc<1> : L.P == 32 ? k_group_tc<2> : L.P == 48 ? k_group_tc<3> : k_group_tc<4>;
+    FCIB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     ensure_counter(c);
     FCIB_CUDA(cudaMemsetAsync(c.counter.p + 4, 0, sizeof(int), c.stream));
     const int grid = std::min(ngroups, 2 * c.num_sms);
-    k_group_tc<<<grid, kGtThreads, smem, c.stream>>>(C, S, ncols, rows, labs, G, M, ldm, ngroups, c.counter.p + 4,
-                                                     c.counter.p + 5);
+    kern<<<grid, kGtThreads, smem, c.stream>>>(C, S, ncols, rows, labs, G, M, ldm, ngroups, c.counter.p + 4,
+                                               c.counter.p + 5);
     FCIB_KCHECK();
     return true;
 }
