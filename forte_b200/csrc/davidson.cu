@@ -720,69 +720,105 @@ void dl_solve(Context& c) {
     c.n_ab64 = 0;
     c.trace.clear();
 
-    // ---- initial guess ----
+    // ---- initial guess, or restart from the previous solution ----
+    // FCISolver::compute_energy (fci_solver.cc:205-233) keeps its Davidson-Liu solver between
+    // calls and resets it with a fresh guess only on the first run or when the guess space
+    // covers the whole space; otherwise DavidsonLiuSolver::setup_guesses (davidson_liu_solver.cc:
+    // 312-316) restarts from the first nroot vectors, recomputing their sigma with the current
+    // integrals, and keeps projecting out the first run's unwanted roots.
     int num_guess_states = (int)std::min<int64_t>((int64_t)o.guess_per_root * nroot, Neff);
+    std::vector<int64_t> space = {c.n, c.na, c.nb, c.irrep, c.nirrep, (int64_t)N, Neff, nroot, m};
+    for (int x : c.orbsym) space.push_back(x);
+    const bool restart = c.dl_prev && c.dl_prev_space == space &&
+                         (int64_t)num_guess_states * o.dets_per_guess < Neff;
+    c.dl_prev = false;  // set again when this solve completes
+    if (restart) {
+        if (o.print) printf("\n  Davidson-Liu solver: restarting from previous calculation.\n");
+        c.restarted = true;
+    } else {
+        c.restarted = false;
+    }
     int ng = (int)std::min<int64_t>((int64_t)num_guess_states * o.dets_per_guess, Neff);
     double t_guess0 = now_ms();
-    auto lowest = lowest_diagonal(c, ng);
-    std::vector<uint32_t> sa(c.nas), sbv(c.nbs);
-    FCIB_CUDA(cudaMemcpy(sa.data(), c.A.str.p, 4 * c.nas, cudaMemcpyDeviceToHost));
-    FCIB_CUDA(cudaMemcpy(sbv.data(), c.B.str.p, 4 * c.nbs, cudaMemcpyDeviceToHost));
-    HostInts hi;
-    hi.n = c.n;
-    hi.oa = &c.oei_a; hi.ob = &c.oei_b; hi.taa = &c.tei_aa; hi.tab = &c.tei_ab; hi.tbb = &c.tei_bb;
-    const int64_t nbs = c.nbs;
-    const int n = c.n;
-    GuessResult gr;
-    try {
-        gr = make_guess(
-            hi, lowest, [&](int64_t I) { return Det{sa[I / nbs], sbv[I % nbs]}; },
-            [&](const Det& d) { return (int64_t)host_rank((uint32_t)d.a, n) * nbs + host_rank((uint32_t)d.b, n); },
-            num_guess_states, c.multiplicity);
-    } catch (std::exception& e) {
-        throw Error{FCIB_ERR_ARG, e.what()};
-    }
-    int nguess = (int)gr.guesses.size();
-    c.t_guess_ms = now_ms() - t_guess0;
-    c.guess_dets = gr.guesses.empty() ? 0 : (int)gr.guesses[0].size();
-    FCIB_CHECK(nguess >= nroot && nguess <= m, FCIB_ERR_ARG,
-               "DavidsonLiuSolver: number of guess vectors must be between nroot and the subspace size");
-    std::vector<SparseDev> bad(gr.bad_roots.size());
-    for (size_t i = 0; i < bad.size(); i++) {
-        std::vector<int64_t> ix;
-        std::vector<double> vv;
-        for (auto& e : gr.bad_roots[i]) { ix.push_back(e.first); vv.push_back(e.second); }
-        bad[i].idx.upload(ix, c.stream);
-        bad[i].val.upload(vv, c.stream);
-        bad[i].cnt = (int)ix.size();
-    }
-    FCIB_CUDA(cudaMemsetAsync(c.tmp.p, 0, sizeof(double) * (size_t)m * N, c.stream));
-    for (int g = 0; g < nguess; g++) {
-        SparseDev sd;
-        std::vector<int64_t> ix;
-        std::vector<double> vv;
-        for (auto& e : gr.guesses[g]) { ix.push_back(e.first); vv.push_back(e.second); }
-        sd.idx.upload(ix, c.stream);
-        sd.val.upload(vv, c.stream);
-        k_fill_sparse<<<((int)ix.size() + 255) / 256, 256, 0, c.stream>>>(tmp[g], sd.idx.p, sd.val.p, (int)ix.size());
-        FCIB_KCHECK();
-        FCIB_CUDA(cudaStreamSynchronize(c.stream));
-    }
-    if (gr.perturb) {
-        // Without spin selection the lowest state may lie in a spin sector the guess space does
-        // not contain; exact FP64 iterations never leave the sectors of the guess, so every
-        // guess gets a seeded pseudo-random component of norm ~1e-3 over all determinants.
-        for (int k = 0; k < nguess; k++) {
-            k_add_random<<<ops.nblk, kRedThreads, 0, c.stream>>>(tmp[k], N, 0x9E3779B97F4A7C15ull * (k + 1),
-                                                                 1.0e-3 * std::sqrt(3.0 / (double)N));
-            FCIB_KCHECK();
-            apply_mask(c, tmp[k]);
+    int basis = 0;
+    std::vector<SparseDev> bad;
+    auto upload_bad = [&](const std::vector<std::vector<std::pair<int64_t, double>>>& src) {
+        std::vector<SparseDev> v(src.size());  // device buffers are neither copied nor moved
+        for (size_t i = 0; i < src.size(); i++) {
+            std::vector<int64_t> ix;
+            std::vector<double> vv;
+            for (auto& e : src[i]) { ix.push_back(e.first); vv.push_back(e.second); }
+            v[i].idx.upload(ix, c.stream);
+            v[i].val.upload(vv, c.stream);
+            v[i].cnt = (int)ix.size();
         }
+        bad.swap(v);
+        FCIB_CUDA(cudaStreamSynchronize(c.stream));  // the host index vectors go out of scope
+    };
+    // a fresh guess (FCISolver::initial_guess_det): lowest diagonal determinants, spin-adapted
+    // guess vectors and the unwanted roots to project out
+    auto fresh_guess = [&]() -> int {
+        auto lowest = lowest_diagonal(c, ng);
+        std::vector<uint32_t> sa(c.nas), sbv(c.nbs);
+        FCIB_CUDA(cudaMemcpy(sa.data(), c.A.str.p, 4 * c.nas, cudaMemcpyDeviceToHost));
+        FCIB_CUDA(cudaMemcpy(sbv.data(), c.B.str.p, 4 * c.nbs, cudaMemcpyDeviceToHost));
+        HostInts hi;
+        hi.n = c.n;
+        hi.oa = &c.oei_a; hi.ob = &c.oei_b; hi.taa = &c.tei_aa; hi.tab = &c.tei_ab; hi.tbb = &c.tei_bb;
+        const int64_t nbs = c.nbs;
+        const int n = c.n;
+        GuessResult gr;
+        try {
+            gr = make_guess(
+                hi, lowest, [&](int64_t I) { return Det{sa[I / nbs], sbv[I % nbs]}; },
+                [&](const Det& d) { return (int64_t)host_rank((uint32_t)d.a, n) * nbs + host_rank((uint32_t)d.b, n); },
+                num_guess_states, c.multiplicity);
+        } catch (std::exception& e) {
+            throw Error{FCIB_ERR_ARG, e.what()};
+        }
+        int nguess = (int)gr.guesses.size();
+        c.t_guess_ms = now_ms() - t_guess0;
+        c.guess_dets = gr.guesses.empty() ? 0 : (int)gr.guesses[0].size();
+        FCIB_CHECK(nguess >= nroot && nguess <= m, FCIB_ERR_ARG,
+                   "DavidsonLiuSolver: number of guess vectors must be between nroot and the subspace size");
+        c.dl_bad = gr.bad_roots;
+        upload_bad(c.dl_bad);
+        FCIB_CUDA(cudaMemsetAsync(c.tmp.p, 0, sizeof(double) * (size_t)m * N, c.stream));
+        for (int g = 0; g < nguess; g++) {
+            SparseDev sd;
+            std::vector<int64_t> ix;
+            std::vector<double> vv;
+            for (auto& e : gr.guesses[g]) { ix.push_back(e.first); vv.push_back(e.second); }
+            sd.idx.upload(ix, c.stream);
+            sd.val.upload(vv, c.stream);
+            k_fill_sparse<<<((int)ix.size() + 255) / 256, 256, 0, c.stream>>>(tmp[g], sd.idx.p, sd.val.p, (int)ix.size());
+            FCIB_KCHECK();
+            FCIB_CUDA(cudaStreamSynchronize(c.stream));
+        }
+        if (gr.perturb) {
+            // Without spin selection the lowest state may lie in a spin sector the guess space does
+            // not contain; exact FP64 iterations never leave the sectors of the guess, so every
+            // guess gets a seeded pseudo-random component of norm ~1e-3 over all determinants.
+            for (int k = 0; k < nguess; k++) {
+                k_add_random<<<ops.nblk, kRedThreads, 0, c.stream>>>(tmp[k], N, 0x9E3779B97F4A7C15ull * (k + 1),
+                                                                     1.0e-3 * std::sqrt(3.0 / (double)N));
+                FCIB_KCHECK();
+                apply_mask(c, tmp[k]);
+            }
+        }
+        project_out(c, bad, tmp, std::min(nroot, nguess));
+        int should = std::max(nroot, nguess);
+        const int added = add_rows_orth(ops, b, 0, std::vector<double*>(tmp.begin(), tmp.begin() + should), should);
+        FCIB_CHECK(added == should, FCIB_ERR_NUMERIC, "DavidsonLiuSolver: guess vectors are zero or linearly dependent");
+        return added;
+    };
+    if (restart) {
+        upload_bad(c.dl_bad);
+        basis = nroot;  // rows 0..nroot-1 of b hold the previous eigenvectors
+        c.t_guess_ms = 0.0;
+    } else {
+        basis = fresh_guess();
     }
-    project_out(c, bad, tmp, std::min(nroot, nguess));
-    int should = std::max(nroot, nguess);
-    int basis = add_rows_orth(ops, b, 0, std::vector<double*>(tmp.begin(), tmp.begin() + should), should);
-    FCIB_CHECK(basis == should, FCIB_ERR_NUMERIC, "DavidsonLiuSolver: guess vectors are zero or linearly dependent");
 
     const bool mixed = (o.precision != FCIB_PREC_FP64);
     const int lowp = o.precision;
@@ -794,6 +830,7 @@ void dl_solve(Context& c) {
 
     int nsig = 0;
     std::vector<double> G((size_t)m * m, 0.0), alpha((size_t)m * m, 0.0), lambda(m, 0.0), lambda_old(m, 0.0);
+    if (restart && (int)c.dl_lambda_old.size() == m) lambda_old = c.dl_lambda_old;  // a member of the reference solver
     std::vector<double> rnorm(nroot, 0.0), cnorm(nroot, 0.0);
     int gvalid = 0;
     bool converged = false;
@@ -1003,6 +1040,9 @@ void dl_solve(Context& c) {
     c.t_total_ms = tot;
     c.solved = true;
     c.converged = converged;
+    c.dl_prev = true;
+    c.dl_prev_space = space;
+    c.dl_lambda_old = lambda;
     c.spin2.resize(nroot);
     for (int k = 0; k < nroot; k++) c.spin2[k] = spin2_device(c, c.b.p + (size_t)k * N);
     FCIB_CUDA(cudaStreamSynchronize(c.stream));

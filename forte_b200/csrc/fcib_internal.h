@@ -184,6 +184,14 @@ struct Context {
     double t_tc_ms = 0.0;  // tensor-core contraction kernel alone (mixed sigma)
     int guess_dets = 0;
     bool converged = false;
+    // restart state of the Davidson-Liu solver (DavidsonLiuSolver::setup_guesses restarts a solver
+    // that already ran from its first nroot vectors): the determinant space it ran on and the
+    // vectors its first guess asked to project out
+    bool dl_prev = false;
+    bool restarted = false;  // the last solve restarted from the previous solution
+    std::vector<int64_t> dl_prev_space;
+    std::vector<std::vector<std::pair<int64_t, double>>> dl_bad;
+    std::vector<double> dl_lambda_old;  // eigenvalues of the previous solve's last iteration
     std::vector<std::array<double, 5>> trace;
     // learned preconditioner weights (FP32 master copy, BF16-rounded at use)
     DBuf<float> mlp_w;
