@@ -129,7 +129,9 @@ class Clocks:
 
 
 def solve_once(solver, torch, stream):
-    """One Davidson solve timed with CUDA events on the engine stream; returns seconds."""
+    """One Davidson solve from a fresh guess (no restart from the previous solve's vectors), timed
+    with CUDA events on the engine stream; returns seconds."""
+    solver.reset_guess()
     st = torch.cuda.Event(enable_timing=True)
     en = torch.cuda.Event(enable_timing=True)
     st.record(stream)
@@ -512,6 +514,7 @@ def main():
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             s.set_integrals(ints)
+            s.reset_guess()  # a fresh solve, not a restart from the previous step's vectors
             s.compute_energy()
             capi.check(capi.lib().fcib_get_vector(s._h, 0, capi.dptr(host_vec)))
             torch.cuda.synchronize()

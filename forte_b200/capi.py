@@ -81,6 +81,7 @@ SIGNATURES = {
     "fcib_set_options": (C.c_int, [_vp, C.POINTER(FcibOptions)]),
     "fcib_size": (C.c_int, [_vp, C.POINTER(C.c_int64)]),
     "fcib_solve": (C.c_int, [_vp, _dp, _dp, C.POINTER(C.c_int)]),
+    "fcib_reset_guess": (C.c_int, [_vp]),
     "fcib_get_vector": (C.c_int, [_vp, C.c_int, _dp]),
     "fcib_sigma": (C.c_int, [_vp, _dp, _dp]),
     "fcib_sigma_device": (C.c_int, [_vp, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),

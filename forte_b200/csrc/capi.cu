@@ -335,6 +335,12 @@ int fcib_solve(fcib_ctx* ctx, double* energies, double* spin2, int* iterations) 
     return rc;
 }
 
+int fcib_reset_guess(fcib_ctx* ctx) {
+    if (!ctx) { set_error("null context"); return FCIB_ERR_ARG; }
+    ctx->c.dl_prev = false;
+    return FCIB_OK;
+}
+
 int fcib_get_vector(fcib_ctx* ctx, int root, double* out) {
     if (!ctx || !out) { set_error("null argument"); return FCIB_ERR_ARG; }
     return guarded(ctx, [&] {

@@ -184,6 +184,11 @@ class FCISolver:
         self._energies, self._spin2, self._iterations = e, s2, it.value
         return float(e[self._root])
 
+    def reset_guess(self):
+        """Forget the previous solution: the next compute_energy starts from a fresh guess, as a
+        newly constructed FCISolver would, instead of restarting from the previous eigenvectors."""
+        capi.check(capi.lib().fcib_reset_guess(self._h))
+
     def energies(self):
         return list(self._energies)
 

@@ -98,6 +98,12 @@ int fcib_size(fcib_ctx* ctx, int64_t* ndet);
  * (may be NULL).  Returns FCIB_ERR_NOT_CONVERGED when the solver did not converge and
  * die_if_not_converged is set (the results are still stored). */
 int fcib_solve(fcib_ctx* ctx, double* energies, double* spin2, int* iterations);
+/* A context that solved before restarts the next fcib_solve from its previous eigenvectors
+ * (FCISolver::compute_energy keeps its DavidsonLiuSolver, fci_solver.cc:205-233), as long as the
+ * determinant space, nroot and subspace size are unchanged and the guess space does not cover the
+ * whole space.  fcib_reset_guess forgets the previous solution, so that the next solve starts from
+ * a fresh guess, as a newly constructed FCISolver would. */
+int fcib_reset_guess(fcib_ctx* ctx);
 /* eigenvector of a root in FCIVector flat order (size from fcib_size) */
 int fcib_get_vector(fcib_ctx* ctx, int root, double* out);
 

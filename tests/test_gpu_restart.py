@@ -79,3 +79,14 @@ def test_state_change_starts_fresh():
     f = FCISolver(StateInfo(4, 3, 0, 1), 1, ints, OPTS)
     assert abs(e - f.compute_energy()) < 1e-10
     assert s.iterations() == f.iterations()
+
+
+def test_reset_guess_repeats_a_fresh_solve():
+    ints = synthetic(8, 24, 9)
+    s = FCISolver(StateInfo(4, 4, 0), 2, ints, OPTS)
+    s.compute_energy()
+    e1, it1 = np.array(s.energies()), s.iterations()
+    s.reset_guess()
+    s.compute_energy()
+    assert s.iterations() == it1
+    assert np.max(np.abs(np.array(s.energies()) - e1)) < 1e-10
