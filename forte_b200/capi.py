@@ -89,6 +89,8 @@ SIGNATURES = {
     "fcib_spin2": (C.c_int, [_vp, _dp, _dp]),
     "fcib_rdms": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp]),
     "fcib_compute_rdms": (C.c_int, [_vp, _dp, _dp, C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp]),
+    "fcib_rdms3": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _dp]),
+    "fcib_compute_rdms3": (C.c_int, [_vp, _dp, _dp, C.c_int, _dp, _dp, _dp, _dp]),
     "fcib_num_strings": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_int64)]),
     "fcib_strings": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_uint32)]),
     "fcib_string_list": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,

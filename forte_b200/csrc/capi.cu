@@ -414,8 +414,9 @@ int fcib_rdms(fcib_ctx* ctx, int root_left, int root_right, int level, int spin_
             throw Error{FCIB_ERR_ARG, "Cannot compute RDMs <" + std::to_string(root_left) + "| ... |" +
                                           std::to_string(root_right) + "> (0-based) because nroot = " +
                                           std::to_string(c.nroot)};
-        FCIB_CHECK(level <= 2, FCIB_ERR_UNSUPPORTED, "RDMs of order 3 or higher are not available in this engine");
+        FCIB_CHECK(level <= 3, FCIB_ERR_UNSUPPORTED, "RDMs of order higher than 3 are not available");
         if (level <= 0) return;
+        level = std::min(level, 2);  // the three-body blocks come from fcib_rdms3
         RdmBlocks blk;
         compute_rdms(c, c.b.p + (size_t)root_left * c.ndet, c.b.p + (size_t)root_right * c.ndet, level, blk);
         rdms_to_outputs(blk, level, spin_free, g1a, g1b, g2aa, g2ab, g2bb);
@@ -428,8 +429,9 @@ int fcib_compute_rdms(fcib_ctx* ctx, const double* left, const double* right, in
     return guarded(ctx, [&] {
         Context& c = ctx->c;
         ensure_setup(c);
-        FCIB_CHECK(level <= 2, FCIB_ERR_UNSUPPORTED, "RDMs of order 3 or higher are not available in this engine");
+        FCIB_CHECK(level <= 3, FCIB_ERR_UNSUPPORTED, "RDMs of order higher than 3 are not available");
         if (level <= 0) return;
+        level = std::min(level, 2);  // the three-body blocks come from fcib_compute_rdms3
         DBuf<double> dl, dr;
         dl.alloc(c.ndet);
         upload_flat(c, left, dl.p);
@@ -442,6 +444,74 @@ int fcib_compute_rdms(fcib_ctx* ctx, const double* left, const double* right, in
         RdmBlocks blk;
         compute_rdms(c, dl.p, R, level, blk);
         rdms_to_outputs(blk, level, spin_free, g1a, g1b, g2aa, g2ab, g2bb);
+    });
+}
+
+// 3-RDM blocks -> caller's arrays; spin_free: G3 of FCIVector::compute_rdms (fci_vector_rdm.cc:127-130)
+static void rdms3_to_outputs(const Rdm3Blocks& b, int spin_free, double* g3aaa, double* g3aab, double* g3abb,
+                             double* g3bbb) {
+    if (!spin_free) {
+        if (g3aaa) std::copy(b.aaa.begin(), b.aaa.end(), g3aaa);
+        if (g3aab) std::copy(b.aab.begin(), b.aab.end(), g3aab);
+        if (g3abb) std::copy(b.abb.begin(), b.abb.end(), g3abb);
+        if (g3bbb) std::copy(b.bbb.begin(), b.bbb.end(), g3bbb);
+        return;
+    }
+    if (!g3aaa) return;
+    const int n = b.n;
+    auto six = [n](int p, int q, int r, int s, int t, int u) {
+        return (((((size_t)p * n + q) * n + r) * n + s) * n + t) * n + u;
+    };
+    for (int p = 0; p < n; p++)
+        for (int q = 0; q < n; q++)
+            for (int r = 0; r < n; r++)
+                for (int s = 0; s < n; s++)
+                    for (int t = 0; t < n; t++)
+                        for (int u = 0; u < n; u++) {
+                            const size_t o = six(p, q, r, s, t, u);
+                            double g = b.aaa[o];
+                            g += b.aab[o] + b.aab[six(p, r, q, s, u, t)] + b.aab[six(q, r, p, t, u, s)];
+                            g += b.abb[o] + b.abb[six(q, p, r, t, s, u)] + b.abb[six(r, p, q, u, s, t)];
+                            g += b.bbb[o];
+                            g3aaa[o] = g;
+                        }
+}
+
+int fcib_rdms3(fcib_ctx* ctx, int root_left, int root_right, int spin_free, double* g3aaa, double* g3aab,
+               double* g3abb, double* g3bbb) {
+    if (!ctx) { set_error("null context"); return FCIB_ERR_ARG; }
+    return guarded(ctx, [&] {
+        Context& c = ctx->c;
+        FCIB_CHECK(c.solved, FCIB_ERR_STATE, "FCIVector is not assigned. Cannot compute RDMs.");
+        FCIB_CHECK(root_left >= 0 && root_right >= 0, FCIB_ERR_ARG, "negative root index");
+        if (std::max(root_left, root_right) >= c.nroot)
+            throw Error{FCIB_ERR_ARG, "Cannot compute RDMs <" + std::to_string(root_left) + "| ... |" +
+                                          std::to_string(root_right) + "> (0-based) because nroot = " +
+                                          std::to_string(c.nroot)};
+        Rdm3Blocks blk;
+        compute_rdms3(c, c.b.p + (size_t)root_left * c.ndet, c.b.p + (size_t)root_right * c.ndet, blk);
+        rdms3_to_outputs(blk, spin_free, g3aaa, g3aab, g3abb, g3bbb);
+    });
+}
+
+int fcib_compute_rdms3(fcib_ctx* ctx, const double* left, const double* right, int spin_free, double* g3aaa,
+                       double* g3aab, double* g3abb, double* g3bbb) {
+    if (!ctx || !left) { set_error("null argument"); return FCIB_ERR_ARG; }
+    return guarded(ctx, [&] {
+        Context& c = ctx->c;
+        ensure_setup(c);
+        DBuf<double> dl, dr;
+        dl.alloc(c.ndet);
+        upload_flat(c, left, dl.p);
+        const double* R = dl.p;
+        if (right && right != left) {
+            dr.alloc(c.ndet);
+            upload_flat(c, right, dr.p);
+            R = dr.p;
+        }
+        Rdm3Blocks blk;
+        compute_rdms3(c, dl.p, R, blk);
+        rdms3_to_outputs(blk, spin_free, g3aaa, g3aab, g3abb, g3bbb);
     });
 }
 

@@ -6,6 +6,7 @@
 #include "sigma_same_tc.cu"
 #include "davidson.cu"
 #include "rdms.cu"
+#include "rdms3.cu"
 #include "capi.cu"
 #include "mlp.cu"
 #include "batch.cu"

@@ -226,6 +226,12 @@ struct RdmBlocks {
     std::vector<double> g1a, g1b, g2aa, g2ab, g2bb;
 };
 void compute_rdms(Context& c, const double* L, const double* R, int level, RdmBlocks& out);
+// rdms3.cu: host copies of the 3-RDM blocks (row-major n^6, reference index order and orientation)
+struct Rdm3Blocks {
+    int n = 0;
+    std::vector<double> aaa, aab, abb, bbb;
+};
+void compute_rdms3(Context& c, const double* L, const double* R, Rdm3Blocks& out);
 // mlp.cu: learned preconditioner, in place on a diagonal correction t
 void mlp_apply(Context& c, double* t, double lambda, double rnorm, double tnorm);
 // davidson.cu

@@ -135,6 +135,9 @@ __global__ void __launch_bounds__(kRdmThreads)
     }
 }
 
+// FULL: every (i, j) element (the 3-RDM triple groups); otherwise only lab_i >= lab_j, the half the
+// reference's 2-RDM loops form
+template <bool FULL>
 __global__ void __launch_bounds__(kRdmThreads)
     k_rdm_pairs(const double* __restrict__ L, const double* __restrict__ R, int ncol,
                 const uint32_t* __restrict__ rows, const uint16_t* __restrict__ labs, int ng, int m, int npl,
@@ -176,7 +179,7 @@ __global__ void __launch_bounds__(kRdmThreads)
                     const int t = t0 + u * kRdmThreads + threadIdx.x;
                     if (t >= mm) continue;
                     const int i = t / m, j = t - i * m;
-                    if (lab[i] < lab[j]) continue;
+                    if (!FULL && lab[i] < lab[j]) continue;
                     const double* li = Lt + i * LD;
                     const double* rj = Rt + j * LD;
                     double a = acc[u];
@@ -190,7 +193,7 @@ __global__ void __launch_bounds__(kRdmThreads)
                 const int t = t0 + u * kRdmThreads + threadIdx.x;
                 if (t >= mm) continue;
                 const int i = t / m, j = t - i * m;
-                if (lab[i] < lab[j] || acc[u] == 0.0) continue;
+                if ((!FULL && lab[i] < lab[j]) || acc[u] == 0.0) continue;
                 const double sg = ((rI[i] ^ rI[j]) >> 31) ? -1.0 : 1.0;
                 atomicAdd(M + (size_t)lab[i] * npl + lab[j], sg * acc[u]);
             }
@@ -226,10 +229,10 @@ static void rdm_pairs(Context& c, const double* L, const double* R, int ncol, co
     const int m = T.g2, npl = c.n * (c.n - 1) / 2;
     const size_t smem = 2 * (size_t)m * (kPairTB + 1) * 8 + (size_t)m * 8;
     FCIB_CHECK(smem + 1024 <= (size_t)c.smem_optin, FCIB_ERR_UNSUPPORTED, "RDMs: pair group exceeds shared memory");
-    FCIB_CUDA(cudaFuncSetAttribute(k_rdm_pairs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    FCIB_CUDA(cudaFuncSetAttribute(k_rdm_pairs<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int per_sm = std::max(1, std::min(8, (int)(c.smem_per_sm / (smem + 1024))));
     const int grid = std::min(T.ng2, per_sm * c.num_sms);
-    k_rdm_pairs<<<grid, kRdmThreads, smem, c.stream>>>(L, R, ncol, T.g2row.p, T.g2lab.p, T.ng2, m, npl, M);
+    k_rdm_pairs<false><<<grid, kRdmThreads, smem, c.stream>>>(L, R, ncol, T.g2row.p, T.g2lab.p, T.ng2, m, npl, M);
     FCIB_KCHECK();
 }
 

@@ -244,28 +244,30 @@ class FCISolver:
 
     def rdms(self, root_list, max_rdm_level=2, rdm_type="spin_dependent"):
         """FCISolver::rdms (forte/fci/fci_solver_rdms.cc:40-104): one RDMs object per (left, right)
-        root pair of the last solve; max_rdm_level <= 0 gives empty objects."""
-        if max_rdm_level > 2:
-            raise RuntimeError("RDMs of order 3 or higher are not implemented in this engine")
+        root pair of the last solve; max_rdm_level <= 0 gives empty objects, 3 adds the 3-RDMs."""
+        if max_rdm_level > 3:
+            raise RuntimeError("RDMs of order higher than 3 are not available")
         out = []
         for (rl, rr) in root_list:
             if max(rl, rr) >= self.nroot:
                 raise RuntimeError(f"Cannot compute RDMs <{rl}| ... |{rr}> (0-based) because nroot = {self.nroot}")
             out.append(self._rdm_call(lambda *a, rl=rl, rr=rr: capi.lib().fcib_rdms(self._h, rl, rr, *a),
-                                      max_rdm_level, rdm_type))
+                                      max_rdm_level, rdm_type,
+                                      lambda *a, rl=rl, rr=rr: capi.lib().fcib_rdms3(self._h, rl, rr, *a)))
         return out
 
     def compute_rdms(self, left, right=None, max_rdm_level=2, rdm_type="spin_dependent"):
         """FCIVector::compute_rdms (forte/fci/fci_vector_rdm.cc:43-145) between two vectors in
         FCIVector flat order (right defaults to left)."""
-        if max_rdm_level > 2:
-            raise RuntimeError("RDMs of order 3 or higher are not implemented in this engine")
         left = np.ascontiguousarray(left, dtype=np.float64)
         right = left if right is None else np.ascontiguousarray(right, dtype=np.float64)
         return self._rdm_call(lambda *a: capi.lib().fcib_compute_rdms(self._h, capi.dptr(left), capi.dptr(right), *a),
-                              max_rdm_level, rdm_type)
+                              max_rdm_level, rdm_type,
+                              lambda *a: capi.lib().fcib_compute_rdms3(self._h, capi.dptr(left), capi.dptr(right), *a))
 
-    def _rdm_call(self, fn, level, rdm_type):
+    def _rdm_call(self, fn, level, rdm_type, fn3=None):
+        """One- and two-body blocks through fn; with max_rdm_level 3 the three-body blocks through
+        fn3 (RDMsSpinDependent g3aaa, g3aab, g3abb, g3bbb or RDMsSpinFree g3)."""
         n = self.ints.n
         sf = rdm_type in ("spin_free", 1)
         if level <= 0:
@@ -275,9 +277,15 @@ class FCISolver:
         g2 = [np.zeros((n,) * 4) for _ in range(3)] if level > 1 else [None] * 3
         ptr = [capi.dptr(x) if x is not None else None for x in (g1a, g1b, *g2)]
         capi.check(fn(level, 1 if sf else 0, *ptr))
+        g3 = {}
+        if level >= 3:
+            blocks = [np.zeros((n,) * 6) for _ in range(1 if sf else 4)]
+            ptr3 = [capi.dptr(x) for x in blocks] + [None] * (4 - len(blocks))
+            capi.check(fn3(1 if sf else 0, *ptr3))
+            g3 = {"g3": blocks[0]} if sf else dict(zip(("g3aaa", "g3aab", "g3abb", "g3bbb"), blocks))
         if sf:
-            return RDMs(True, g1=g1a, g2=g2[0])
-        return RDMs(False, g1a=g1a, g1b=g1b, g2aa=g2[0], g2ab=g2[1], g2bb=g2[2])
+            return RDMs(True, g1=g1a, g2=g2[0], **g3)
+        return RDMs(False, g1a=g1a, g1b=g1b, g2aa=g2[0], g2ab=g2[1], g2bb=g2[2], **g3)
 
     # ---- string tables (parity checks) ----------------------------------------------------
     def strings(self, spin):

@@ -126,6 +126,19 @@ int fcib_rdms(fcib_ctx* ctx, int root_left, int root_right, int level, int spin_
  * replaces FCIVector::compute_rdms(C_left, C_right, max_rdm_level, type) (fci_vector_rdm.cc:43-145). */
 int fcib_compute_rdms(fcib_ctx* ctx, const double* left, const double* right, int level, int spin_free,
                       double* g1a, double* g1b, double* g2aa, double* g2ab, double* g2bb);
+/* 3-RDMs (max_rdm_level = 3 of FCISolver::rdms / FCIVector::compute_rdms, fci_vector_rdm.cc:70-137,
+ * blocks compute_3rdm_aaa/aab/abb_same_irrep :395-565); fcib_rdms and fcib_compute_rdms accept
+ * level 3 and return its one- and two-body parts.  Blocks are n^6 row-major in the reference's
+ * index order and orientation (its loops take the creation indices from the right vector):
+ *   g3aaa[p,q,r,s,t,u] = <right| a+_p a+_q a+_r a_u a_t a_s |left>, all alpha;
+ *   g3aab: p, q, s, t alpha and r, u beta;  g3abb: p, s alpha and q, r, t, u beta;  g3bbb: beta.
+ * For left == right these are the usual 3-RDMs.  spin_free: g3aaa receives the spin-free
+ * G3 = aaa + aab + aab(prqsut) + aab(qrptus) + abb + abb(qprtsu) + abb(rpqust) + bbb (:127-130)
+ * and the other pointers are ignored.  Any output may be NULL. */
+int fcib_rdms3(fcib_ctx* ctx, int root_left, int root_right, int spin_free, double* g3aaa, double* g3aab,
+               double* g3abb, double* g3bbb);
+int fcib_compute_rdms3(fcib_ctx* ctx, const double* left, const double* right, int spin_free, double* g3aaa,
+                       double* g3aab, double* g3abb, double* g3bbb);
 
 /* ---- learned preconditioner (no counterpart in the reference) ------------------------------
  * With preconditioner = FCIB_PRECOND_MLP each diagonal correction t_I = r_I / (lambda - H_II)

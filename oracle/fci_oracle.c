@@ -1373,3 +1373,190 @@ int orc_rdms(void* h, const double* L, const double* R, int level, double* g1a, 
     if (level >= 2) { rdm2_same(c, L, R, g2aa, 1); rdm2_same(c, L, R, g2bb, 0); rdm2_ab(c, L, R, g2ab); }
     return 0;
 }
+
+/* ------------------------------------------------------------------------------------------ */
+/* 3-RDMs (FCIVector::compute_3rdm_aaa/aab/abb_same_irrep, forte/fci/fci_vector_rdm.cc:395-565), */
+/* restated over the 1h/2h/3h string lists of FCIStringLists::make_1h/2h/3h_list               */
+/* (fci_string_hole_list.cc:59-223).  An entry (sign, o1[, o2[, o3]], I) of the list of the    */
+/* (k-h)-string K means <K| a_o1 [a_o2 [a_o3]] |I> = sign; the 2h and 3h lists hold every       */
+/* ordering of the removed orbitals.  Blocks are n^6 row-major, filled with the reference's     */
+/* loops: the first index triple comes from the entries of the right vector, the second from    */
+/* those of the left vector.                                                                   */
+/* ------------------------------------------------------------------------------------------ */
+typedef struct {
+    double sign;
+    int o[3];
+    uint32_t I; /* address of the k-string */
+} hentry;
+
+#define SIX(p, q, r, s, t, u) \
+    ((((((size_t)(p) * n + (q)) * n + (r)) * n + (s)) * n + (t)) * n + (u))
+
+/* the h-hole list of the (k-h)-string K over the k-strings of S; returns the entry count */
+static int hole_list(const spinlists* S, uint64_t K, int h, hentry* out) {
+    int n = S->n, cnt = 0;
+    if (h == 1) {
+        for (int p = 0; p < n; p++) {
+            if (K >> p & 1) continue;
+            hentry e = {sgn_below(K, p), {p, 0, 0}, (uint32_t)addr_of(S, K | 1ull << p)};
+            out[cnt++] = e;
+        }
+    } else if (h == 2) {
+        for (int q = 0; q < n; q++)
+            for (int p = q + 1; p < n; p++) {
+                if ((K >> p & 1) || (K >> q & 1)) continue;
+                /* make_2h_list: remove q, then p */
+                double s = sgn_below(K | 1ull << p, q) * sgn_below(K, p);
+                uint32_t I = (uint32_t)addr_of(S, K | 1ull << p | 1ull << q);
+                hentry a = {s, {p, q, 0}, I}, b = {-s, {q, p, 0}, I};
+                out[cnt++] = a;
+                out[cnt++] = b;
+            }
+    } else {
+        for (int r = 0; r < n; r++)
+            for (int q = r + 1; q < n; q++)
+                for (int p = q + 1; p < n; p++) {
+                    if ((K >> p & 1) || (K >> q & 1) || (K >> r & 1)) continue;
+                    /* make_3h_list: remove r, then q, then p */
+                    double s = sgn_below(K | 1ull << p | 1ull << q, r) * sgn_below(K | 1ull << p, q) * sgn_below(K, p);
+                    uint32_t I = (uint32_t)addr_of(S, K | 1ull << p | 1ull << q | 1ull << r);
+                    hentry e[6] = {{+s, {p, q, r}, I}, {-s, {p, r, q}, I}, {-s, {q, p, r}, I},
+                                   {+s, {q, r, p}, I}, {-s, {r, q, p}, I}, {+s, {r, p, q}, I}};
+                    for (int x = 0; x < 6; x++) out[cnt++] = e[x];
+                }
+    }
+    return cnt;
+}
+
+/* all (k-h)-strings of n orbitals, in any order; returns the count */
+static int64_t hole_strings(int n, int kh, uint64_t** out) {
+    int64_t ns = binom(n, kh);
+    *out = (uint64_t*)malloc(sizeof(uint64_t) * (ns > 0 ? ns : 1));
+    if (ns > 0) orc_make_strings(n, kh, *out);
+    return ns;
+}
+
+/* compute_3rdm_aaa_same_irrep (fci_vector_rdm.cc:395-437): rdm[p,q,r,s,t,u] += sign_K sign_L
+ * <Cl[J], Cr[I]> over the pairs of entries (sign_K, p, q, r, I), (sign_L, s, t, u, J) of one
+ * 3h list; the dots are formed once per pair of strings */
+static void rdm3_same(orc_ctx* c, const double* L, const double* R, double* g, int alfa) {
+    int n = c->n;
+    spinlists* S = alfa ? &c->A : &c->B;
+    memset(g, 0, sizeof(double) * (size_t)n * n * n * n * n * n);
+    if (S->k < 3) return;
+    int64_t maxL = alfa ? c->nbs : c->nas;
+    const double *Cl = L, *Cr = R;
+    double *tl = NULL, *tr = NULL;
+    if (!alfa) {
+        tl = (double*)malloc(sizeof(double) * c->ndet);
+        tr = (double*)malloc(sizeof(double) * c->ndet);
+        transpose(L, tl, c->nas, c->nbs);
+        transpose(R, tr, c->nas, c->nbs);
+        Cl = tl; Cr = tr;
+    }
+    uint64_t* Ks = NULL;
+    int64_t nK = hole_strings(n, S->k - 3, &Ks);
+    hentry* e = (hentry*)malloc(sizeof(hentry) * 6 * (size_t)binom(n, 3));
+    int m3 = (int)binom(n - S->k + 3, 3);
+    double* D = (double*)malloc(sizeof(double) * (size_t)m3 * m3);
+    for (int64_t k = 0; k < nK; k++) {
+        int cnt = hole_list(S, Ks[k], 3, e);
+        int nr = cnt / 6; /* distinct strings: entries 6x, 6x+1, ... share I */
+        for (int a = 0; a < nr; a++)
+            for (int b = 0; b < nr; b++)
+                D[a * nr + b] = ddot(maxL, Cl + (int64_t)e[6 * b].I * maxL, Cr + (int64_t)e[6 * a].I * maxL);
+        for (int x = 0; x < cnt; x++)
+            for (int y = 0; y < cnt; y++) {
+                const hentry* K = &e[x];
+                const hentry* J = &e[y];
+                g[SIX(K->o[0], K->o[1], K->o[2], J->o[0], J->o[1], J->o[2])] +=
+                    K->sign * J->sign * D[(x / 6) * nr + (y / 6)];
+            }
+    }
+    free(D); free(e); free(Ks); free(tl); free(tr);
+}
+
+/* compute_3rdm_aab_same_irrep (fci_vector_rdm.cc:439-502) */
+static void rdm3_aab(orc_ctx* c, const double* L, const double* R, double* g) {
+    int n = c->n;
+    memset(g, 0, sizeof(double) * (size_t)n * n * n * n * n * n);
+    if (c->A.k < 2 || c->B.k < 1) return;
+    int64_t nbs = c->nbs;
+    uint64_t *Ka = NULL, *Kb = NULL;
+    int64_t nKa = hole_strings(n, c->A.k - 2, &Ka), nKb = hole_strings(n, c->B.k - 1, &Kb);
+    hentry* I2 = (hentry*)malloc(sizeof(hentry) * 2 * (size_t)binom(n, 2));
+    hentry* M1 = (hentry*)malloc(sizeof(hentry) * (size_t)n);
+    for (int64_t ka = 0; ka < nKa; ka++) {
+        int ni = hole_list(&c->A, Ka[ka], 2, I2);
+        for (int64_t kb = 0; kb < nKb; kb++) {
+            int nm = hole_list(&c->B, Kb[kb], 1, M1);
+            for (int x = 0; x < ni; x++) {
+                int q = I2[x].o[0], p = I2[x].o[1];
+                const double* Cr = R + (int64_t)I2[x].I * nbs;
+                for (int y = 0; y < ni; y++) {
+                    int t = I2[y].o[0], s = I2[y].o[1];
+                    const double* Cl = L + (int64_t)I2[y].I * nbs;
+                    for (int u = 0; u < nm; u++) {
+                        int r = M1[u].o[0];
+                        double cr = Cr[M1[u].I];
+                        if (cr == 0.0) continue;
+                        for (int v = 0; v < nm; v++) {
+                            int a = M1[v].o[0];
+                            double sign = I2[x].sign * I2[y].sign * M1[u].sign * M1[v].sign;
+                            g[SIX(p, q, r, s, t, a)] += sign * cr * Cl[M1[v].I];
+                        }
+                    }
+                }
+            }
+        }
+    }
+    free(I2); free(M1); free(Ka); free(Kb);
+}
+
+/* compute_3rdm_abb_same_irrep (fci_vector_rdm.cc:504-565) */
+static void rdm3_abb(orc_ctx* c, const double* L, const double* R, double* g) {
+    int n = c->n;
+    memset(g, 0, sizeof(double) * (size_t)n * n * n * n * n * n);
+    if (c->A.k < 1 || c->B.k < 2) return;
+    int64_t nbs = c->nbs;
+    uint64_t *Ka = NULL, *Kb = NULL;
+    int64_t nKa = hole_strings(n, c->A.k - 1, &Ka), nKb = hole_strings(n, c->B.k - 2, &Kb);
+    hentry* I1 = (hentry*)malloc(sizeof(hentry) * (size_t)n);
+    hentry* M2 = (hentry*)malloc(sizeof(hentry) * 2 * (size_t)binom(n, 2));
+    for (int64_t ka = 0; ka < nKa; ka++) {
+        int ni = hole_list(&c->A, Ka[ka], 1, I1);
+        for (int64_t kb = 0; kb < nKb; kb++) {
+            int nm = hole_list(&c->B, Kb[kb], 2, M2);
+            for (int x = 0; x < ni; x++) {
+                int p = I1[x].o[0];
+                const double* Cr = R + (int64_t)I1[x].I * nbs;
+                for (int u = 0; u < nm; u++) {
+                    int q = M2[u].o[0], r = M2[u].o[1];
+                    double cr = Cr[M2[u].I];
+                    if (cr == 0.0) continue;
+                    for (int y = 0; y < ni; y++) {
+                        int s = I1[y].o[0];
+                        const double* Cl = L + (int64_t)I1[y].I * nbs;
+                        for (int v = 0; v < nm; v++) {
+                            int t = M2[v].o[0], a = M2[v].o[1];
+                            double sign = I1[x].sign * I1[y].sign * M2[u].sign * M2[v].sign;
+                            g[SIX(p, q, r, s, t, a)] += sign * cr * Cl[M2[v].I];
+                        }
+                    }
+                }
+            }
+        }
+    }
+    free(I1); free(M2); free(Ka); free(Kb);
+}
+
+int orc_rdms3(void* h, const double* L, const double* R, double* g3aaa, double* g3aab, double* g3abb,
+              double* g3bbb) {
+    orc_ctx* c = (orc_ctx*)h;
+    if (c->n > 12) return fail("orc_rdms3: at most 12 orbitals");
+    rdm3_same(c, L, R, g3aaa, 1);
+    rdm3_aab(c, L, R, g3aab);
+    rdm3_abb(c, L, R, g3abb);
+    rdm3_same(c, L, R, g3bbb, 0);
+    return 0;
+}

@@ -56,6 +56,7 @@ def lib():
         L.orc_spin2.restype = C.c_double
         L.orc_spin2.argtypes = [vp, dp]
         L.orc_rdms.argtypes = [vp, dp, dp, C.c_int, dp, dp, dp, dp, dp]
+        L.orc_rdms3.argtypes = [vp, dp, dp, dp, dp, dp, dp]
         L.orc_last_error.restype = C.c_char_p
         _LIB = L
     return _LIB
@@ -162,6 +163,18 @@ class Oracle:
         g2aa = np.zeros((n,) * 4); g2ab = np.zeros((n,) * 4); g2bb = np.zeros((n,) * 4)
         lib().orc_rdms(self.h, _dp(cl), _dp(cr), level, _dp(g1a), _dp(g1b), _dp(g2aa), _dp(g2ab), _dp(g2bb))
         return {"g1a": g1a, "g1b": g1b, "g2aa": g2aa, "g2ab": g2ab, "g2bb": g2bb}
+
+    def rdms3(self, cl, cr=None):
+        """3-RDM blocks g3aaa, g3aab, g3abb, g3bbb (n^6 each) in the reference's index order and
+        orientation (FCIVector::compute_3rdm_*_same_irrep)."""
+        cr = cl if cr is None else cr
+        cl = np.ascontiguousarray(cl, dtype=np.float64)
+        cr = np.ascontiguousarray(cr, dtype=np.float64)
+        n = self.n
+        out = {k: np.zeros((n,) * 6) for k in ("g3aaa", "g3aab", "g3abb", "g3bbb")}
+        if lib().orc_rdms3(self.h, _dp(cl), _dp(cr), *[_dp(out[k]) for k in ("g3aaa", "g3aab", "g3abb", "g3bbb")]) < 0:
+            raise RuntimeError(lib().orc_last_error().decode())
+        return out
 
 
 def jacobi(A):

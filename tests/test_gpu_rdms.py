@@ -126,7 +126,7 @@ def test_rdm_errors_like_reference():
     with pytest.raises(RuntimeError, match="because nroot = 2"):
         s.rdms([(0, 2)], 2)
     with pytest.raises(RuntimeError):
-        s.rdms([(0, 0)], 3)
+        s.rdms([(0, 0)], 4)
     empty = s.rdms([(0, 1)], 0)[0]
     assert not hasattr(empty, "g1a")
 
