@@ -59,8 +59,10 @@ def dist_init(args):
         import torch
         import torch.distributed as dist
         from datetime import timedelta
-        torch.cuda.set_device(local)
+        # the reference arm is CPU work: gloo, no device; the GPU arms: NCCL, one GPU per rank
         backend = "gloo" if args.impl == "reference" else "nccl"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
         dist.init_process_group(backend, timeout=timedelta(seconds=600))
     return world, rank, local
 
@@ -76,7 +78,7 @@ def allmax(world, v):
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    t = torch.tensor([v], dtype=torch.float64, device="cuda" if dist.get_backend() == "nccl" else "cpu")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
