@@ -47,6 +47,7 @@ class FcibOptions(C.Structure):
         ("preconditioner", C.c_int),
         ("mixed_switch", C.c_double),
         ("same_spin_kernel", C.c_int),
+        ("spin_adapt", C.c_int),
     ]
 
 
@@ -90,6 +91,8 @@ SIGNATURES = {
     "fcib_rdms": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp]),
     "fcib_compute_rdms": (C.c_int, [_vp, _dp, _dp, C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp]),
     "fcib_rdms3": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _dp]),
+    "fcib_csf_coupling": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _dp, C.POINTER(C.c_uint32),
+                                    C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "fcib_compute_rdms3": (C.c_int, [_vp, _dp, _dp, C.c_int, _dp, _dp, _dp, _dp]),
     "fcib_num_strings": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_int64)]),
     "fcib_strings": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_uint32)]),

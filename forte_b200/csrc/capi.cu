@@ -68,6 +68,7 @@ void ensure_setup(Context& c) {
     FCIB_CHECK(c.has_state, FCIB_ERR_STATE, "state has not been set");
     if (c.tables_ready) return;
     c.mlp_tables_ready = false;
+    c.csf_ready = false;
     FCIB_CHECK(c.na <= c.n && c.nb <= c.n, FCIB_ERR_ARG, "more electrons than orbitals");
     bool fold = (c.na >= 1 && c.nb >= 1);
     c.tgtR16.release();
@@ -170,6 +171,7 @@ void fcib_default_options(fcib_options* o) {
     o->preconditioner = FCIB_PRECOND_DIAG;
     o->mixed_switch = 1.0e-4;
     o->same_spin_kernel = FCIB_SAME_TC;
+    o->spin_adapt = 0;
 }
 
 const char* fcib_last_error(void) { return g_last_error.c_str(); }

@@ -1,0 +1,198 @@
+// Spin adaptation (option spin_adapt; Forte's CI_SPIN_ADAPT, SpinAdapter in
+// forte/sparse_ci/ci_spin_adaptation.h:81-183, used by fci_solver.cc:136-141,246-253).
+//
+// The reference solves in a basis of configuration state functions (CSFs) of the target spin S.
+// This engine keeps the determinant basis and projects every new Davidson vector (guesses,
+// corrections, random fill-ins) onto the span of those CSFs.  H commutes with S^2, so the subspace
+// stays in the spin-S sector and the solver converges to the lowest roots of that sector: the
+// energies, eigenvectors and RDMs of the CSF solve.
+//
+// CSFs of a configuration (doubly occupied set D, open-shell set O, N = |O|) are the genealogical
+// couplings of the N open shells taken in orbital order (the published construction that adds one
+// spin 1/2 at a time with Clebsch-Gordan coefficients, e.g. Pauncz, "Spin Eigenfunctions"), times
+// the closed-shell pairs, which commute with the spin operators and with any pair of fermion
+// operators.  Written in this engine's determinants |D+Oa ; D+Ob> (alpha string, then beta string),
+// the coefficient of the spin pattern m over O (bit k set: the k-th open shell is alpha) is
+//     O_N[i][m] = (-1)^(number of beta open shells below an alpha open shell) * prod_k CG_k(i, m)
+// up to a sign common to the configuration.  So a configuration's projector is P = O_N^T O_N, the
+// same matrix for every configuration with N open shells, and configurations that cannot couple
+// to S (N < 2S) are projected to zero.
+#include "fcib_internal.h"
+
+namespace fcib {
+
+// <S' M-m; 1/2 m | S M> for adding one spin 1/2, in units of 1/2: twoS, twoM after the step,
+// dS = +-1 the change of 2S, dm = +-1 the change of 2M
+static double cg_half(int twoS, int twoM, int dS, int dm) {
+    if (dS == 1) return std::sqrt(0.5 * (twoS + dm * twoM) / (double)twoS);
+    return -dm * std::sqrt(0.5 * (twoS + 2 - dm * twoM) / (double)(twoS + 2));
+}
+
+// Coupling matrix of N open shells to 2S = twoS at 2Ms = twoMs: O[i * nd + m] for the f coupling
+// paths i (bit k set: the spin rises at step k) and the nd spin patterns m in increasing mask order
+static void csf_coupling(int N, int twoS, int twoMs, std::vector<double>& O, std::vector<uint32_t>& pats, int& f,
+                         int& nd) {
+    pats.clear();
+    std::vector<uint32_t> paths;
+    const int na_open = (N + twoMs) / 2;
+    for (uint32_t m = 0; m < (1u << N); m++) {
+        if (__builtin_popcount(m) == na_open) pats.push_back(m);
+        if (twoS > N || (N - twoS) % 2) continue;
+        int s = 0;
+        bool ok = true;
+        for (int k = 0; k < N && ok; k++) {
+            s += (m >> k & 1u) ? 1 : -1;
+            ok = s >= 0;
+        }
+        if (ok && s == twoS) paths.push_back(m);
+    }
+    f = (int)paths.size();
+    nd = (int)pats.size();
+    O.assign((size_t)f * nd, 0.0);
+    for (int i = 0; i < f; i++)
+        for (int j = 0; j < nd; j++) {
+            const uint32_t p = paths[i], m = pats[j];
+            double v = 1.0;
+            int s = 0, mm = 0, betas = 0, inv = 0;
+            for (int k = 0; k < N; k++) {
+                const int dS = (p >> k & 1u) ? 1 : -1;
+                const int dm = (m >> k & 1u) ? 1 : -1;
+                s += dS;
+                mm += dm;
+                if (std::abs(mm) > s) { v = 0.0; break; }
+                v *= cg_half(s, mm, dS, dm);
+                if (dm > 0) inv += betas;  // beta open shells below this alpha one
+                else betas++;
+            }
+            O[(size_t)i * nd + j] = (inv & 1) ? -v : v;
+        }
+}
+
+// One CTA per configuration of a group with N open shells: gather the coefficients of its nd
+// determinants, z = O x (f CSFs), scatter back x' = O^T z.  Every determinant belongs to exactly
+// one configuration, so the scatter has no conflicts.
+__global__ void k_csf_project(double* __restrict__ v, const uint32_t* __restrict__ conf, int nconf, int N, int nd,
+                              int f, const uint32_t* __restrict__ pats, const double* __restrict__ O, int n,
+                              int nbs) {
+    extern __shared__ __align__(16) unsigned char csf_smem[];
+    double* x = reinterpret_cast<double*>(csf_smem);  // [nd]
+    double* z = x + nd;                               // [f]
+    int* idx = reinterpret_cast<int*>(z + f);         // [nd]
+    for (int cf = blockIdx.x; cf < nconf; cf += gridDim.x) {
+        const uint32_t D = conf[2 * (size_t)cf], Om = conf[2 * (size_t)cf + 1];
+        __syncthreads();
+        for (int m = threadIdx.x; m < nd; m += blockDim.x) {
+            const uint32_t pat = pats[m];
+            uint32_t a = D, b = D, rest = Om;
+            for (int k = 0; k < N; k++) {
+                const uint32_t bit = rest & (0u - rest);  // k-th open shell in orbital order
+                rest ^= bit;
+                if (pat >> k & 1u) a |= bit;
+                else b |= bit;
+            }
+            const int id = (int)(d_rank(a, n) * (uint32_t)nbs + d_rank(b, n));
+            idx[m] = id;
+            x[m] = v[id];
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < f; i += blockDim.x) {
+            const double* row = O + (size_t)i * nd;
+            double s = 0.0;
+            for (int m = 0; m < nd; m++) s = fma(row[m], x[m], s);
+            z[i] = s;
+        }
+        __syncthreads();
+        for (int m = threadIdx.x; m < nd; m += blockDim.x) {
+            double s = 0.0;
+            for (int i = 0; i < f; i++) s = fma(O[(size_t)i * nd + m], z[i], s);
+            v[idx[m]] = s;
+        }
+    }
+}
+
+// Configuration groups of the current state and target spin (rebuilt when either changes)
+static void ensure_csf(Context& c) {
+    const int twoS = c.multiplicity - 1, twoMs = c.na - c.nb;
+    if (c.csf_ready && c.csf_twoS == twoS) return;
+    FCIB_CHECK(c.multiplicity >= 1, FCIB_ERR_ARG, "spin adaptation needs the multiplicity of the target state");
+    FCIB_CHECK(twoS >= std::abs(twoMs) && (twoS - twoMs) % 2 == 0, FCIB_ERR_ARG,
+               "spin adaptation: multiplicity incompatible with the number of alpha and beta electrons");
+    const int n = c.n, nd_occ_max = std::min(c.na, c.nb);
+    std::vector<std::vector<uint32_t>> byN(n + 1);
+    for (int d = 0; d <= nd_occ_max; d++) {
+        const int N = c.na + c.nb - 2 * d;
+        if (N > n - d) continue;
+        const uint32_t full = (n >= 32) ? 0xFFFFFFFFu : ((1u << n) - 1u);
+        const int64_t nD = host_binom().c[n][d];
+        for (int64_t di = 0; di < nD; di++) {
+            const uint32_t D = host_unrank((uint32_t)di, n, d);
+            const uint32_t free_m = full & ~D;
+            const int64_t nO = host_binom().c[n - d][N];
+            for (int64_t oi = 0; oi < nO; oi++) {
+                // oi-th N-subset of the free orbitals
+                const uint32_t sub = host_unrank((uint32_t)oi, n - d, N);
+                uint32_t Om = 0, fm = free_m;
+                for (int k = 0; k < n - d; k++) {
+                    const uint32_t bit = fm & (0u - fm);
+                    fm ^= bit;
+                    if (sub >> k & 1u) Om |= bit;
+                }
+                int h = 0;
+                for (int p = 0; p < n; p++)
+                    if (Om >> p & 1u) h ^= c.orbsym[p];
+                if (h != c.irrep) continue;
+                byN[N].push_back(D);
+                byN[N].push_back(Om);
+            }
+        }
+    }
+    c.csf.clear();
+    c.ncsf = 0;
+    for (int N = 0; N <= n; N++) {
+        if (byN[N].empty()) continue;
+        c.csf.emplace_back(new CsfGroup());
+        CsfGroup& g = *c.csf.back();
+        std::vector<double> O;
+        std::vector<uint32_t> pats;
+        csf_coupling(N, twoS, twoMs, O, pats, g.f, g.nd);
+        g.N = N;
+        g.nconf = (int)(byN[N].size() / 2);
+        g.conf.upload(byN[N], c.stream);
+        g.pats.upload(pats, c.stream);
+        if (!O.empty()) g.O.upload(O, c.stream);
+        c.ncsf += (int64_t)g.f * g.nconf;
+    }
+    FCIB_CUDA(cudaStreamSynchronize(c.stream));
+    c.csf_ready = true;
+    c.csf_twoS = twoS;
+}
+
+// v <- projection of v onto the spin-S sector (C1 layout)
+void csf_project(Context& c, double* v) {
+    ensure_csf(c);
+    for (auto& gp : c.csf) {
+        CsfGroup& g = *gp;
+        const size_t smem = (size_t)g.nd * 12 + (size_t)g.f * 8;
+        FCIB_CHECK(smem + 1024 <= (size_t)c.smem_optin, FCIB_ERR_UNSUPPORTED, "spin adaptation: configuration too large");
+        FCIB_CUDA(cudaFuncSetAttribute(k_csf_project, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const int grid = std::min(g.nconf, 8 * c.num_sms);
+        k_csf_project<<<grid, g.nd > 64 ? 256 : 64, smem, c.stream>>>(v, g.conf.p, g.nconf, g.N, g.nd, g.f, g.pats.p,
+                                                                       g.f > 0 ? g.O.p : nullptr, c.n, (int)c.nbs);
+        FCIB_KCHECK();
+    }
+}
+
+}  // namespace fcib
+
+// Host-only access to the coupling matrix (no device needed): O[f][nd] and the spin patterns.
+// Returns FCIB_ERR_ARG when the sizes do not fit the caller's capacity cap (f * nd and nd).
+extern "C" int fcib_csf_coupling(int N, int twoS, int twoMs, int cap, double* O, uint32_t* pats, int* f, int* nd) {
+    if (N < 0 || N > 20 || !f || !nd) return FCIB_ERR_ARG;
+    std::vector<double> o;
+    std::vector<uint32_t> p;
+    fcib::csf_coupling(N, twoS, twoMs, o, p, *f, *nd);
+    if ((size_t)cap < o.size() || (size_t)cap < p.size()) return FCIB_ERR_ARG;
+    if (O) std::copy(o.begin(), o.end(), O);
+    if (pats) std::copy(p.begin(), p.end(), pats);
+    return FCIB_OK;
+}

@@ -599,6 +599,9 @@ static void project_out(Context& c, std::vector<SparseDev>& bad, std::vector<dou
             k_project_sparse<<<1, 256, 0, c.stream>>>(V[k], b.idx.p, b.val.p, b.cnt);
             FCIB_KCHECK();
         }
+    // spin adaptation: every vector that enters the basis is kept in the target spin sector
+    if (c.opt.spin_adapt)
+        for (int k = 0; k < nvec; k++) csf_project(c, V[k]);
 }
 
 double spin2_device(Context& c, const double* C) {
@@ -931,7 +934,7 @@ void dl_solve(Context& c) {
         }
         // 4. project out undesired roots; normalisation is folded into Gram-Schmidt
         project_out(c, bad, r, nroot);
-        if (!bad.empty())
+        if (!bad.empty() || o.spin_adapt)
             for (int k = 0; k < nroot; k++) cnorm[k] = std::sqrt(ops.norm2(r[k]));
         // 5./6. convergence
         int ne = 0, nr = 0;

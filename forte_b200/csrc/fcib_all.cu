@@ -11,3 +11,4 @@
 #include "mlp.cu"
 #include "batch.cu"
 #include "noalloc.cu"
+#include "csf.cu"

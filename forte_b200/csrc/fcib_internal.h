@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include <array>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -126,6 +127,14 @@ struct EventPair {
 // ------------------------------------------------------------------------------------------
 // engine context
 // ------------------------------------------------------------------------------------------
+// configurations with N open shells of the spin-adapted space (csf.cu)
+struct CsfGroup {
+    int N = 0, f = 0, nd = 0, nconf = 0;  // open shells, CSFs and determinants per configuration
+    DBuf<uint32_t> conf;                  // [nconf][2]: doubly occupied mask, open-shell mask
+    DBuf<uint32_t> pats;                  // [nd] spin patterns over the open shells (bit k: alpha)
+    DBuf<double> O;                       // [f][nd] coupling coefficients
+};
+
 struct Context {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -189,6 +198,11 @@ struct Context {
     // vectors its first guess asked to project out
     bool dl_prev = false;
     bool restarted = false;  // the last solve restarted from the previous solution
+    // spin adaptation (csf.cu): configuration groups of the current state and target spin
+    std::vector<std::unique_ptr<CsfGroup>> csf;
+    bool csf_ready = false;
+    int csf_twoS = -1;
+    int64_t ncsf = 0;
     std::vector<int64_t> dl_prev_space;
     std::vector<std::vector<std::pair<int64_t, double>>> dl_bad;
     std::vector<double> dl_lambda_old;  // eigenvalues of the previous solve's last iteration
@@ -212,6 +226,8 @@ inline void ensure_counter(Context& c) {
 
 // kernels / launchers (sigma.cu)
 void prepare_integrals(Context& c);
+// csf.cu: v <- its projection onto the spin sector of the target multiplicity
+void csf_project(Context& c, double* v);
 void sigma_fp64(Context& c, const double* C, double* S);
 void sigma_mixed(Context& c, const double* C, double* S, bool three);
 void apply_mask(Context& c, double* v);

@@ -68,6 +68,8 @@ typedef struct fcib_options {
     int preconditioner;        /* FCIB_PRECOND_* */
     double mixed_switch;       /* mixed modes: residual norm at which sigma switches to FP64 */
     int same_spin_kernel;      /* mixed modes: FCIB_SAME_TC (default) or FCIB_SAME_CUDA_CORES */
+    int spin_adapt;            /* CI_SPIN_ADAPT: keep the Davidson space in the spin sector of the
+                                  state's multiplicity (projection onto its CSFs); default 0 */
 } fcib_options;
 
 typedef struct fcib_ctx fcib_ctx;
@@ -135,6 +137,11 @@ int fcib_compute_rdms(fcib_ctx* ctx, const double* left, const double* right, in
  * For left == right these are the usual 3-RDMs.  spin_free: g3aaa receives the spin-free
  * G3 = aaa + aab + aab(prqsut) + aab(qrptus) + abb + abb(qprtsu) + abb(rpqust) + bbb (:127-130)
  * and the other pointers are ignored.  Any output may be NULL. */
+/* Coupling coefficients of the spin adaptation (host only, no device): N open shells coupled to
+ * 2S = twoS at 2Ms = twoMs; O[f][nd] for the f genealogical CSFs over the nd spin patterns pats[nd]
+ * (bit k set: the k-th open shell in orbital order is alpha), in this engine's determinant phase
+ * convention (alpha string, then beta string).  cap: capacity of O and pats in elements. */
+int fcib_csf_coupling(int N, int twoS, int twoMs, int cap, double* O, uint32_t* pats, int* f, int* nd);
 int fcib_rdms3(fcib_ctx* ctx, int root_left, int root_right, int spin_free, double* g3aaa, double* g3aab,
                double* g3abb, double* g3bbb);
 int fcib_compute_rdms3(fcib_ctx* ctx, const double* left, const double* right, int spin_free, double* g3aaa,
