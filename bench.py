@@ -7,7 +7,7 @@ h symmetric with diagonal ~ U[-2, 1] (sorted, +0.3 Eh on orbitals 8..15) and off
 (pq|rs) = sum_L B^L_pq B^L_rs with L = 48 symmetric B^L ~ N(0, 0.15), numpy PCG64(seed 1).
 
 One step = one complete Davidson-Liu solve from the initial guess to convergence
-(E_CONVERGENCE 1e-9, R_CONVERGENCE 1e-5 judged by the FP64 sigma), timed with CUDA events on the
+(E_CONVERGENCE 1e-9, R_CONVERGENCE 1e-5 certified by the FP64 sigma), timed with CUDA events on the
 engine's stream.  The CI vectors (1.3 GB each) are far larger than L2, so no flush is needed.
 One FP64 solve of the same problem gives the reference energy (|dE| check) and the FP64 time.
 

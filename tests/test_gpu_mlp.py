@@ -78,7 +78,7 @@ def test_trained_network_improves_corrections_on_unseen_instance():
 
 
 def test_davidson_with_learned_preconditioner_reaches_fp64_energy():
-    """Same energy as the diagonal preconditioner (every converged energy is judged by the FP64
+    """Same energy as the diagonal preconditioner (every converged energy is certified by the FP64
     sigma); the iteration counts of both are printed -- on these synthetic instances the learned
     factor does not reduce them."""
     ints = synthetic(10, 30, 4242)
