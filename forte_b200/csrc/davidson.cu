@@ -730,7 +730,10 @@ void dl_solve(Context& c) {
     // 312-316) restarts from the first nroot vectors, recomputing their sigma with the current
     // integrals, and keeps projecting out the first run's unwanted roots.
     int num_guess_states = (int)std::min<int64_t>((int64_t)o.guess_per_root * nroot, Neff);
-    std::vector<int64_t> space = {c.n, c.na, c.nb, c.irrep, c.nirrep, (int64_t)N, Neff, nroot, m};
+    // the spin sector is part of the space: with spin adaptation the previous vectors must come
+    // from a solve of the same multiplicity that was itself spin adapted
+    std::vector<int64_t> space = {c.n, c.na, c.nb, c.irrep, c.nirrep, (int64_t)N, Neff, nroot, m,
+                                  o.spin_adapt ? c.multiplicity : -1};
     for (int x : c.orbsym) space.push_back(x);
     const bool restart = c.dl_prev && c.dl_prev_space == space &&
                          (int64_t)num_guess_states * o.dets_per_guess < Neff;
