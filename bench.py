@@ -266,6 +266,66 @@ def run_sigma(args, world, rank, local):
         dist.destroy_process_group()
 
 
+def run_configs(args, world, rank, local):
+    """Time to solution of the two small workloads: CAS(8,8) (4,900 determinants, 1 root, FP64,
+    synthetic L = 24; also solved by the CPU oracle on one core) and CAS(12,12) (853,776
+    determinants, 3 roots, L = 36, FP64 vs mixed, plus the 1-/2-RDMs of the three roots).  Every
+    step is a fresh solve (no restart), timed with CUDA events on the engine stream."""
+    import torch
+    from forte_b200 import FCISolver, StateInfo, build, synthetic
+    build.build()
+    torch.cuda.set_device(local)
+    out = {}
+    # CAS(8,8)
+    ints8 = synthetic(8, 24, SEED)
+    opts = {"E_CONVERGENCE": 1e-9, "R_CONVERGENCE": 1e-6}
+    s8 = FCISolver(StateInfo(4, 4, 0), 1, ints8, opts, device=local)
+    st8 = torch.cuda.ExternalStream(s8.stream())
+    for _ in range(args.warmup):
+        solve_once(s8, torch, st8)
+    t8 = [solve_once(s8, torch, st8) for _ in range(args.steps)]
+    cpu8 = None
+    if rank == 0 and not args.no_cpu:
+        from oracle.oracle import Oracle
+        o = Oracle(8, 4, 4)
+        o.set_integrals(ints8)
+        t0 = time.perf_counter()
+        r = o.solve(nroot=1, multiplicity=0, e_conv=1e-9, r_conv=1e-6)
+        cpu8 = {"seconds": time.perf_counter() - t0, "iterations": r["iterations"],
+                "energy_difference": abs(r["energies"][0] - s8.energies()[0]), "cores": 1, "kind": "port"}
+    out["cas8_fp64"] = {"seconds": allmax(world, statistics.mean(t8)), "iterations": s8.iterations(),
+                        "energy": s8.energies()[0], "cpu_oracle": cpu8}
+    # CAS(12,12), 3 roots
+    ints12 = synthetic(12, 36, SEED)
+    opts12 = {"E_CONVERGENCE": 1e-10, "R_CONVERGENCE": 1e-6, "DL_SUBSPACE_PER_ROOT": 8}
+    res = {}
+    for prec in ("FP64", "MIXED"):
+        s = FCISolver(StateInfo(6, 6, 0), 3, ints12, dict(opts12, FCI_PRECISION=prec), device=local)
+        st = torch.cuda.ExternalStream(s.stream())
+        for _ in range(args.warmup):
+            solve_once(s, torch, st)
+        ts = [solve_once(s, torch, st) for _ in range(args.steps)]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s.rdms([(0, 0), (1, 1), (2, 2)], 2)
+        rdm_s = time.perf_counter() - t0
+        res[prec] = {"seconds": allmax(world, statistics.mean(ts)), "iterations": s.iterations(),
+                     "energies": s.energies(), "rdms_3_roots_seconds": rdm_s}
+        del s
+        torch.cuda.empty_cache()
+    de = max(abs(a - b) for a, b in zip(res["MIXED"]["energies"], res["FP64"]["energies"]))
+    out["cas12_3roots"] = dict(res, max_energy_difference=de,
+                               speedup_mixed_vs_fp64=res["FP64"]["seconds"] / res["MIXED"]["seconds"])
+    if rank == 0:
+        print(json.dumps({
+            "metric": "time to solution of the CAS(8,8) and CAS(12,12) workloads", "value": res["MIXED"]["seconds"],
+            "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64 / tf32x3", "data": "synthetic",
+            "config": {"workload": "CAS(8,8) L=24 1 root FP64; CAS(12,12) L=36 3 roots FP64 vs mixed",
+                       "parallelism": f"replicas x{world}"},
+            **out}), flush=True)
+
+
 def run_precond(args, world, rank, local):
     """Learned vs diagonal preconditioner: Davidson at CAS(14,14) (11,778,624 determinants, Ms = 0,
     2 roots, synthetic L = 42), same precision for both, every energy certified by FP64 sigma."""
@@ -418,10 +478,11 @@ def main():
     ap.add_argument("--batch-sizes", default="6,7,8,9,10")
     ap.add_argument("--maxiter", type=int, default=0, help="batch mode: Davidson iteration cap (0 = 200)")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--mode", default="solve", choices=["solve", "sigma", "precond", "batch"],
+    ap.add_argument("--mode", default="solve", choices=["solve", "sigma", "precond", "batch", "configs"],
                     help="solve: the Davidson time-to-solution metric; sigma: sigma builds/s at CAS(n,n); "
                          "precond: learned vs diagonal preconditioner at CAS(14,14), 2 roots; "
-                         "batch: batched CASCI instances/s")
+                         "batch: batched CASCI instances/s; configs: time to solution at CAS(8,8) and "
+                         "CAS(12,12) (3 roots, FP64 vs mixed)")
     ap.add_argument("--n", type=int, default=16, help="active orbitals of the sigma mode")
     args = ap.parse_args()
     world, rank, local = dist_init(args)
@@ -436,6 +497,9 @@ def main():
         return
     if args.mode == "batch":
         run_batch(args, world, rank, local)
+        return
+    if args.mode == "configs":
+        run_configs(args, world, rank, local)
         return
 
     import torch
