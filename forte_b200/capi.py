@@ -117,6 +117,10 @@ SIGNATURES = {
     "fcib_batch_solve": (C.c_int, [_vp, _dp, C.POINTER(C.c_int), C.POINTER(C.c_int), _dp]),
     "fcib_batch_tune": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int), _dp]),
     "fcib_captured_residual": (C.c_int, [_vp, C.c_int, _dp, _dp, C.POINTER(C.c_int)]),
+    "fcib_fp64_peak": (C.c_int, [C.c_int, _dp, _dp]),
+    "fcib_transition_rdms": (C.c_int, [_vp, C.c_int, _vp, C.c_int, C.c_int, C.c_int, _dp, _dp]),
+    "fcib_max_abs_elements": (C.c_int, [_vp, C.c_int, C.c_int, _dp, _dp, C.POINTER(C.c_int), C.POINTER(C.c_int64),
+                                        C.POINTER(C.c_int64), C.POINTER(C.c_int)]),
 }
 MLP_NWEIGHTS = 10689
 

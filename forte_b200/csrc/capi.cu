@@ -318,6 +318,8 @@ int fcib_size(fcib_ctx* ctx, int64_t* ndet) {
     });
 }
 
+static void print_solutions(Context& c);
+
 int fcib_solve(fcib_ctx* ctx, double* energies, double* spin2, int* iterations) {
     if (!ctx) { set_error("null context"); return FCIB_ERR_ARG; }
     int rc = guarded(ctx, [&] {
@@ -329,18 +331,157 @@ int fcib_solve(fcib_ctx* ctx, double* energies, double* spin2, int* iterations) 
             if (spin2) spin2[k] = c.spin2[k];
         }
         if (iterations) *iterations = c.iterations;
+        if (c.opt.print >= 1 && (c.converged || !c.opt.die_if_not_converged)) print_solutions(c);
     });
     if (rc == FCIB_OK && !ctx->c.converged && ctx->c.opt.die_if_not_converged) {
-        set_error("Davidson-Liu solver did not converge. Try to increase DL_MAXITER, DL_SUBSPACE_PER_ROOT or DL_GUESS_PER_ROOT");
+        // the reference's message (forte/fci/fci_solver.cc:269-276)
+        set_error("Davidson-Liu solver did not converge.\nPlease try to increase the number of "
+                  "Davidson-Liu iterations (DL_MAXITER). You can also try to increase:\n - the "
+                  "maximum "
+                  "size of the subspace (DL_SUBSPACE_PER_ROOT)"
+                  "\n - the number of guess states (DL_GUESS_PER_ROOT)");
         return FCIB_ERR_NOT_CONVERGED;
     }
     return rc;
+}
+
+// FCIVector::max_abs_elements (forte/fci/fci_vector_h_diag.cc:37-68): the num_dets largest |C| of a
+// root in the reference's order (descending |C|; equal values in FCIVector flat order, which the
+// reference's insertion keeps), each as (|C|, C, alpha irrep, alpha and beta string address within
+// their irreps); slots past the nonzero elements hold zeros, as the reference's preset tuples do.
+static void max_abs_elements(Context& c, int root, int num_dets, std::vector<double>& absv, std::vector<double>& val,
+                             std::vector<int>& irr, std::vector<int64_t>& ia, std::vector<int64_t>& ib) {
+    const int64_t N = c.ndet;
+    const int64_t nflat = c.nirrep <= 1 ? N : (int64_t)c.block_to_c1.size();
+    num_dets = (int)std::min<int64_t>(num_dets, nflat);
+    absv.assign(num_dets, 0.0);
+    val.assign(num_dets, 0.0);
+    irr.assign(num_dets, 0);
+    ia.assign(num_dets, 0);
+    ib.assign(num_dets, 0);
+    if (num_dets <= 0) return;
+    const double* x = c.b.p + (size_t)root * N;
+    double* keys = c.tmp.p;  // scratch once the solve has finished
+    k_neg_abs<<<4 * c.num_sms, 256, 0, c.stream>>>(x, keys, (size_t)N);
+    FCIB_KCHECK();
+    auto sel = lowest_keys(c, keys, num_dets);
+    // C1 index -> (alpha irrep, addresses within the irrep blocks, FCIVector flat position)
+    std::vector<uint32_t> sa(c.nas), sb(c.nbs);
+    FCIB_CUDA(cudaMemcpy(sa.data(), c.A.str.p, 4 * c.nas, cudaMemcpyDeviceToHost));
+    FCIB_CUDA(cudaMemcpy(sb.data(), c.B.str.p, 4 * c.nbs, cudaMemcpyDeviceToHost));
+    auto sym = [&](uint32_t s) {
+        int h = 0;
+        for (int i = 0; i < c.n; i++)
+            if (s >> i & 1u) h ^= c.orbsym[i];
+        return h;
+    };
+    std::vector<int> ha(c.nas), hb(c.nbs);
+    std::vector<int64_t> ra(c.nas), rb(c.nbs), pa(c.nas), pb(c.nbs);
+    {
+        std::vector<int64_t> cnta(8, 0), cntb(8, 0);
+        for (int64_t i = 0; i < c.nas; i++) { ha[i] = c.nirrep > 1 ? sym(sa[i]) : 0; ra[i] = cnta[ha[i]]++; }
+        for (int64_t i = 0; i < c.nbs; i++) { hb[i] = c.nirrep > 1 ? sym(sb[i]) : 0; rb[i] = cntb[hb[i]]++; }
+        // start of each alpha irrep block in flat order
+        std::vector<int64_t> blk(9, 0);
+        for (int h = 0; h < 8; h++) blk[h + 1] = blk[h] + cnta[h] * cntb[h ^ (c.nirrep > 1 ? c.irrep : 0)];
+        for (int64_t i = 0; i < c.nas; i++) pa[i] = blk[ha[i]] + ra[i] * cntb[ha[i] ^ (c.nirrep > 1 ? c.irrep : 0)];
+    }
+    std::vector<std::pair<std::pair<double, int64_t>, int64_t>> order;  // ((-|C|, flat), c1)
+    for (auto& e : sel) {
+        const int64_t i = e.second / c.nbs, j = e.second % c.nbs;
+        order.push_back({{e.first, pa[i] + rb[j]}, e.second});
+    }
+    std::sort(order.begin(), order.end());
+    std::vector<double> h(order.size());
+    for (size_t t = 0; t < order.size(); t++)
+        FCIB_CUDA(cudaMemcpyAsync(&h[t], x + order[t].second, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    FCIB_CUDA(cudaStreamSynchronize(c.stream));
+    for (int t = 0; t < num_dets && t < (int)order.size(); t++) {
+        const double a = -order[t].first.first;
+        if (!(a > 0.0)) break;
+        const int64_t i = order[t].second / c.nbs, j = order[t].second % c.nbs;
+        absv[t] = a;
+        val[t] = h[t];
+        irr[t] = ha[i];
+        ia[t] = ra[i];
+        ib[t] = rb[j];
+    }
+}
+
+// FCISolver::print_solutions (forte/fci/fci_solver.cc:316-367): per root, the determinants with
+// |C| >= 0.01 among the 100 largest, as occupation strings per irrep block (2, a, b, 0), then the
+// root's energy and <S^2>.
+static void print_solutions(Context& c) {
+    std::vector<double> absv, val;
+    std::vector<int> irr;
+    std::vector<int64_t> ia, ib;
+    std::vector<uint32_t> sa(c.nas), sb(c.nbs);
+    FCIB_CUDA(cudaMemcpy(sa.data(), c.A.str.p, 4 * c.nas, cudaMemcpyDeviceToHost));
+    FCIB_CUDA(cudaMemcpy(sb.data(), c.B.str.p, 4 * c.nbs, cudaMemcpyDeviceToHost));
+    // strings of each irrep in string order, to turn (irrep, address) back into a string
+    auto sym = [&](uint32_t s) {
+        int h = 0;
+        for (int i = 0; i < c.n; i++)
+            if (s >> i & 1u) h ^= c.orbsym[i];
+        return h;
+    };
+    std::vector<std::vector<uint32_t>> bya(8), byb(8);
+    for (auto s : sa) bya[c.nirrep > 1 ? sym(s) : 0].push_back(s);
+    for (auto s : sb) byb[c.nirrep > 1 ? sym(s) : 0].push_back(s);
+    for (int r = 0; r < c.nroot; r++) {
+        printf("\n\n  ==> Root No. %d <==\n", r);
+        max_abs_elements(c, r, 100, absv, val, irr, ia, ib);
+        for (size_t t = 0; t < absv.size(); t++) {
+            if (absv[t] < 0.01) continue;
+            const uint32_t A = bya[irr[t]][ia[t]];
+            const uint32_t B = byb[irr[t] ^ (c.nirrep > 1 ? c.irrep : 0)][ib[t]];
+            printf("\n    ");
+            for (int h = 0; h < std::max(1, c.nirrep); h++) {
+                int cnt = 0;
+                for (int i = 0; i < c.n; i++) {
+                    if ((c.nirrep > 1 ? c.orbsym[i] : 0) != h) continue;
+                    const bool a = A >> i & 1u, b = B >> i & 1u;
+                    if (a == b) printf("%d", a ? 2 : 0);
+                    else printf("%c", a ? 'a' : 'b');
+                    cnt++;
+                }
+                if (cnt) printf(" ");
+            }
+            printf("%15.8f", val[t]);
+        }
+        printf("\n\n    Total Energy: %20.12f, <S^2>: %8.6f", c.energies[r], c.spin2[r]);
+    }
+    printf("\n");
+    fflush(stdout);
 }
 
 int fcib_reset_guess(fcib_ctx* ctx) {
     if (!ctx) { set_error("null context"); return FCIB_ERR_ARG; }
     ctx->c.dl_prev = false;
     return FCIB_OK;
+}
+
+int fcib_max_abs_elements(fcib_ctx* ctx, int root, int num_dets, double* abs_c, double* c_out, int* alfa_irrep,
+                          int64_t* alfa_address, int64_t* beta_address, int* count) {
+    if (!ctx) { set_error("null context"); return FCIB_ERR_ARG; }
+    return guarded(ctx, [&] {
+        Context& c = ctx->c;
+        FCIB_CHECK(c.solved, FCIB_ERR_STATE, "no solution available");
+        FCIB_CHECK(root >= 0 && root < c.nroot, FCIB_ERR_ARG, "root out of range");
+        FCIB_CHECK(num_dets >= 0, FCIB_ERR_ARG, "negative determinant count");
+        std::vector<double> a, v;
+        std::vector<int> h;
+        std::vector<int64_t> ia, ib;
+        max_abs_elements(c, root, num_dets, a, v, h, ia, ib);
+        for (size_t t = 0; t < a.size(); t++) {
+            if (abs_c) abs_c[t] = a[t];
+            if (c_out) c_out[t] = v[t];
+            if (alfa_irrep) alfa_irrep[t] = h[t];
+            if (alfa_address) alfa_address[t] = ia[t];
+            if (beta_address) beta_address[t] = ib[t];
+        }
+        if (count) *count = (int)a.size();
+    });
 }
 
 int fcib_get_vector(fcib_ctx* ctx, int root, double* out) {
@@ -422,6 +563,55 @@ int fcib_rdms(fcib_ctx* ctx, int root_left, int root_right, int level, int spin_
         RdmBlocks blk;
         compute_rdms(c, c.b.p + (size_t)root_left * c.ndet, c.b.p + (size_t)root_right * c.ndet, level, blk);
         rdms_to_outputs(blk, level, spin_free, g1a, g1b, g2aa, g2ab, g2bb);
+    });
+}
+
+// FCISolver::transition_rdms(root_list, method2, max_rdm_level, type) for one pair
+// (forte/fci/fci_solver_transition_rdms.cc:37-109) and compute_transition_rdms /
+// compute_1rdm_different_irrep (fci_vector_transition_rdm.cc:43-165): <left root| a+_p a_q |right root>
+// between the solutions of two contexts whose states may belong to different irreps.  Both vectors
+// live on the device in the full C1 layout (zero outside each state's irrep), so the one kernel pass
+// over the C1 space sums exactly the irrep blocks the reference loops over.
+int fcib_transition_rdms(fcib_ctx* left, int root_left, fcib_ctx* right, int root_right, int level,
+                         int spin_free, double* g1a, double* g1b) {
+    if (!left || !right) { set_error("null context"); return FCIB_ERR_ARG; }
+    return guarded(left, [&] {
+        Context& c = left->c;
+        const Context& r = right->c;
+        FCIB_CHECK(c.solved && r.solved, FCIB_ERR_STATE, "FCIVector is not assigned. Cannot compute RDMs.");
+        FCIB_CHECK(level <= 3 && level >= 1, FCIB_ERR_ARG, "Invalid max_rdm_level, required 1 <= max_rdm_level <= 3.");
+        FCIB_CHECK(root_left >= 0 && root_right >= 0, FCIB_ERR_ARG, "negative root index");
+        if (root_left >= c.nroot || root_right >= r.nroot)
+            throw Error{FCIB_ERR_ARG, "Cannot compute RDMs <" + std::to_string(root_left) + "| ... |" +
+                                          std::to_string(root_right) + "> (0-based) because nroot_left = " +
+                                          std::to_string(c.nroot) + " and nroot_right = " + std::to_string(r.nroot)};
+        FCIB_CHECK(c.n == r.n, FCIB_ERR_ARG,
+                   "FCI transition RDMs: The number of MOs must be the same in the two wave functions.");
+        FCIB_CHECK(c.na == r.na && c.nb == r.nb, FCIB_ERR_ARG,
+                   "FCI transition RDMs: The number of alfa and beta electrons must be the same in the two wave "
+                   "functions.");
+        FCIB_CHECK(c.device == r.device, FCIB_ERR_UNSUPPORTED, "transition RDMs: the two contexts use different devices");
+        FCIB_CHECK(level < 2, FCIB_ERR_UNSUPPORTED,
+                   "Transition RDMs of order 2 or higher are not implemented in FCISolver (and more generally in "
+                   "Forte).");
+        const int n = c.n;
+        std::vector<double> a((size_t)n * n, 0.0), b((size_t)n * n, 0.0);
+        // the reference returns empty blocks when the left state has no alpha electrons, for both
+        // spins (compute_1rdm_different_irrep takes nb from the alpha address), and so does this call
+        if (c.na >= 1) {
+            FCIB_CUDA(cudaStreamSynchronize(r.stream));
+            RdmBlocks blk;
+            compute_rdms(c, c.b.p + (size_t)root_left * c.ndet, r.b.p + (size_t)root_right * r.ndet, 1, blk);
+            a = blk.g1a;
+            b = blk.g1b;
+        }
+        if (spin_free) {
+            if (g1a)
+                for (size_t i = 0; i < a.size(); i++) g1a[i] = a[i] + b[i];
+        } else {
+            if (g1a) std::copy(a.begin(), a.end(), g1a);
+            if (g1b) std::copy(b.begin(), b.end(), g1b);
+        }
     });
 }
 

@@ -169,6 +169,9 @@ static void ensure_csf(Context& c) {
 
 // v <- projection of v onto the spin-S sector (C1 layout)
 void csf_project(Context& c, double* v) {
+    // k_csf_project keeps determinant indices as int in shared memory
+    FCIB_CHECK(c.ndet < ((int64_t)1 << 31), FCIB_ERR_UNSUPPORTED,
+               "spin adaptation: more than 2^31 - 1 determinants");
     ensure_csf(c);
     for (auto& gp : c.csf) {
         CsfGroup& g = *gp;

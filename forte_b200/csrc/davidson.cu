@@ -616,7 +616,9 @@ double spin2_device(Context& c, const double* C) {
 
 // lowest `count` diagonal entries ordered by (value, address), like the insertion list of
 // FCISolver::initial_guess_generate_dets (fci_solver_initial_guess.cc:44-69)
-static std::vector<std::pair<double, int64_t>> lowest_diagonal(Context& c, int count) {
+// the `count` smallest keys[] of the determinants in the target irrep with their C1 indices, sorted by
+// (key, index); ties at the boundary are resolved by the index
+std::vector<std::pair<double, int64_t>> lowest_keys(Context& c, const double* keys, int count) {
     const size_t N = (size_t)c.ndet;
     const uint8_t* mask = (c.nirrep > 1) ? c.mask.p : nullptr;
     DBuf<unsigned int> hist;
@@ -626,7 +628,7 @@ static std::vector<std::pair<double, int64_t>> lowest_diagonal(Context& c, int c
     int grid = 4 * c.num_sms;
     for (int shift = 56; shift >= 0; shift -= 8) {
         FCIB_CUDA(cudaMemsetAsync(hist.p, 0, 256 * sizeof(unsigned int), c.stream));
-        k_radix_hist<<<grid, 256, 0, c.stream>>>(c.hdiag.p, mask, N, prefix, pmask, shift, hist.p);
+        k_radix_hist<<<grid, 256, 0, c.stream>>>(keys, mask, N, prefix, pmask, shift, hist.p);
         FCIB_KCHECK();
         unsigned int h[256];
         FCIB_CUDA(cudaMemcpyAsync(h, hist.p, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
@@ -650,12 +652,12 @@ static std::vector<std::pair<double, int64_t>> lowest_diagonal(Context& c, int c
     ev.alloc(cap);
     ei.alloc(cap);
     FCIB_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(int), c.stream));
-    k_collect_le<<<grid, 256, 0, c.stream>>>(c.hdiag.p, mask, N, prefix, cap, cnt.p, ev.p, ei.p);
+    k_collect_le<<<grid, 256, 0, c.stream>>>(keys, mask, N, prefix, cap, cnt.p, ev.p, ei.p);
     FCIB_KCHECK();
     int hc = 0;
     FCIB_CUDA(cudaMemcpyAsync(&hc, cnt.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
     FCIB_CUDA(cudaStreamSynchronize(c.stream));
-    FCIB_CHECK(hc <= cap, FCIB_ERR_NUMERIC, "too many degenerate diagonal entries for the guess selection");
+    FCIB_CHECK(hc <= cap, FCIB_ERR_NUMERIC, "too many degenerate entries for the lowest-k selection");
     std::vector<double> he(hc);
     std::vector<int64_t> hi(hc);
     FCIB_CUDA(cudaMemcpy(he.data(), ev.p, sizeof(double) * hc, cudaMemcpyDeviceToHost));
@@ -665,6 +667,14 @@ static std::vector<std::pair<double, int64_t>> lowest_diagonal(Context& c, int c
     std::sort(v.begin(), v.end());
     if ((int)v.size() > count) v.resize(count);
     return v;
+}
+static std::vector<std::pair<double, int64_t>> lowest_diagonal(Context& c, int count) {
+    return lowest_keys(c, c.hdiag.p, count);
+}
+
+__global__ void k_neg_abs(const double* __restrict__ x, double* __restrict__ out, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = -fabs(x[i]);
 }
 
 static double now_ms() {

@@ -161,10 +161,13 @@ struct Context {
     DBuf<uint8_t> mask;   // determinant in target irrep (only when nirrep > 1)
     // work vectors
     DBuf<double> ct, st;  // transposed C and sigma for beta same-spin terms
-    DBuf<uint16_t> tgtR16; // beta replacement targets [pair/8][string][pair%8] for the tensor-core kernel
+    DBuf<uint16_t> tgtR16; // beta replacement targets [column/8][string][column%8] for the tensor-core kernel
+    DBuf<int> tc_perm;     // pair of each tensor-core column: off-diagonal pairs, then the diagonal ones
     DBuf<float> tf_hi;        // interleaved (tf32 hi, tf32 lo) pairs of the sigma input (mixed path)
     DBuf<float> c32, ct32;    // FP32 copy of the sigma input and its transpose (mixed same-spin)
-    DBuf<float> s32a, st32;   // FP32 same-spin sigma parts: alpha (row-major), beta (transposed)
+    DBuf<unsigned long long> s64a, st64;  // mixed same-spin sigma parts, int64 fixed point: alpha
+                                          // (row-major), beta (transposed)
+    double same_mmax = 0.0;   // max |same-spin block element| (fixed-point grid of those sums)
     bool c32_ready = false;   // c32 holds the current sigma input (written by the tensor-core split)
     float vmax = 0.0f;    // max |V| (fixed-point grid of the tensor-core scatter)
     DBuf<double> hdiag;
@@ -217,6 +220,11 @@ struct Context {
     std::vector<double> cap_lambda;  // iteration, ms, lambda_0, max residual, fp64 basis
 };
 
+// counter slots: 0 opposite-spin row counter, 1 its timeout flag, 2 CUDA-core group counter,
+// 3 bits of max|C| of the sigma input, 4 tensor-core group counter, 5 its timeout flag,
+// 6 exponent el of the mixed same-spin fixed-point grid 2^-el
+constexpr int kSlotCmax = 3;
+constexpr int kSlotSameGrid = 6;
 // the work counters and error flags of the persistent kernels, zeroed when first allocated
 inline void ensure_counter(Context& c) {
     if (c.counter.p) return;
@@ -252,6 +260,7 @@ void compute_rdms3(Context& c, const double* L, const double* R, Rdm3Blocks& out
 void mlp_apply(Context& c, double* t, double lambda, double rnorm, double tnorm);
 // davidson.cu
 void dl_solve(Context& c);
+std::vector<std::pair<double, int64_t>> lowest_keys(Context& c, const double* keys, int count);
 double spin2_device(Context& c, const double* C);
 
 }  // namespace fcib

@@ -10,8 +10,13 @@
 // partial sums and the reduced result live in a file-scope device array instead of buffers
 // allocated per call.  Host code cannot use that array's name as a device address, so the
 // first call on each device, with that device current, takes the address with
-// cudaGetSymbolAddress (return code checked) and keeps it; later calls reuse it.  Make that
-// first call before any stream capture that might include the entry point.
+// cudaGetSymbolAddress (return code checked) and keeps it together with the unique ID of the
+// device's current CUDA context; later calls reuse it while that context is still current.
+// A device reset (cudaDeviceReset) or a torn-down and recreated primary context loads the
+// module again at a new address: the next call sees a different context ID and looks the
+// address up again, so a stale address is never launched on.  Make the first call on a device
+// (and the first call after a reset) before any stream capture that might include the entry
+// point.
 //
 // Scratch limits: kNoAllocMaxBlocks partial-sum blocks of kSlots doubles plus one result row,
 // (1024 + 1) * 73 * 8 B = 598,600 B per device.  The grid is min(4 * SMs, ceil(ndet / 256)), so a
@@ -33,19 +38,52 @@ constexpr size_t kNoAllocDoubles = (size_t)(kNoAllocMaxBlocks + 1) * kSlots;
 
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
 
+// Unique ID of the calling thread's current CUDA context (0 when none), through driver entry
+// points fetched once from the runtime, so the library needs no link dependency on libcuda.
+typedef int (*CtxGetCurrentFn)(void** ctx);
+typedef int (*CtxGetIdFn)(void* ctx, unsigned long long* id);
+static unsigned long long current_context_id() {
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    if (!get_current || !get_id) {
+        cudaDriverEntryPointQueryResult q1 = cudaDriverEntryPointSymbolNotFound, q2 = q1;
+        void* f1 = nullptr;
+        void* f2 = nullptr;
+        FCIB_CUDA(cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f1, 12000, cudaEnableDefault, &q1));
+        FCIB_CUDA(cudaGetDriverEntryPointByVersion("cuCtxGetId", &f2, 12000, cudaEnableDefault, &q2));
+        FCIB_CHECK(q1 == cudaDriverEntryPointSuccess && q2 == cudaDriverEntryPointSuccess && f1 && f2,
+                   FCIB_ERR_CUDA, "fcib_spin2_device_noalloc: driver entry points cuCtxGetCurrent/cuCtxGetId missing");
+        get_current = reinterpret_cast<CtxGetCurrentFn>(f1);
+        get_id = reinterpret_cast<CtxGetIdFn>(f2);
+    }
+    void* ctx = nullptr;
+    FCIB_CHECK(get_current(&ctx) == 0, FCIB_ERR_CUDA, "fcib_spin2_device_noalloc: cuCtxGetCurrent failed");
+    if (!ctx) return 0;
+    unsigned long long id = 0;
+    FCIB_CHECK(get_id(ctx, &id) == 0, FCIB_ERR_CUDA, "fcib_spin2_device_noalloc: cuCtxGetId failed");
+    return id;
+}
+
 static double* noalloc_scratch(int device) {
     static std::mutex mu;
     static double* addr[kNoAllocMaxDevices] = {};
+    static unsigned long long ctx_id[kNoAllocMaxDevices] = {};
     FCIB_CHECK(device >= 0 && device < kNoAllocMaxDevices, FCIB_ERR_UNSUPPORTED,
                "fcib_spin2_device_noalloc: device ordinal above the scratch table size (64)");
     std::lock_guard<std::mutex> lock(mu);
-    if (!addr[device]) {
-        int cur = -1;
-        FCIB_CUDA(cudaGetDevice(&cur));
-        FCIB_CHECK(cur == device, FCIB_ERR_STATE, "fcib_spin2_device_noalloc: context device is not current");
+    int cur = -1;
+    FCIB_CUDA(cudaGetDevice(&cur));
+    FCIB_CHECK(cur == device, FCIB_ERR_STATE, "fcib_spin2_device_noalloc: context device is not current");
+    // binds the device's primary context to this thread (CUDA 12: created if needed; the device
+    // is already the current one, so nothing else changes) before its ID is read
+    FCIB_CUDA(cudaSetDevice(cur));
+    const unsigned long long id = current_context_id();
+    FCIB_CHECK(id != 0, FCIB_ERR_STATE, "fcib_spin2_device_noalloc: no current CUDA context");
+    if (!addr[device] || ctx_id[device] != id) {
         void* p = nullptr;
         FCIB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
         addr[device] = static_cast<double*>(p);
+        ctx_id[device] = id;
     }
     return addr[device];
 }

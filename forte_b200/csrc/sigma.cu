@@ -65,108 +65,169 @@ void prepare_integrals(Context& c) {
     }
     c.Ha.upload(c.oei_a, c.stream);
     c.Hb.upload(c.oei_b, c.stream);
+    // largest same-spin block element (the mixed same-spin fixed-point grid); the one-body blocks
+    // count only when they are not folded into the opposite-spin pair matrix
+    double mm = 0.0;
+    for (int p = 0; p < n; p++)
+        for (int q = 0; q < n; q++)
+            for (int r = 0; r < n; r++)
+                for (int t = 0; t < n; t++) {
+                    const size_t idx = (size_t)p * n3 + q * n2 + r * n + t;
+                    mm = std::max(mm, std::max(std::fabs(c.tei_aa[idx]), std::fabs(c.tei_bb[idx])));
+                }
+    if (!c.fold_h)
+        for (size_t i = 0; i < n2; i++) mm = std::max(mm, std::max(std::fabs(c.oei_a[i]), std::fabs(c.oei_b[i])));
+    c.same_mmax = mm * (1.0 + 1e-6) + 1e-300;
 }
 
 // ------------------------------------------------------------------------------------------
-// opposite-spin kernel (FP64)
+// opposite-spin kernel (FP64 on the tensor cores: mma.sync m8n8k4 f64)
 // ------------------------------------------------------------------------------------------
-constexpr int kAbTM = 64;  // beta rows per tile
-constexpr int kAbRows = 8; // tile rows per thread (broadcast operand)
-constexpr int kAbCols = 2; // pair columns per thread
+// One CTA per SM, persistent over target alpha rows Ia.  Per row: B[k][R] = sgn_k V[P_k][R]
+// (FP64) and the sigma row (initialised to E0 * C row) stay in shared memory; per tile of 64 beta
+// strings the connected C rows are gathered into A[k][Jb] (coalesced, one tile ahead in
+// registers), T = A^T B is formed with FP64 tensor-core MMAs (16 warps: 8 strings x 72 pairs each,
+// 9 independent 8x8 accumulators per warp, the fragments of the next k step loaded while the
+// current step's MMAs run), and T[Jb][R] is scattered over the beta single replacements F_R Jb with
+// FP64 shared-memory atomics.  A and B rows are stored with an XOR swizzle of bit 3 of the column by
+// the parity of k, so the fragment loads (4 rows x 8 consecutive columns) and the gather stores take
+// two wavefronts, the minimum for 256 bytes.
+constexpr int kDmTM = 64;              // beta rows per tile
+constexpr int kDmThreads = 512;        // 16 warps: row tile mt = warp & 7 (8 strings), pair half h = warp >> 3
+constexpr int kDmNT = 9;               // n8 pair tiles per warp: 2 halves x 9 x 8 = 144 >= npair (n <= 16)
+constexpr int kDmLdB = 2 * kDmNT * 8;  // B row stride in doubles (1152 bytes, a multiple of 128)
+constexpr int kDmMaxK = 72;            // connections per string (n <= 16)
+constexpr int kDmG = kDmMaxK * kDmTM / kDmThreads;  // gathered elements per thread per tile
 
 size_t ab_fp64_smem(int nbs, int s1a, int npp) {
-    return (size_t)((nbs + 1) & ~1) * 8 + (size_t)s1a * npp * 8 + (size_t)s1a * kAbTM * 8 + (size_t)s1a * 4 + 16;
+    (void)npp;
+    const int kpad = (s1a + 7) / 8 * 8;
+    return (size_t)((nbs + 1) & ~1) * 8 + (size_t)kpad * kDmLdB * 8 + (size_t)kpad * kDmTM * 8 + (size_t)kpad * 4 + 16;
 }
 
-__global__ void __launch_bounds__(576) k_ab_fp64(
-    const double* __restrict__ C, double* __restrict__ S, const uint32_t* __restrict__ connA,
-    int s1a, const int32_t* __restrict__ tgtB, int npp, const double* __restrict__ V, int nas,
-    int nbs, double e0, int* __restrict__ row_counter) {
+// D (8x8) += A (8x4, row) B (4x8, col); lane holds A[lane/4][lane%4], B[lane%4][lane/4] and
+// D[lane/4][2 (lane%4) + {0,1}]
+__device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+        : "+d"(d[0]), "+d"(d[1])
+        : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(kDmThreads, 1) k_ab_fp64(
+    const double* __restrict__ C, double* __restrict__ S, const uint32_t* __restrict__ connA, int s1a, int kpad,
+    const int32_t* __restrict__ tgtB, int npp, int npair, const double* __restrict__ V, int nas, int nbs, double e0,
+    int* __restrict__ row_counter) {
     extern __shared__ __align__(16) unsigned char smem[];
     double* srow = reinterpret_cast<double*>(smem);
-    double* Bm = srow + ((nbs + 1) & ~1);          // [s1a][npp], 16-byte aligned
-    double* At = Bm + (size_t)s1a * npp;           // [s1a][kAbTM]
-    uint32_t* cs = reinterpret_cast<uint32_t*>(At + (size_t)s1a * kAbTM);
+    double* Bs = srow + ((nbs + 1) & ~1);           // [kpad][kDmLdB]: (k, R) at k*kDmLdB + (R ^ ((k & 1) << 3))
+    double* As = Bs + (size_t)kpad * kDmLdB;        // [kpad][kDmTM]: (k, Jb) at k*kDmTM + (Jb ^ ((k & 1) << 3))
+    uint32_t* cs = reinterpret_cast<uint32_t*>(As + (size_t)kpad * kDmTM);
     __shared__ int s_row;
 
-    const int tid = threadIdx.x;
-    const int ncg = npp / kAbCols;
-    const int nmt = (kAbTM / kAbRows) * ncg;
-    const int cg = tid % ncg, rg = tid / ncg;
-    const bool active = tid < nmt;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int mt = warp & 7, h = warp >> 3;
+    const int nnt = (npair + 7) / 8;        // pair tiles holding at least one pair
+    const int nks = kpad / 4;
+    const int ng = kpad * kDmTM / kDmThreads;  // gathered elements per thread (kpad is a multiple of 8)
+    const int fr = lane >> 2, fk = lane & 3;   // fragment row / k of this lane
+    double g[kDmG];
 
     while (true) {
         if (tid == 0) s_row = atomicAdd(row_counter, 1);
         __syncthreads();
         const int Ia = s_row;
         if (Ia >= nas) break;
-        for (int k = tid; k < s1a; k += blockDim.x) cs[k] = connA[(size_t)Ia * s1a + k];
-        __syncthreads();
-        for (int idx = tid; idx < s1a * npp; idx += blockDim.x) {
-            int k = idx / npp, R = idx - k * npp;
-            uint32_t e = cs[k];
-            int P = (e >> 21) & 1023;
-            double v = V[(size_t)P * npp + R];
-            Bm[idx] = (e & kSignBit) ? -v : v;
-        }
+        for (int k = tid; k < kpad; k += kDmThreads) cs[k] = k < s1a ? connA[(size_t)Ia * s1a + k] : 0u;
         const double* Crow = C + (size_t)Ia * nbs;
-        for (int j = tid; j < nbs; j += blockDim.x) srow[j] = e0 * Crow[j];
+        for (int j = tid; j < nbs; j += kDmThreads) srow[j] = e0 * Crow[j];
         __syncthreads();
-
-        for (int jb0 = 0; jb0 < nbs; jb0 += kAbTM) {
-            for (int idx = tid; idx < s1a * kAbTM; idx += blockDim.x) {
-                int k = idx / kAbTM, t = idx - k * kAbTM;
-                int jb = jb0 + t;
-                uint32_t J = cs[k] & kConnIdxMask;
-                At[idx] = (jb < nbs) ? C[(size_t)J * nbs + jb] : 0.0;
+        for (int idx = tid; idx < kpad * kDmLdB; idx += kDmThreads) {
+            const int k = idx / kDmLdB, R = idx - k * kDmLdB;
+            double v = 0.0;
+            if (k < s1a && R < npair) {
+                const uint32_t e = cs[k];
+                v = V[(size_t)((e >> 21) & 1023) * npp + R];
+                if (e & kSignBit) v = -v;
+            }
+            Bs[(size_t)k * kDmLdB + (R ^ ((k & 1) << 3))] = v;
+        }
+        // element e = it * kDmThreads + tid of the [kpad][kDmTM] tile: k = e / kDmTM, Jb = e % kDmTM
+        auto gather = [&](int jb0) {
+#pragma unroll
+            for (int it = 0; it < kDmG; it++) {
+                if (it < ng) {
+                    const int e = it * kDmThreads + tid;
+                    const int k = e / kDmTM, jb = jb0 + (e % kDmTM);
+                    g[it] = (jb < nbs && k < s1a) ? C[(size_t)(cs[k] & kConnIdxMask) * nbs + jb] : 0.0;
+                }
+            }
+        };
+        gather(0);
+        for (int jb0 = 0; jb0 < nbs; jb0 += kDmTM) {
+            __syncthreads();  // the previous tile's fragment loads are done; B and cs are visible
+#pragma unroll
+            for (int it = 0; it < kDmG; it++) {
+                if (it < ng) {
+                    const int e = it * kDmThreads + tid;
+                    const int k = e / kDmTM, c = e % kDmTM;
+                    As[(size_t)k * kDmTM + (c ^ ((k & 1) << 3))] = g[it];
+                }
             }
             __syncthreads();
-            if (active) {
-                double acc[kAbRows][kAbCols];
+            if (jb0 + kDmTM < nbs) gather(jb0 + kDmTM);
+            double acc[kDmNT][2];
 #pragma unroll
-                for (int i = 0; i < kAbRows; i++)
+            for (int j = 0; j < kDmNT; j++) acc[j][0] = acc[j][1] = 0.0;
+            // fragments of k step ks: A[mt*8 + fr][4 ks + fk] and B[4 ks + fk][nt*8 + fr]
+            double fa[2], fb[2][kDmNT];
+            auto load_frag = [&](int ks, int buf) {
+                const int k = 4 * ks + fk;
+                const int sw = (k & 1) << 3;
+                fa[buf] = As[(size_t)k * kDmTM + ((mt * 8 + fr) ^ sw)];
+                const double* br = Bs + (size_t)k * kDmLdB;
 #pragma unroll
-                    for (int j = 0; j < kAbCols; j++) acc[i][j] = 0.0;
-                const double* ap = At + rg * kAbRows;
-                const double* bp = Bm + cg * kAbCols;
-#pragma unroll 2
-                for (int k = 0; k < s1a; k++) {
-                    double a[kAbRows];
-                    const double2* a2 = reinterpret_cast<const double2*>(ap + (size_t)k * kAbTM);
-#pragma unroll
-                    for (int i = 0; i < kAbRows / 2; i++) {
-                        double2 t2 = a2[i];
-                        a[2 * i] = t2.x;
-                        a[2 * i + 1] = t2.y;
-                    }
-                    double2 b2 = *reinterpret_cast<const double2*>(bp + (size_t)k * npp);
-#pragma unroll
-                    for (int i = 0; i < kAbRows; i++) {
-                        acc[i][0] = fma(a[i], b2.x, acc[i][0]);
-                        acc[i][1] = fma(a[i], b2.y, acc[i][1]);
-                    }
+                for (int j = 0; j < kDmNT; j++) {
+                    const int nt = h * kDmNT + j;
+                    fb[buf][j] = nt < nnt ? br[(nt * 8 + fr) ^ sw] : 0.0;
                 }
+            };
+            load_frag(0, 0);
+            for (int ks = 0; ks < nks; ks += 2) {
+                if (ks + 1 < nks) load_frag(ks + 1, 1);
 #pragma unroll
-                for (int i = 0; i < kAbRows; i++) {
-                    int jb = jb0 + rg * kAbRows + i;
-                    if (jb < nbs) {
-                        int2 tg = *reinterpret_cast<const int2*>(tgtB + (size_t)jb * npp + cg * kAbCols);
+                for (int j = 0; j < kDmNT; j++)
+                    if (h * kDmNT + j < nnt) dmma_8x8x4(acc[j], fa[0], fb[0][j]);
+                if (ks + 1 < nks) {
+                    if (ks + 2 < nks) load_frag(ks + 2, 0);
+#pragma unroll
+                    for (int j = 0; j < kDmNT; j++)
+                        if (h * kDmNT + j < nnt) dmma_8x8x4(acc[j], fa[1], fb[1][j]);
+                }
+            }
+            // scatter T[Jb][R] over the beta single replacements into the sigma row
+            const int jb = jb0 + mt * 8 + fr;
+            if (jb < nbs) {
+#pragma unroll
+                for (int j = 0; j < kDmNT; j++) {
+                    const int nt = h * kDmNT + j;
+                    if (nt < nnt) {
+                        const int R = nt * 8 + 2 * fk;
+                        const int2 tg = *reinterpret_cast<const int2*>(tgtB + (size_t)jb * npp + R);
                         if (tg.x != kNoTarget) {
-                            double v = acc[i][0];
+                            const double v = acc[j][0];
                             atomicAdd(&srow[tg.x & kConnIdxMask], (tg.x & (int)kSignBit) ? -v : v);
                         }
                         if (tg.y != kNoTarget) {
-                            double v = acc[i][1];
+                            const double v = acc[j][1];
                             atomicAdd(&srow[tg.y & kConnIdxMask], (tg.y & (int)kSignBit) ? -v : v);
                         }
                     }
                 }
             }
-            __syncthreads();
         }
-        double* Srow = S + (size_t)Ia * nbs;
-        for (int j = tid; j < nbs; j += blockDim.x) Srow[j] = srow[j];
         __syncthreads();
+        double* Srow = S + (size_t)Ia * nbs;
+        for (int j = tid; j < nbs; j += kDmThreads) Srow[j] = srow[j];
     }
 }
 
@@ -181,14 +242,31 @@ constexpr int kGrRows = 8;   // rows per thread
 // C and sigma a chunk touches stay L2-resident while every group of that chunk is processed.
 // The pair-pair block M stays in shared memory; W = M[lab_i][lab_j] is rebuilt per item from it.
 // T = double (FP64 path: FP64 in, FP64 atomics) or float (mixed path: an FP32 copy of C in, FP32
-// accumulation, float2 vector atomics into an FP32 sigma buffer that is added to FP64 sigma later).
+// accumulation, each result rounded to the sigma's fixed-point grid 2^-el and added with 64-bit
+// integer reductions into an int64 buffer, so the sum does not depend on the order of the groups).
 constexpr int kGrLoads = 16;  // X elements per thread per item (G*kGrTN/threads <= 16 by construction)
 
 template <typename T>
+struct GroupOut {
+    using type = double;
+};
+template <>
+struct GroupOut<float> {
+    using type = unsigned long long;
+};
+
+// one FP32 same-spin result -> its fixed-point integer on the grid 2^-el (two's complement in a u64)
+__device__ __forceinline__ unsigned long long fixed64(float v, float scale) {
+    return (unsigned long long)__float2ll_rn(v * scale);
+}
+
+template <typename T>
 __global__ void __launch_bounds__(1024) k_group(
-    const T* __restrict__ C, T* __restrict__ S, int ncols,
+    const T* __restrict__ C, typename GroupOut<T>::type* __restrict__ S, int ncols,
     const uint32_t* __restrict__ rows, const uint16_t* __restrict__ labs, int G, int Gp,
-    const double* __restrict__ M, int ldm, int ngroups, int nchunks, int* __restrict__ counter, int m_in_smem) {
+    const double* __restrict__ M, int ldm, int ngroups, int nchunks, int* __restrict__ counter, int m_in_smem,
+    const int* __restrict__ grid_el) {
+    const float scale = grid_el ? ldexpf(1.0f, *grid_el) : 1.0f;
     using T2 = typename std::conditional<std::is_same<T, double>::value, double2, float2>::type;
     extern __shared__ __align__(16) unsigned char smem[];
     T* Ms = reinterpret_cast<T*>(smem);       // [ldm][ldm] when m_in_smem (else M is read from L2)
@@ -281,14 +359,15 @@ __global__ void __launch_bounds__(1024) k_group(
                 if (ii < G) {
                     uint32_t e = rs[ii];
                     const size_t off = (size_t)(e & kConnIdxMask) * ncols + col;
-                    T* dst = S + off;
+                    auto* dst = S + off;
                     const T a0 = (e & kSignBit) ? -acc[i][0] : acc[i][0];
                     const T a1 = (e & kSignBit) ? -acc[i][1] : acc[i][1];
-                    if (!std::is_same<T, double>::value && col + 1 < ncols && (off & 1) == 0) {
-                        atomicAdd(reinterpret_cast<float2*>(dst), make_float2((float)a0, (float)a1));
-                    } else {
+                    if constexpr (std::is_same<T, double>::value) {
                         if (col < ncols) atomicAdd(dst, a0);
                         if (col + 1 < ncols) atomicAdd(dst + 1, a1);
+                    } else {
+                        if (col < ncols) atomicAdd(dst, fixed64(a0, scale));
+                        if (col + 1 < ncols) atomicAdd(dst + 1, fixed64(a1, scale));
                     }
                 }
             }
@@ -297,8 +376,9 @@ __global__ void __launch_bounds__(1024) k_group(
 }
 
 template <typename T>
-static void launch_group_t(Context& c, const T* C, T* S, int ncols, int ngroups, int G,
-                           const uint32_t* rows, const uint16_t* labs, const double* M, int ldm) {
+static void launch_group_t(Context& c, const T* C, typename GroupOut<T>::type* S, int ncols, int ngroups, int G,
+                           const uint32_t* rows, const uint16_t* labs, const double* M, int ldm,
+                           const int* grid_el) {
     if (ngroups == 0 || G == 0) return;
     int Gp = (G + kGrRows - 1) / kGrRows * kGrRows;
     size_t smem_tiles = (size_t)G * Gp * sizeof(T) + (size_t)G * kGrTN * sizeof(T) + (size_t)Gp * 4 + (size_t)Gp * 2 + 16;
@@ -316,17 +396,18 @@ static void launch_group_t(Context& c, const T* C, T* S, int ncols, int ngroups,
     int grid = std::min(ngroups * nchunks, per_sm * c.num_sms);
     ensure_counter(c);
     FCIB_CUDA(cudaMemsetAsync(c.counter.p + 2, 0, sizeof(int), c.stream));
-    k_group<T><<<grid, threads, smem, c.stream>>>(C, S, ncols, rows, labs, G, Gp, M, ldm, ngroups, nchunks, c.counter.p + 2, m_in_smem);
+    k_group<T><<<grid, threads, smem, c.stream>>>(C, S, ncols, rows, labs, G, Gp, M, ldm, ngroups, nchunks, c.counter.p + 2,
+                                                  m_in_smem, grid_el);
     FCIB_KCHECK();
 }
 
 static void launch_group(Context& c, const double* C, double* S, int ncols, int ngroups, int G,
                          const uint32_t* rows, const uint16_t* labs, const double* M, int ldm) {
-    launch_group_t<double>(c, C, S, ncols, ngroups, G, rows, labs, M, ldm);
+    launch_group_t<double>(c, C, S, ncols, ngroups, G, rows, labs, M, ldm, nullptr);
 }
-static void launch_group(Context& c, const float* C, float* S, int ncols, int ngroups, int G,
+static void launch_group(Context& c, const float* C, unsigned long long* S, int ncols, int ngroups, int G,
                          const uint32_t* rows, const uint16_t* labs, const double* M, int ldm) {
-    launch_group_t<float>(c, C, S, ncols, ngroups, G, rows, labs, M, ldm);
+    launch_group_t<float>(c, C, S, ncols, ngroups, G, rows, labs, M, ldm, c.counter.p + kSlotSameGrid);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -381,15 +462,18 @@ __global__ void k_transpose_f32(const float* __restrict__ in, float* __restrict_
     }
 }
 
-// S[r][c] += A[r][c] + Bt[c][r]: the alpha (row-major) and beta (transposed) FP32 same-spin parts
-__global__ void k_add_same_f32(double* __restrict__ S, const float* __restrict__ A, const float* __restrict__ Bt,
-                               int rows, int cols) {
-    __shared__ float tile[32][33];
+// S[r][c] += (A[r][c] + Bt[c][r]) 2^-el: the alpha (row-major) and beta (transposed) same-spin parts,
+// exact integers on the fixed-point grid 2^-el of this sigma (each part below 2^62 in magnitude)
+__global__ void k_add_same_fixed(double* __restrict__ S, const unsigned long long* __restrict__ A,
+                                 const unsigned long long* __restrict__ Bt, int rows, int cols,
+                                 const int* __restrict__ grid_el) {
+    __shared__ long long tile[32][33];
+    const double inv = ldexp(1.0, -*grid_el);
     int x = blockIdx.x * 32 + threadIdx.x;  // Bt column = S row
     int y0 = blockIdx.y * 32;               // Bt row = S column
     for (int j = threadIdx.y; j < 32; j += blockDim.y) {
         int y = y0 + j;
-        if (x < rows && y < cols) tile[j][threadIdx.x] = Bt[(size_t)y * rows + x];
+        if (x < rows && y < cols) tile[j][threadIdx.x] = (long long)Bt[(size_t)y * rows + x];
     }
     __syncthreads();
     int oc = y0 + threadIdx.x;
@@ -397,14 +481,28 @@ __global__ void k_add_same_f32(double* __restrict__ S, const float* __restrict__
         int orow = blockIdx.x * 32 + j;
         if (orow < rows && oc < cols) {
             const size_t o = (size_t)orow * cols + oc;
-            S[o] += (double)A[o] + (double)tile[threadIdx.x][j];
+            S[o] += (double)((long long)A[o] + tile[threadIdx.x][j]) * inv;
         }
     }
 }
 
-__global__ void k_to_f32(const double* __restrict__ in, float* __restrict__ out, size_t n) {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+// fixed-point grid of the mixed same-spin sums: every |element| <= kbound * max|C| * max|M|, so
+// 2^el times that stays below 2^62
+__global__ void k_same_grid(const unsigned int* __restrict__ cmax_bits, float kbound_mmax, int* __restrict__ el) {
+    const float b = fmaxf(1.01f * kbound_mmax * __uint_as_float(*cmax_bits), 1e-30f);
+    *el = min(100, (int)floorf(62.0f - log2f(b)));
+}
+
+// FP32 copy of the sigma input and bits of max|C| rounded up (when the tensor-core split did not run)
+__global__ void k_to_f32(const double* __restrict__ in, float* __restrict__ out, size_t n,
+                         unsigned int* __restrict__ cmax_bits) {
+    float mx = 0.f;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         out[i] = (float)in[i];
+        mx = fmaxf(mx, fabsf(out[i]));
+    }
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(cmax_bits, __float_as_uint(mx) + 1u);
 }
 
 __global__ void k_scale_copy(const double* __restrict__ in, double* __restrict__ out, double a, size_t n) {
@@ -438,11 +536,11 @@ void apply_mask(Context& c, double* v) {
 // ------------------------------------------------------------------------------------------
 // sigma orchestration
 // ------------------------------------------------------------------------------------------
-bool launch_group_tc(Context& c, const float* C, float* S, int ncols, int ngroups, int G, const uint32_t* rows,
-                     const uint16_t* labs, const double* M, int ldm);
+bool launch_group_tc(Context& c, const float* C, unsigned long long* S, int ncols, int ngroups, int G,
+                     const uint32_t* rows, const uint16_t* labs, const double* M, int ldm);
 
 // mixed same-spin two-body groups: tensor cores unless disabled or the groups are too large
-static void launch_group_same_f32(Context& c, const float* C, float* S, int ncols, int ngroups, int G,
+static void launch_group_same_f32(Context& c, const float* C, unsigned long long* S, int ncols, int ngroups, int G,
                                   const uint32_t* rows, const uint16_t* labs, const double* M, int ldm) {
     if (c.opt.same_spin_kernel == FCIB_SAME_TC && launch_group_tc(c, C, S, ncols, ngroups, G, rows, labs, M, ldm))
         return;
@@ -472,30 +570,43 @@ static void sigma_same_spin(Context& c, const double* C, double* S, bool fp32) {
     // mixed: FP32 copy of C (written by the tensor-core split when it ran), FP32 accumulation
     const bool any_a = a_g1 || c.A.ng2, any_b = b_g1 || c.B.ng2;
     if (!any_a && !any_b) return;
+    ensure_counter(c);
+    unsigned int* cmax_bits = reinterpret_cast<unsigned int*>(c.counter.p + kSlotCmax);
     if (!c.c32_ready) {
         c.c32.alloc(N);
-        k_to_f32<<<4 * c.num_sms, 256, 0, c.stream>>>(C, c.c32.p, N);
+        FCIB_CUDA(cudaMemsetAsync(cmax_bits, 0, sizeof(unsigned int), c.stream));
+        k_to_f32<<<4 * c.num_sms, 256, 0, c.stream>>>(C, c.c32.p, N, cmax_bits);
         FCIB_KCHECK();
     }
     c.c32_ready = false;
-    ensure_counter(c);
+    // fixed-point grid from max|C| (just computed on the device) and the host bound kbound * max|M|
+    {
+        auto kb = [&](const SpinTables& t, bool g1, int ne) {
+            double v = (double)t.ng2 > 0 ? (double)ne * (ne - 1) / 2 * ((t.g2 + 15) / 16 * 16) : 0.0;
+            if (g1 && t.ng1) v += (double)ne * ((t.g1 + 15) / 16 * 16);
+            return v;
+        };
+        const double kbound = std::max(kb(c.A, a_g1, c.na), kb(c.B, b_g1, c.nb));
+        k_same_grid<<<1, 1, 0, c.stream>>>(cmax_bits, (float)(kbound * c.same_mmax), c.counter.p + kSlotSameGrid);
+        FCIB_KCHECK();
+    }
     FCIB_CUDA(cudaMemsetAsync(c.counter.p + 5, 0, sizeof(int), c.stream));  // tensor-core group timeout flag
-    c.s32a.alloc(N);
-    c.st32.alloc(N);
-    FCIB_CUDA(cudaMemsetAsync(c.s32a.p, 0, N * sizeof(float), c.stream));
-    FCIB_CUDA(cudaMemsetAsync(c.st32.p, 0, N * sizeof(float), c.stream));
-    if (a_g1) launch_group(c, c.c32.p, c.s32a.p, nbs, c.A.ng1, c.A.g1, c.A.g1row.p, c.A.g1lab.p, c.Ha.p, c.n);
-    if (c.A.ng2) launch_group_same_f32(c, c.c32.p, c.s32a.p, nbs, c.A.ng2, c.A.g2, c.A.g2row.p, c.A.g2lab.p, c.M2a.p, np2);
+    c.s64a.alloc(N);
+    c.st64.alloc(N);
+    FCIB_CUDA(cudaMemsetAsync(c.s64a.p, 0, N * sizeof(unsigned long long), c.stream));
+    FCIB_CUDA(cudaMemsetAsync(c.st64.p, 0, N * sizeof(unsigned long long), c.stream));
+    if (a_g1) launch_group(c, c.c32.p, c.s64a.p, nbs, c.A.ng1, c.A.g1, c.A.g1row.p, c.A.g1lab.p, c.Ha.p, c.n);
+    if (c.A.ng2) launch_group_same_f32(c, c.c32.p, c.s64a.p, nbs, c.A.ng2, c.A.g2, c.A.g2row.p, c.A.g2lab.p, c.M2a.p, np2);
     if (any_b) {
         c.ct32.alloc(N);
         dim3 grid((nbs + 31) / 32, (nas + 31) / 32), block(32, 8);
         k_transpose_f32<<<grid, block, 0, c.stream>>>(c.c32.p, c.ct32.p, nas, nbs);
         FCIB_KCHECK();
-        if (b_g1) launch_group(c, c.ct32.p, c.st32.p, nas, c.B.ng1, c.B.g1, c.B.g1row.p, c.B.g1lab.p, c.Hb.p, c.n);
-        if (c.B.ng2) launch_group_same_f32(c, c.ct32.p, c.st32.p, nas, c.B.ng2, c.B.g2, c.B.g2row.p, c.B.g2lab.p, c.M2b.p, np2);
+        if (b_g1) launch_group(c, c.ct32.p, c.st64.p, nas, c.B.ng1, c.B.g1, c.B.g1row.p, c.B.g1lab.p, c.Hb.p, c.n);
+        if (c.B.ng2) launch_group_same_f32(c, c.ct32.p, c.st64.p, nas, c.B.ng2, c.B.g2, c.B.g2row.p, c.B.g2lab.p, c.M2b.p, np2);
     }
     dim3 grid2((nas + 31) / 32, (nbs + 31) / 32), block2(32, 8);
-    k_add_same_f32<<<grid2, block2, 0, c.stream>>>(S, c.s32a.p, c.st32.p, nas, nbs);
+    k_add_same_fixed<<<grid2, block2, 0, c.stream>>>(S, c.s64a.p, c.st64.p, nas, nbs, c.counter.p + kSlotSameGrid);
     FCIB_KCHECK();
 }
 
@@ -535,19 +646,19 @@ void sigma_fp64(Context& c, const double* C, double* S) {
     FCIB_CUDA(cudaEventRecord(ev.e[0], c.stream));
     if (c.fold_h) {
         const int s1a = c.A.s1, npp = c.A.npair_pad;
+        const int kpad = (s1a + 7) / 8 * 8;
+        FCIB_CHECK(kpad <= kDmMaxK && c.A.npair <= 2 * kDmNT * 8 && c.B.npair_pad == npp, FCIB_ERR_UNSUPPORTED,
+                   "too many orbitals for the FP64 opposite-spin kernel");
         size_t smem = ab_fp64_smem(nbs, s1a, npp);
         FCIB_CHECK(smem + 1024 <= (size_t)c.smem_optin, FCIB_ERR_UNSUPPORTED,
                    "opposite-spin row block exceeds shared memory (beta string count too large)");
         FCIB_CUDA(cudaFuncSetAttribute(k_ab_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        int threads = (kAbTM / kAbRows) * (npp / kAbCols);
-        threads = (threads + 31) / 32 * 32;
-        FCIB_CHECK(threads <= 576, FCIB_ERR_UNSUPPORTED, "too many orbitals for the FP64 opposite-spin kernel");
         int per_sm = std::max(1, (int)(c.smem_per_sm / (smem + 1024)));
-        per_sm = std::min(per_sm, 2048 / threads);
+        per_sm = std::min(per_sm, 2048 / kDmThreads);
         int grid = std::min(nas, per_sm * c.num_sms);
         FCIB_CUDA(cudaMemsetAsync(c.counter.p, 0, sizeof(int), c.stream));
-        k_ab_fp64<<<grid, threads, smem, c.stream>>>(C, S, c.A.conn.p, s1a, c.B.tgt.p, npp, c.V.p,
-                                                     nas, nbs, c.scalar, c.counter.p);
+        k_ab_fp64<<<grid, kDmThreads, smem, c.stream>>>(C, S, c.A.conn.p, s1a, kpad, c.B.tgt.p, npp, c.A.npair, c.V.p,
+                                                        nas, nbs, c.scalar, c.counter.p);
         FCIB_KCHECK();
     } else {
         k_scale_copy<<<4 * c.num_sms, 256, 0, c.stream>>>(C, S, c.scalar, N);

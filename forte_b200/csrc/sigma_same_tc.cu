@@ -14,9 +14,10 @@
 //   Xlo Whi + Xhi Wlo + Xhi Whi accumulate in FP32 in TMEM;
 // * two accumulators are double buffered, so the MMAs of tile t overlap the epilogue of tile t-1,
 //   and the gather of tile t+1 is in flight during both;
-// * the epilogue reads the accumulator with tcgen05.ld and adds each element to the FP32 sigma
-//   buffer with a global reduction (a warp covers 32 consecutive columns of one row); each sigma
-//   element receives one addition per group that holds its row, C(k,2) in all.
+// * the epilogue reads the accumulator with tcgen05.ld, rounds each element to the sigma's
+//   fixed-point grid 2^-el and adds it to an int64 sigma buffer with a 64-bit integer reduction
+//   (a warp covers 32 consecutive columns of one row); each sigma element receives one addition
+//   per group that holds its row, C(k,2) in all, and the integer sum does not depend on their order.
 // Groups of more than 64 strings (few electrons in many orbitals) keep the CUDA-core kernel.
 //
 // Every mbarrier wait is bounded; on timeout the kernel records an error code, waits (bounded)
@@ -75,9 +76,11 @@ __device__ __forceinline__ void reg_after4(uint32_t (&r)[4]) {
 
 template <int Q>
 __global__ void __launch_bounds__(kGtThreads, 2)
-    k_group_tc(const float* __restrict__ C, float* __restrict__ S, int ncols, const uint32_t* __restrict__ rows,
-               const uint16_t* __restrict__ labs, int G, const double* __restrict__ M, int ldm, int ngroups,
-               int* __restrict__ counter, int* __restrict__ err) {
+    k_group_tc(const float* __restrict__ C, unsigned long long* __restrict__ S, int ncols,
+               const uint32_t* __restrict__ rows, const uint16_t* __restrict__ labs, int G,
+               const double* __restrict__ M, int ldm, int ngroups, int* __restrict__ counter,
+               int* __restrict__ err, const int* __restrict__ grid_el) {
+    const float scale = ldexpf(1.0f, *grid_el);  // fixed-point grid 2^-el of this sigma
     extern __shared__ __align__(128) unsigned char smem[];
     const GtLayout L = gt_layout(G);
     unsigned char* Bhi = smem + L.off_bhi;
@@ -233,7 +236,8 @@ __global__ void __launch_bounds__(kGtThreads, 2)
 #pragma unroll
                         for (int u = 0; u < 4; u++)
                             if (off[i][u] != kGtNoRow)
-                                atomicAdd(S + (size_t)(off[i][u] + (uint32_t)col), __uint_as_float(rv[i][u]));
+                                atomicAdd(S + (size_t)(off[i][u] + (uint32_t)col),
+                                          fixed64(__uint_as_float(rv[i][u]), scale));
                 }
                 tc_fence_before();
             }
@@ -260,8 +264,8 @@ __global__ void __launch_bounds__(kGtThreads, 2)
 // 32-bit element offsets; the caller then uses k_group<float>.  The group counter and the timeout
 // flag live in counter slots 4 and 5; the flag is cleared by the caller once per sigma and read
 // back by tc_check_error.
-bool launch_group_tc(Context& c, const float* C, float* S, int ncols, int ngroups, int G, const uint32_t* rows,
-                     const uint16_t* labs, const double* M, int ldm) {
+bool launch_group_tc(Context& c, const float* C, unsigned long long* S, int ncols, int ngroups, int G,
+                     const uint32_t* rows, const uint16_t* labs, const double* M, int ldm) {
     if (G < 1 || G > kGtMaxG || (uint64_t)c.nas * (uint64_t)c.nbs >= (1ull << 32) - kGtM) return false;
     if (ngroups == 0) return true;
     const GtLayout L = gt_layout(G);
@@ -274,7 +278,7 @@ bool launch_group_tc(Context& c, const float* C, float* S, int ncols, int ngroup
     FCIB_CUDA(cudaMemsetAsync(c.counter.p + 4, 0, sizeof(int), c.stream));
     const int grid = std::min(ngroups, 2 * c.num_sms);
     kern<<<grid, kGtThreads, smem, c.stream>>>(C, S, ncols, rows, labs, G, M, ldm, ngroups, c.counter.p + 4,
-                                               c.counter.p + 5);
+                                               c.counter.p + 5, c.counter.p + kSlotSameGrid);
     FCIB_KCHECK();
     return true;
 }

@@ -108,10 +108,22 @@ __device__ __forceinline__ void reg_after(uint32_t (&r)[8]) {
                  : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]));
 }
 
+// ------------------------------------------------------------------------------------------
+// k_ab_tc layout.  Dynamic shared memory of the one CTA per SM:
+//   [0, 4 nbs)                   acc_hi: signed high words of the sigma row's fixed-point sums
+//   [kAccLoOff, kAccLoOff+4 nbs) acc_lo: low words, at a fixed distance from acc_hi so that one
+//                                address register serves both reductions (immediate offset)
+//   B hi, B lo                   Npad x Kpad TF32 planes, K-major core matrices, no swizzle
+//   cs[Kpad], koff[Kpad]         the row's connections and the byte offsets of their plane rows
+//   barriers, TMEM address
+// ------------------------------------------------------------------------------------------
+constexpr uint32_t kAccLoOff = 65536;
+constexpr int kMaxBetaStrings = 16383;  // Ib * 4 and a sign bit fit the 16-bit target entries
+
 struct TcLayout {
     int kpad, npad;          // K (connections) and N (pairs) padded to 8 / 16
     uint32_t b_bytes;        // one B plane
-    uint32_t off_bhi, off_blo, off_acc, off_conn, off_bar, total;
+    uint32_t off_bhi, off_blo, off_cs, off_koff, off_bar, total;
 };
 
 __host__ __device__ inline TcLayout tc_layout(int s1a, int npair, int nbs, bool three) {
@@ -119,11 +131,11 @@ __host__ __device__ inline TcLayout tc_layout(int s1a, int npair, int nbs, bool 
     L.kpad = (s1a + 7) / 8 * 8;
     L.npad = (npair + 15) / 16 * 16;
     L.b_bytes = (uint32_t)L.npad * L.kpad * 4;
-    uint32_t o = 0;
+    uint32_t o = kAccLoOff + ((uint32_t)nbs * 4 + 127) / 128 * 128;
     L.off_bhi = o; o += L.b_bytes;
     L.off_blo = o; o += three ? L.b_bytes : 0;
-    L.off_acc = o; o += ((uint32_t)nbs * 8 + 127) / 128 * 128;  // int32 high words, then low words
-    L.off_conn = o; o += ((uint32_t)L.kpad * 4 + 127) / 128 * 128;
+    L.off_cs = o; o += ((uint32_t)L.kpad * 4 + 127) / 128 * 128;
+    L.off_koff = o; o += ((uint32_t)L.kpad * 4 + 127) / 128 * 128;
     L.off_bar = o; o += 128;
     L.total = o;
     return L;
@@ -137,6 +149,15 @@ __device__ __forceinline__ uint32_t kmaj_off(int row, int k, int rows) {
 // no "memory" clobber: the accumulator is read only after a __syncthreads, which orders it
 __device__ __forceinline__ void red_add_u32(uint32_t saddr, uint32_t v) {
     asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(saddr), "r"(v));
+}
+// both words of one fixed-point contribution (the low word kAccLoOff bytes above the high word),
+// predicated on the 16-bit target entry g holding a target (g != 0xFFFF): no branch, so the slots of
+// a chunk form straight-line code the compiler can interleave
+__device__ __forceinline__ void red_pair_if(uint32_t saddr, uint32_t hi, uint32_t lo, uint32_t g) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.u32 p, %3, 65535;\n"
+        " @p red.shared.add.u32 [%0], %1;\n @p red.shared.add.u32 [%0+65536], %2;\n}\n" ::"r"(saddr),
+        "r"(hi), "r"(lo), "r"(g));
 }
 
 __device__ __forceinline__ void mma_tf32_ta(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc, uint32_t idesc,
@@ -161,26 +182,42 @@ constexpr int kErrTimeoutMma = 1;
 
 // TMEM columns: accumulators at 0 and 256 (npad <= 144), A hi at 160, A lo at 416 (kpad <= 72)
 constexpr uint32_t kColAccStride = 256, kColAhi = 160, kColAlo = 416;
-constexpr int kTcWarps = kTcThreads / 32;
-constexpr int kTcGat = 3;    // 8-column A chunks per warp per tile: 9 chunks over 4 column groups
-constexpr int kTcEpiC = 5;   // 8-column accumulator chunks per warp: 18 chunks over 4 column groups
+// Column groups cg = warp / 4.  Gather: A chunks c8 = cg and cg + 4, then chunk 8 + (3 - cg).
+// Epilogue: off-diagonal accumulator chunks c8 = (3 - cg) + 4 i; the diagonal-pair chunks (the
+// last ones) go to cg 0, which has one off-diagonal chunk fewer at n = 16 (15 chunks).
+constexpr int kTcGat = 3;    // 8-column A chunks per warp per tile
+constexpr int kTcEpiC = 4;   // off-diagonal accumulator chunks per warp
+constexpr int kTcMmaThread = 5 * 32;  // issues the MMAs (warp 5: two gather chunks, four epilogue chunks)
 constexpr int kFixLoBits = 22;
 constexpr float kMagic = 12582912.0f;       // 1.5 * 2^23: x + kMagic rounds |x| < 2^22 to an integer
 constexpr int kMagicBits = 0x4B400000;      // bit pattern of kMagic
 
+// One CTA per SM, persistent over target alpha rows Ia (dynamic counter).  Per row: the s1a
+// connections (J_k, P_k, sign_k) and B[R][k] = sign_k V[P_k][R] 2^el (TF32 hi/lo, the fixed-point
+// grid folded in exactly) are staged in shared memory; per tile of 128 beta strings Jb:
+//   gather   A[Jb][k] = plane[J_k][Jb] (interleaved TF32 hi/lo pairs; one coalesced 8-byte load per
+//            element, address = tile base + koff[k]) into registers, one tile ahead;
+//   store    registers -> A in TMEM (tcgen05.st), after the previous tile's MMAs released it;
+//   MMA      T = A B, 3xTF32, FP32 accumulator in TMEM (two accumulators, double buffered);
+//   scatter  the previous tile's T[Jb][R] to sigma[F_R Jb] in exact 2-word fixed point.
+// Plane rows are padded to whole tiles (zeros) and the target table to whole tiles (no target), so
+// neither the gather nor the scatter checks bounds.  Per tile: one mbarrier wait and one block
+// barrier.
 template <bool THREE>
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_ab_tc(const float2* __restrict__ Phl, int ldp, const double* __restrict__ C,
             double* __restrict__ S, const uint32_t* __restrict__ connA, int s1a, const uint16_t* __restrict__ tgtR,
-            int npair, const double* __restrict__ V, int ldv, float vmax, const unsigned int* __restrict__ cmax_bits,
-            int nas, int nbs, int s1b, double e0, int* __restrict__ row_counter, int* __restrict__ err) {
-    extern __shared__ __align__(128) unsigned char smem[];
+            int npair, const int* __restrict__ perm, int noff8, int n, const uint32_t* __restrict__ bstr, int kb,
+            const double* __restrict__ V, int ldv, float vmax, const unsigned int* __restrict__ cmax_bits,
+            int nas, int nbs, int ncontrib, double e0, int* __restrict__ row_counter, int* __restrict__ err) {
+    extern __shared__ __align__(1024) unsigned char smem[];
     const TcLayout L = tc_layout(s1a, npair, nbs, THREE);
     unsigned char* Bhi = smem + L.off_bhi;
     unsigned char* Blo = smem + L.off_blo;
-    int* acc_hi = reinterpret_cast<int*>(smem + L.off_acc);
-    unsigned int* acc_lo = reinterpret_cast<unsigned int*>(acc_hi + nbs);
-    uint32_t* cs = reinterpret_cast<uint32_t*>(smem + L.off_conn);
+    int* acc_hi = reinterpret_cast<int*>(smem);
+    unsigned int* acc_lo = reinterpret_cast<unsigned int*>(smem + kAccLoOff);
+    uint32_t* cs = reinterpret_cast<uint32_t*>(smem + L.off_cs);
+    uint32_t* koff = reinterpret_cast<uint32_t*>(smem + L.off_koff);
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L.off_bar);  // [0],[1]: MMA done per accumulator
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + L.off_bar + 64);
     __shared__ int s_row;
@@ -209,39 +246,76 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const uint32_t tmem_base = *tmem_slot;
     const uint32_t tlane = (uint32_t)(32 * q) << 16;
 
-    // fixed-point grid: |y| <= kpad * max|C| * max|V| < 2^44 * 2^-el
+    // fixed-point grid: every contribution, the sum of a string's kb diagonal-pair products included,
+    // is at most kb * kpad * max|C| * max|V| < 2^44 * 2^-el
     const float cmax = __uint_as_float(*cmax_bits);
-    const float ybound = fmaxf(1.01f * (float)kpad * cmax * vmax, 1e-30f);
+    const float ybound = fmaxf(1.01f * (float)max(kb, 1) * (float)kpad * cmax * vmax, 1e-30f);
     const int el = min(60, (int)floorf(44.0f - log2f(ybound)));
     const double inv_grid = ldexp(1.0, -el);
-    const float gridf = ldexpf(1.0f, el);  // exact power of two (el <= 60 is within float range)
-    const unsigned magic_total = (unsigned)s1b * (unsigned)kMagicBits;  // removed once per element (mod 2^32)
+    const double grid = ldexp(1.0, el);
+    // every element receives exactly ncontrib contributions: kb (n - kb) off-diagonal ones and the
+    // diagonal sum of its own string; ncontrib * kMagicBits is removed once per element (mod 2^32)
+    const unsigned magic_total = (unsigned)ncontrib * (unsigned)kMagicBits;
 
     // instruction descriptor: D f32, A/B tf32, both K-major, N = npad, M = 128
     const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(npad >> 3) << 17) | ((uint32_t)(kTcM >> 4) << 24);
     const uint32_t lbo_b = (uint32_t)(npad / 8) * 128;
     const uint32_t sb_hi = smem_u32(Bhi), sb_lo = smem_u32(Blo);
-    const uint32_t acc_hi_s = smem_u32(acc_hi), acc_lo_s = smem_u32(acc_lo);
+    const uint32_t acc_s = smem_u32(acc_hi);
 
     uint32_t mma_count[2] = {0u, 0u};  // commits issued per accumulator (parity tracking)
     const int ntiles = (nbs + kTcM - 1) / kTcM;
-    const int nk8 = kpad / 8, nn8 = npad / 8;
+    const int nk8 = kpad / 8;
+    const int nn8 = noff8 / 8;        // accumulator chunks of off-diagonal pairs
+    const int ndc = (n + 7) / 8;      // accumulator chunks of the diagonal pairs (r,r), after them
+    const unsigned char* pbase = reinterpret_cast<const unsigned char*>(Phl);
+
+    float gh[kTcGat][8], gl[kTcGat][8];
+    // A-tile gather: the thread owning tile row m = 32q + lane loads A[m][k] = plane[J_k][jb0 + m] for
+    // the 8-column chunks c8 = cg + 4j (coalesced across lanes)
+    auto gather = [&](int tt) {
+        const unsigned char* pj = pbase + (size_t)(tt * kTcM + 32 * q + lane) * sizeof(float2);
+#pragma unroll
+        for (int j = 0; j < kTcGat; j++) {
+            const int c8 = j < 2 ? cg + 4 * j : 8 + (3 - cg);
+            if (c8 < nk8) {
+                const uint4 o0 = *reinterpret_cast<const uint4*>(koff + 8 * c8);
+                const uint4 o1 = *reinterpret_cast<const uint4*>(koff + 8 * c8 + 4);
+                const uint32_t o[8] = {o0.x, o0.y, o0.z, o0.w, o1.x, o1.y, o1.z, o1.w};
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    const float2 x = __ldg(reinterpret_cast<const float2*>(pj + o[u]));
+                    gh[j][u] = x.x;
+                    gl[j][u] = x.y;
+                }
+            }
+        }
+    };
 
     while (true) {
         if (tid == 0) s_row = atomicAdd(row_counter, 1);
         __syncthreads();
         const int Ia = s_row;
         if (Ia >= nas || s_abort) break;
-        for (int k = tid; k < kpad; k += blockDim.x) cs[k] = k < s1a ? connA[(size_t)Ia * s1a + k] : 0u;
-        for (int j = tid; j < 2 * nbs; j += blockDim.x) acc_hi[j] = 0;
+        for (int k = tid; k < kpad; k += blockDim.x) {
+            const uint32_t e = k < s1a ? connA[(size_t)Ia * s1a + k] : 0u;
+            cs[k] = e;
+            koff[k] = (e & kConnIdxMask) * (uint32_t)ldp * (uint32_t)sizeof(float2);
+        }
+        for (int j = tid; j < nbs; j += blockDim.x) {
+            acc_hi[j] = 0;
+            acc_lo[j] = 0u;
+        }
         __syncthreads();
-        // B[R][k] = sgn_k V[P_k][R], split into tf32 hi/lo
+        // B[c][k] = sgn_k V[P_k][perm[c]] 2^el, split into tf32 hi/lo; column c holds pair perm[c]
+        // (off-diagonal pairs first, then the diagonal ones; -1 = padding)
         for (int idx = tid; idx < npad * kpad; idx += blockDim.x) {
             int R = idx / kpad, k = idx - R * kpad;
             float hi = 0.f, lo = 0.f;
-            if (k < s1a && R < npair) {
+            const int pr = perm[R];
+            if (k < s1a && pr >= 0) {
                 uint32_t e = cs[k];
-                double v = V[(size_t)((e >> 21) & 1023) * ldv + R];
+                double v = V[(size_t)((e >> 21) & 1023) * ldv + pr] * grid;
                 if (e & kSignBit) v = -v;
                 hi = __uint_as_float(to_tf32((float)v));
                 lo = __uint_as_float(to_tf32((float)(v - (double)hi)));
@@ -251,47 +325,33 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             if (THREE) *reinterpret_cast<float*>(Blo + off) = lo;
         }
         fence_proxy_async();  // B (generic-proxy stores) becomes visible to the tensor core's reads
-        // A-tile gather: the thread owning tile row m = 32q + lane loads A[m][k] = plane[J_k][jb0 + m]
-        // for the 8-column chunks c8 = cg + 4j (coalesced across lanes); one tile ahead in registers
-        float gh[kTcGat][8], gl[kTcGat][8];
-        auto prefetch = [&](int tt) {
-            const int jb = tt * kTcM + 32 * q + lane;
-#pragma unroll
-            for (int j = 0; j < kTcGat; j++) {
-                const int c8 = cg + 4 * j;
-#pragma unroll
-                for (int u = 0; u < 8; u++) {
-                    const int k = 8 * c8 + u;
-                    float h = 0.f, l = 0.f;
-                    if (c8 < nk8 && k < s1a && jb < nbs) {
-                        const size_t o = (size_t)(cs[k] & kConnIdxMask) * ldp + jb;
-                        const float2 x = __ldg(Phl + o);  // interleaved (hi, lo) TF32 pair
-                        h = x.x;
-                        if (THREE) l = x.y;
-                    }
-                    gh[j][u] = h;
-                    gl[j][u] = l;
-                }
-            }
-        };
-        prefetch(0);
+        gather(0);
         for (int t = 0; t <= ntiles; t++) {
             const int cur = t & 1, prv = cur ^ 1;
-            // (a) the TMEM A buffer is free once the previous tile's MMAs completed (one waiter)
-            if (t >= 1 && tid == 0) {
-                if (!mbar_wait_bounded(&bars[prv], (mma_count[prv] - 1) & 1)) {
-                    atomicCAS(err, 0, kErrTimeoutMma);
-                    s_abort = 1;
-                }
+            // targets of the epilogue tile t-1, loaded early (consumed in (d)); rows past nbs and
+            // pairs past npair hold no target
+            const int jb_epi = (t - 1) * kTcM + 32 * q + lane;
+            auto load_tg = [&](int i) {
+                const int c8 = (3 - cg) + 4 * i;
+                return (t >= 1 && c8 < nn8)
+                           ? __ldg(reinterpret_cast<const uint4*>(tgtR + ((size_t)c8 * ntiles * kTcM + jb_epi) * 8))
+                           : make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
+            };
+            uint4 tg[3];
+#pragma unroll
+            for (int i = 0; i < 3; i++) tg[i] = load_tg(i);
+            const uint32_t occ_epi = (cg == 0 && t >= 1 && jb_epi < nbs) ? __ldg(bstr + jb_epi) : 0u;
+            // (a) the TMEM A buffer and accumulator prv are ready once tile t-1's MMAs completed
+            if (t >= 1 && !mbar_wait_bounded(&bars[prv], (mma_count[prv] - 1) & 1)) {
+                atomicCAS(err, 0, kErrTimeoutMma);
+                s_abort = 1;
             }
-            __syncthreads();
-            if (s_abort) break;
             tc_fence_after();
             // (b) registers -> A in tensor memory
             if (t < ntiles) {
 #pragma unroll
                 for (int j = 0; j < kTcGat; j++) {
-                    const int c8 = cg + 4 * j;
+                    const int c8 = j < 2 ? cg + 4 * j : 8 + (3 - cg);
                     if (c8 < nk8) {
                         tmem_st8(tmem_base + tlane + kColAhi + 8 * c8, gh[j]);
                         if (THREE) tmem_st8(tmem_base + tlane + kColAlo + 8 * c8, gl[j]);
@@ -299,23 +359,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 }
                 asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
             }
-            // targets of the epilogue tile t-1, loaded early (consumed in (d))
-            uint4 tg[kTcEpiC];
-            {
-                const int jb = (t - 1) * kTcM + 32 * q + lane;
-#pragma unroll
-                for (int i = 0; i < kTcEpiC; i++) {
-                    const int c8 = cg + 4 * i;
-                    tg[i] = (t >= 1 && c8 < nn8 && jb < nbs)
-                                ? __ldg(reinterpret_cast<const uint4*>(tgtR + ((size_t)c8 * nbs + jb) * 8))
-                                : make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
-                }
-            }
             tc_fence_before();
             __syncthreads();
+            if (s_abort) break;
             tc_fence_after();
             // (c) one thread issues the tile's MMAs into accumulator `cur`
-            if (t < ntiles && tid == 0) {
+            if (t < ntiles && tid == kTcMmaThread) {
                 const uint32_t dt = tmem_base + (uint32_t)cur * kColAccStride;
                 uint32_t acc = 0;
                 for (int ks = 0; ks < nk8; ks++) {
@@ -335,46 +384,68 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             }
             if (t < ntiles) mma_count[cur]++;
             // (b') next tile's loads overlap the MMAs above and the epilogue below
-            if (t + 1 < ntiles) prefetch(t + 1);
-            // (d) epilogue of tile t-1: exact fixed-point scatter over beta replacements
+            if (t + 1 < ntiles) gather(t + 1);
+            // (d) epilogue of tile t-1: exact fixed-point scatter over beta replacements, in two
+            // batches of accumulator chunks (fewer live registers)
             if (t >= 1) {
                 const uint32_t tbase = tmem_base + (uint32_t)prv * kColAccStride + tlane;
-                // all of this warp's accumulator chunks are loaded before a single wait
-                uint32_t rv[kTcEpiC][8];
+                // y 2^el (grid folded into B) exactly in FP32 (|.| < 2^44), split as hi 2^22 + lo with
+                // hi = round(y 2^(el-22)) and lo = round(y 2^el - hi 2^22), |lo| <= 2^21, both rounded by
+                // adding 1.5 * 2^23; the raw bit patterns (integer + kMagicBits) are accumulated and
+                // ncontrib * kMagicBits is removed per element when the row is written
+                auto add_fixed = [&](float ys, uint32_t a, uint32_t g) {
+                    const float t1 = fmaf(ys, 2.38418579e-7f, kMagic);
+                    const float lf = fmaf(t1 - kMagic, -4194304.0f, ys);
+                    red_pair_if(a, __float_as_uint(t1), __float_as_uint(lf + kMagic), g);
+                };
+                auto scatter = [&](const uint32_t (&rv)[8], const uint4& tw) {
+                    const uint32_t w[4] = {tw.x, tw.y, tw.z, tw.w};
 #pragma unroll
-                for (int i = 0; i < kTcEpiC; i++) {
-                    const int c8 = cg + 4 * i;
-                    if (c8 < nn8) tmem_ld8_async(tbase + (uint32_t)(c8 * 8), rv[i]);
-                }
-                tmem_wait_ld8(rv[0]);
-#pragma unroll
-                for (int i = 1; i < kTcEpiC; i++) reg_after(rv[i]);
-#pragma unroll
-                for (int i = 0; i < kTcEpiC; i++) {
-                    const int c8 = cg + 4 * i;
-                    if (c8 < nn8) {
-                        const uint32_t w[4] = {tg[i].x, tg[i].y, tg[i].z, tg[i].w};
-#pragma unroll
-                        for (int u = 0; u < 8; u++) {
-                            const uint32_t g = (w[u >> 1] >> (16 * (u & 1))) & 0xFFFFu;
-                            if (g != 0xFFFFu) {
-                                // y 2^el exactly in FP32 (|.| < 2^44), split as hi 2^22 + lo with
-                                // hi = round(y 2^(el-22)) and lo = round(y 2^el - hi 2^22), |lo| <= 2^21,
-                                // both rounded by adding 1.5 * 2^23; the raw bit patterns (integer +
-                                // kMagicBits) are accumulated and s1b * kMagicBits is removed per element
-                                // when the row is written (every element gets exactly s1b contributions)
-                                const float ys = __uint_as_float(rv[i][u]) * ((g & 0x8000u) ? -gridf : gridf);
-                                const float t1 = fmaf(ys, 2.38418579e-7f, kMagic);
-                                const float lf = fmaf(kMagic - t1, 4194304.0f, ys);
-                                const uint32_t idx = (g & 0x7FFFu) << 2;
-                                red_add_u32(acc_hi_s + idx, __float_as_uint(t1));
-                                red_add_u32(acc_lo_s + idx, __float_as_uint(lf + kMagic));
-                            }
-                        }
+                    for (int u = 0; u < 8; u++) {
+                        // entry = Ib * 4 | sign (bit 0); 0xFFFF = no target
+                        const uint32_t g = (u & 1) ? (w[u >> 1] >> 16) : (w[u >> 1] & 0xFFFFu);
+                        add_fixed(__uint_as_float(rv[u] ^ (g << 31)), acc_s + (g & 0xFFFCu), g);
                     }
+                };
+                uint4 tg2 = load_tg(3);
+                {
+                    uint32_t rv[3][8];
+#pragma unroll
+                    for (int i = 0; i < 3; i++) {
+                        const int c8 = (3 - cg) + 4 * i;
+                        if (c8 < nn8) tmem_ld8_async(tbase + (uint32_t)(c8 * 8), rv[i]);
+                    }
+                    tmem_wait_ld8(rv[0]);
+                    reg_after(rv[1]);
+                    reg_after(rv[2]);
+#pragma unroll
+                    for (int i = 0; i < 3; i++)
+                        if ((3 - cg) + 4 * i < nn8) scatter(rv[i], tg[i]);
                 }
-                tc_fence_before();
+                if ((3 - cg) + 12 < nn8) {
+                    uint32_t rv[8];
+                    tmem_ld8_async(tbase + (uint32_t)(((3 - cg) + 12) * 8), rv);
+                    tmem_wait_ld8(rv);
+                    scatter(rv, tg2);
+                }
+                if (cg == 0) {
+                    // diagonal pairs (r,r): F_rr Jb = Jb for every occupied r, so the string's own
+                    // element receives sum_{r occupied} T[Jb][(r,r)], added in FP32 in a fixed order
+                    // and reduced as one contribution
+                    uint32_t rd[2][8];
+                    tmem_ld8_async(tbase + (uint32_t)(nn8 * 8), rd[0]);
+                    if (ndc > 1) tmem_ld8_async(tbase + (uint32_t)((nn8 + 1) * 8), rd[1]);
+                    tmem_wait_ld8(rd[0]);
+                    reg_after(rd[1]);
+                    const uint32_t occ = occ_epi;
+                    float d = 0.f;
+#pragma unroll
+                    for (int r = 0; r < 16; r++)
+                        if (r < n && ((occ >> r) & 1u)) d += __uint_as_float(rd[r >> 3][r & 7]);
+                    add_fixed(d, acc_s + (uint32_t)jb_epi * 4u, jb_epi < nbs ? 0u : 0xFFFFu);
+                }
             }
+            tc_fence_before();
         }
         if (s_abort) break;
         __syncthreads();
@@ -386,7 +457,6 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             const long long tot = ((long long)hi << kFixLoBits) + (long long)lo;
             Srow[j] = e0 * Crow[j] + (double)tot * inv_grid;
         }
-        __syncthreads();
     }
     // drain: wait (bounded) for any MMA still in flight before releasing tensor memory
     __syncthreads();
@@ -401,21 +471,24 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(kTmemCols) : "memory");
 }
 
-// tgtR[R/8][Jb][R%8] = 16-bit scatter target of F_R Jb: index | sign << 15; no connection -> 0xFFFF.
-// Chunk-major: the 8 targets of one 8-pair chunk of consecutive Jb sit in consecutive 16-byte words,
-// so a warp (32 consecutive Jb) reads one chunk with fully coalesced loads.
-__global__ void k_tgt_rows16(const int32_t* __restrict__ tgt, uint16_t* __restrict__ out, int nstr, int npp_in,
-                             int npad_out) {
-    size_t total = (size_t)npad_out * nstr;
+// tgtR[c/8][Jb][c%8] = 16-bit scatter target of F_R Jb for the pair R = perm[c] of column c:
+// Ib * 4 | sign (bit 0); no connection, padding columns, the diagonal-pair columns (c >= noff8) and rows
+// past nstr (up to nrows, a whole number of tiles) -> 0xFFFF.  Chunk-major: the 8
+// targets of one 8-pair chunk of consecutive Jb sit in consecutive 16-byte words, so a warp (32
+// consecutive Jb) reads one chunk with fully coalesced loads.
+__global__ void k_tgt_rows16(const int32_t* __restrict__ tgt, uint16_t* __restrict__ out, int nstr, int nrows,
+                             int npp_in, const int* __restrict__ perm, int noff8, int npad_out) {
+    size_t total = (size_t)npad_out * nrows;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
         const int u = (int)(i & 7);
         const size_t cj = i >> 3;
-        const int c8 = (int)(cj / nstr), J = (int)(cj - (size_t)c8 * nstr);
-        const int R = 8 * c8 + u;
+        const int c8 = (int)(cj / nrows), J = (int)(cj - (size_t)c8 * nrows);
+        const int col = 8 * c8 + u;
+        const int R = col < noff8 ? perm[col] : -1;  // diagonal pairs are summed in registers, not scattered
         uint16_t v = 0xFFFFu;
-        if (R < npp_in) {
+        if (R >= 0 && J < nstr) {
             int32_t t = tgt[(size_t)J * npp_in + R];
-            if (t != kNoTarget) v = (uint16_t)(((uint32_t)t & kConnIdxMask) | (((uint32_t)t >> 31) << 15));
+            if (t != kNoTarget) v = (uint16_t)((((uint32_t)t & kConnIdxMask) << 2) | ((uint32_t)t >> 31));
         }
         out[i] = v;
     }
@@ -446,16 +519,31 @@ size_t tc_smem_bytes(int s1a, int npair, int nbs, bool three) { return tc_layout
 void ab_tc(Context& c, const double* C, double* S, bool three) {
     const int nas = (int)c.nas, nbs = (int)c.nbs;
     const int s1a = c.A.s1, npair = c.A.npair;
-    FCIB_CHECK(nbs < 32767, FCIB_ERR_UNSUPPORTED, "tensor-core opposite-spin kernel: too many beta strings");
-    TcLayout L = tc_layout(s1a, npair, nbs, three);
-    FCIB_CHECK(L.npad <= 144 && L.kpad <= 72 && L.npad / 8 <= 4 * kTcEpiC && L.kpad / 8 <= 4 * kTcGat,
+    FCIB_CHECK(nbs <= kMaxBetaStrings, FCIB_ERR_UNSUPPORTED, "tensor-core opposite-spin kernel: too many beta strings");
+    // columns: the n(n-1)/2 off-diagonal pairs in pair order (padded to a multiple of 8), then the n
+    // diagonal pairs (r,r)
+    const int n = c.n;
+    const int noff = n * (n - 1) / 2, noff8 = (noff + 7) / 8 * 8;
+    const int ncol = noff8 + n;
+    TcLayout L = tc_layout(s1a, ncol, nbs, three);
+    FCIB_CHECK(L.npad <= 144 && L.kpad <= 72 && noff8 / 8 <= 4 * kTcEpiC - 1 && n <= 16 && L.kpad / 8 <= 9,
                FCIB_ERR_UNSUPPORTED, "tensor-core kernel: more than 16 active orbitals");
+    const int ntiles = (nbs + kTcM - 1) / kTcM;
+    const int ldp = ntiles * kTcM;  // plane rows padded to whole tiles (zeros)
+    FCIB_CHECK((uint64_t)nas * ldp * sizeof(float2) < (1ull << 32), FCIB_ERR_UNSUPPORTED,
+               "tensor-core kernel: TF32 planes exceed the 32-bit gather offsets");
     size_t smem = std::max<size_t>(L.total, 120 * 1024);  // one CTA per SM (owns all tensor memory)
     FCIB_CHECK(smem + 2048 <= (size_t)c.smem_optin, FCIB_ERR_UNSUPPORTED,
                "tensor-core kernel: sigma row and integral block exceed shared memory");
     if (!c.tgtR16.p) {
-        c.tgtR16.alloc((size_t)L.npad * nbs);
-        k_tgt_rows16<<<4 * c.num_sms, 256, 0, c.stream>>>(c.B.tgt.p, c.tgtR16.p, nbs, c.B.npair_pad, L.npad);
+        std::vector<int> perm(L.npad, -1);
+        for (int p = 0, col = 0; p < n; p++)
+            for (int q = 0; q < p; q++) perm[col++] = p * (p + 1) / 2 + q;
+        for (int r = 0; r < n; r++) perm[noff8 + r] = r * (r + 1) / 2 + r;
+        c.tc_perm.upload(perm, c.stream);
+        c.tgtR16.alloc((size_t)L.npad * ldp);
+        k_tgt_rows16<<<4 * c.num_sms, 256, 0, c.stream>>>(c.B.tgt.p, c.tgtR16.p, nbs, ldp, c.B.npair_pad,
+                                                          c.tc_perm.p, noff8, L.npad);
         FCIB_KCHECK();
     }
     if (c.vmax <= 0.0f) {
@@ -465,7 +553,6 @@ void ab_tc(Context& c, const double* C, double* S, bool three) {
         for (double x : hv) m = std::max(m, std::fabs(x));
         c.vmax = (float)(m * (1.0 + 1e-6)) + 1e-30f;
     }
-    const int ldp = (nbs + 3) / 4 * 4;
     c.tf_hi.alloc(2 * (size_t)nas * ldp);  // interleaved hi/lo pairs
     ensure_counter(c);
     FCIB_CUDA(cudaMemsetAsync(c.counter.p, 0, 3 * sizeof(int), c.stream));
@@ -473,8 +560,7 @@ void ab_tc(Context& c, const double* C, double* S, bool three) {
     FCIB_CUDA(cudaMemsetAsync(cmax_bits, 0, sizeof(unsigned int), c.stream));
     c.c32.alloc((size_t)nas * nbs);
     float2* hl = reinterpret_cast<float2*>(c.tf_hi.p);
-    k_split_tf32<<<8 * c.num_sms, 256, 0, c.stream>>>(C, hl, c.c32.p, nas, nbs, ldp,
-                                                     cmax_bits);
+    k_split_tf32<<<8 * c.num_sms, 256, 0, c.stream>>>(C, hl, c.c32.p, nas, nbs, ldp, cmax_bits);
     FCIB_KCHECK();
     c.c32_ready = true;
     auto kern = three ? k_ab_tc<true> : k_ab_tc<false>;
@@ -482,9 +568,10 @@ void ab_tc(Context& c, const double* C, double* S, bool three) {
     int grid = std::min(nas, c.num_sms);
     c.tc_ev.ensure();
     FCIB_CUDA(cudaEventRecord(c.tc_ev.e[0], c.stream));
-    kern<<<grid, kTcThreads, smem, c.stream>>>(hl, ldp, C, S, c.A.conn.p, s1a, c.tgtR16.p, npair, c.V.p,
-                                              c.A.npair_pad, c.vmax, cmax_bits, nas, nbs, c.B.s1, c.scalar,
-                                              c.counter.p, c.counter.p + 1);
+    const int kb = c.nb;
+    kern<<<grid, kTcThreads, smem, c.stream>>>(hl, ldp, C, S, c.A.conn.p, s1a, c.tgtR16.p, ncol, c.tc_perm.p, noff8,
+                                              n, c.B.str.p, kb, c.V.p, c.A.npair_pad, c.vmax, cmax_bits, nas, nbs,
+                                              kb * (n - kb) + 1, c.scalar, c.counter.p, c.counter.p + 1);
     FCIB_KCHECK();
     FCIB_CUDA(cudaEventRecord(c.tc_ev.e[1], c.stream));
     c.tc_recorded = true;

@@ -180,8 +180,11 @@ class FCISolver:
         it = C.c_int()
         rc = capi.lib().fcib_solve(self._h, capi.dptr(e), capi.dptr(s2), C.byref(it))
         if rc == capi.FCIB_ERR_NOT_CONVERGED:
+            # the reference's message (forte/fci/fci_solver.cc:269-276)
             raise RuntimeError("Davidson-Liu solver did not converge.\nPlease try to increase the number of "
-                               "Davidson-Liu iterations (DL_MAXITER).")
+                               "Davidson-Liu iterations (DL_MAXITER). You can also try to increase:\n - the "
+                               "maximum size of the subspace (DL_SUBSPACE_PER_ROOT)"
+                               "\n - the number of guess states (DL_GUESS_PER_ROOT)")
         capi.check(rc)
         self._energies, self._spin2, self._iterations = e, s2, it.value
         return float(e[self._root])
@@ -256,6 +259,38 @@ class FCISolver:
             out.append(self._rdm_call(lambda *a, rl=rl, rr=rr: capi.lib().fcib_rdms(self._h, rl, rr, *a),
                                       max_rdm_level, rdm_type,
                                       lambda *a, rl=rl, rr=rr: capi.lib().fcib_rdms3(self._h, rl, rr, *a)))
+        return out
+
+    def max_abs_elements(self, num_dets, root=0):
+        """FCIVector::max_abs_elements (forte/fci/fci_vector_h_diag.cc:37-68) of a root: a list of
+        (|C|, C, alpha irrep, alpha address, beta address) tuples, largest |C| first."""
+        a = np.zeros(max(num_dets, 1))
+        v = np.zeros(max(num_dets, 1))
+        h = np.zeros(max(num_dets, 1), dtype=np.int32)
+        ia = np.zeros(max(num_dets, 1), dtype=np.int64)
+        ib = np.zeros(max(num_dets, 1), dtype=np.int64)
+        cnt = C.c_int()
+        capi.check(capi.lib().fcib_max_abs_elements(
+            self._h, root, num_dets, capi.dptr(a), capi.dptr(v), h.ctypes.data_as(C.POINTER(C.c_int)),
+            ia.ctypes.data_as(C.POINTER(C.c_int64)), ib.ctypes.data_as(C.POINTER(C.c_int64)), C.byref(cnt)))
+        return [(float(a[i]), float(v[i]), int(h[i]), int(ia[i]), int(ib[i])) for i in range(cnt.value)]
+
+    def transition_rdms(self, root_list, method2, max_rdm_level=1, rdm_type="spin_dependent"):
+        """FCISolver::transition_rdms (forte/fci/fci_solver_transition_rdms.cc:37-109): one RDMs object
+        per (left root of this solver, right root of method2) pair; method2 is another FCISolver on the
+        same orbitals and electrons, possibly for a state of another irrep.  As in the reference only
+        the one-body level exists (max_rdm_level >= 2 raises)."""
+        sf = rdm_type in ("spin_free", 1)
+        if max_rdm_level <= 0:
+            return [RDMs(sf) for _ in root_list]
+        n = self.ints.n
+        out = []
+        for (rl, rr) in root_list:
+            g1a = np.zeros((n, n))
+            g1b = np.zeros((n, n))
+            capi.check(capi.lib().fcib_transition_rdms(self._h, rl, method2._h, rr, max_rdm_level, 1 if sf else 0,
+                                                       capi.dptr(g1a), capi.dptr(g1b)))
+            out.append(RDMs(True, g1=g1a) if sf else RDMs(False, g1a=g1a, g1b=g1b))
         return out
 
     def compute_rdms(self, left, right=None, max_rdm_level=2, rdm_type="spin_dependent"):

@@ -109,6 +109,14 @@ int fcib_reset_guess(fcib_ctx* ctx);
 /* eigenvector of a root in FCIVector flat order (size from fcib_size) */
 int fcib_get_vector(fcib_ctx* ctx, int root, double* out);
 
+/* FCIVector::max_abs_elements (forte/fci/fci_vector_h_diag.cc:37-68) of a root of the last solve:
+ * the num_dets largest |C| in descending order (equal values in FCIVector flat order), each with its
+ * signed value, alpha irrep and the alpha / beta string addresses within their irreps; slots past the
+ * nonzero elements are zero, as in the reference.  *count = min(num_dets, size).  Any output may be
+ * NULL.  With print >= 1, fcib_solve also prints these for the 100 largest elements of every root
+ * (|C| >= 0.01), like FCISolver::print_solutions (fci_solver.cc:316-367). */
+int fcib_max_abs_elements(fcib_ctx* ctx, int root, int num_dets, double* abs_c, double* c, int* alfa_irrep,
+                          int64_t* alfa_address, int64_t* beta_address, int* count);
 /* sigma = H b for a host vector in FCIVector flat order */
 int fcib_sigma(fcib_ctx* ctx, const double* b, double* sigma);
 /* sigma for device vectors in the engine's C1 layout (na_str x nb_str row-major), on a
@@ -128,6 +136,15 @@ int fcib_rdms(fcib_ctx* ctx, int root_left, int root_right, int level, int spin_
  * replaces FCIVector::compute_rdms(C_left, C_right, max_rdm_level, type) (fci_vector_rdm.cc:43-145). */
 int fcib_compute_rdms(fcib_ctx* ctx, const double* left, const double* right, int level, int spin_free,
                       double* g1a, double* g1b, double* g2aa, double* g2ab, double* g2bb);
+/* Transition 1-RDMs <left root| a+_p a_q |right root> between the solutions of two contexts, whose
+ * states may belong to different irreps (FCISolver::transition_rdms(root_list, method2, max_rdm_level,
+ * type), forte/fci/fci_solver_transition_rdms.cc:37-109, compute_1rdm_different_irrep
+ * fci_vector_transition_rdm.cc:43-165).  Same orbitals, electrons and device in both contexts.
+ * level 1..3 is accepted, but as in the reference only level 1 is implemented (FCIB_ERR_UNSUPPORTED
+ * for 2 and 3).  spin_free = 0: g1a, g1b [n*n]; spin_free = 1: g1a <- g1a + g1b.  Like the reference,
+ * both blocks are zero when the states have no alpha electrons. */
+int fcib_transition_rdms(fcib_ctx* left, int root_left, fcib_ctx* right, int root_right, int level,
+                         int spin_free, double* g1a, double* g1b);
 /* 3-RDMs (max_rdm_level = 3 of FCISolver::rdms / FCIVector::compute_rdms, fci_vector_rdm.cc:70-137,
  * blocks compute_3rdm_aaa/aab/abb_same_irrep :395-565); fcib_rdms and fcib_compute_rdms accept
  * level 3 and return its one- and two-body parts.  Blocks are n^6 row-major in the reference's
@@ -237,12 +254,23 @@ int fcib_stream(fcib_ctx* ctx, void** stream);
  * buffers are created; the reduction scratch is a static per-device array of 598,600 bytes
  * (1024 partial-sum blocks) that every call shares.  Same kernels and grid as fcib_spin2, so
  * the value matches it bit for bit.  The first call on a device looks up the array's device
- * address (cudaGetSymbolAddress); make it before any stream capture.  The context's string
- * tables must already exist (FCIB_ERR_STATE otherwise); a launch needing more than 1024
- * blocks returns FCIB_ERR_UNSUPPORTED.  Calls on one device that overlap on the GPU race on
- * the shared scratch: serialise them.  stream: cudaStream_t as void*, NULL = the context's
- * stream; the call synchronizes it.  No counterpart in the reference. */
+ * address (cudaGetSymbolAddress); make it before any stream capture.  The address is kept with
+ * the ID of the device's CUDA context and looked up again when that changes (after
+ * cudaDeviceReset the module is loaded at a new address), so make the first call after a reset
+ * before any capture too.  The context's string tables must already exist (FCIB_ERR_STATE
+ * otherwise); a launch needing more than 1024 blocks returns FCIB_ERR_UNSUPPORTED.  Calls on one
+ * device that overlap on the GPU race on the shared scratch: serialise them.  d_c is in the C1
+ * layout (zeros outside the target irrep when the state has symmetry).  stream: cudaStream_t as
+ * void*, NULL = the context's stream, which is a non-blocking stream and so is NOT ordered after
+ * the legacy default stream or the caller's streams: either pass the stream that wrote d_c, or
+ * make sure d_c is complete before the call.  The call synchronizes the stream it runs on.  No
+ * counterpart in the reference. */
 int fcib_spin2_device_noalloc(fcib_ctx* ctx, const double* d_c, double* s2, void* stream);
+
+/* FP64 throughput of the GPU in TFLOP/s, measured with CUDA events (no setting changed):
+ * dfma = CUDA-core FMA chains, dmma = FP64 tensor-core MMAs (mma.sync m8n8k4).  The
+ * denominators of the FP64 sigma kernels' roofline fractions.  No counterpart in the reference. */
+int fcib_fp64_peak(int device, double* dfma_tflops, double* dmma_tflops);
 
 #ifdef __cplusplus
 }

@@ -643,6 +643,102 @@ double orc_slater_rules(void* h, uint64_t la, uint64_t lb, uint64_t ra, uint64_t
     return slater_rules((orc_ctx*)h, la, lb, ra, rb);
 }
 
+/* Selected rows of sigma = H C in the C1 determinant space, one row at a time from the Slater
+ * rules: sigma_I = e0 C_I + sum_J <I|H|J> C_J over every J that differs from I by at most a
+ * double replacement (ActiveSpaceIntegrals::slater_rules, forte/integrals/active_space_integrals.cc:
+ * 247-411, for the same operator FCIVector::Hamiltonian applies, fci_vector_hamiltonian.cc:46-272).
+ * Needs no substitution lists, so it reaches sizes where a whole oracle sigma would take hours.
+ * C is the full vector in C1 flat order (alpha string index * nbs + beta string index, strings in
+ * FCIStringLists order); rows[] are determinant indices; abs_out[i] (may be NULL) receives
+ * sum_J |<I|H|J> C_J|, the scale of the row's rounding error. */
+int orc_sigma_rows(int n, int na, int nb, double e0, const double* oei_a, const double* oei_b,
+                   const double* tei_aa, const double* tei_ab, const double* tei_bb, const double* C,
+                   int64_t nrows, const int64_t* rows, double* out, double* abs_out) {
+    if (n < 1 || n > ORC_MAXN || na < 0 || nb < 0 || na > n || nb > n) return fail("orc_sigma_rows: bad sizes");
+    orc_ctx c;
+    memset(&c, 0, sizeof(c));
+    c.n = n;
+    c.oei_a = (double*)oei_a; c.oei_b = (double*)oei_b;
+    c.tei_aa = (double*)tei_aa; c.tei_ab = (double*)tei_ab; c.tei_bb = (double*)tei_bb;
+    const int64_t nas = binom(n, na), nbs = binom(n, nb);
+    uint64_t* sa = (uint64_t*)malloc(sizeof(uint64_t) * (nas > 0 ? nas : 1));
+    uint64_t* sb = (uint64_t*)malloc(sizeof(uint64_t) * (nbs > 0 ? nbs : 1));
+    int32_t* addr = (int32_t*)malloc(sizeof(int32_t) * ((size_t)1 << n));
+    if (!sa || !sb || !addr) { free(sa); free(sb); free(addr); return fail("orc_sigma_rows: out of memory"); }
+    orc_make_strings(n, na, sa);
+    orc_make_strings(n, nb, sb);
+    /* string -> index within its spin (the alpha and beta lists are separate when na != nb) */
+    int32_t* addr_b = NULL;
+    for (int64_t i = 0; i < nas; i++) addr[sa[i]] = (int32_t)i;
+    if (na != nb) {
+        addr_b = (int32_t*)malloc(sizeof(int32_t) * ((size_t)1 << n));
+        if (!addr_b) { free(sa); free(sb); free(addr); return fail("orc_sigma_rows: out of memory"); }
+        for (int64_t i = 0; i < nbs; i++) addr_b[sb[i]] = (int32_t)i;
+    }
+    const int32_t* ab = addr_b ? addr_b : addr;
+    const uint64_t full = (n == 64) ? ~0ull : ((1ull << n) - 1ull);
+    for (int64_t t = 0; t < nrows; t++) {
+        const int64_t I = rows[t];
+        const uint64_t Ia = sa[I / nbs], Ib = sb[I % nbs];
+        double acc = 0.0, aacc = 0.0;
+#define ORC_ADD(Ja, Jb)                                                          \
+        do {                                                                     \
+            const int64_t J_ = (int64_t)addr[(Ja)] * nbs + ab[(Jb)];             \
+            double h_ = slater_rules(&c, Ia, Ib, (Ja), (Jb));                    \
+            if ((Ja) == Ia && (Jb) == Ib) h_ += e0;                              \
+            const double v_ = h_ * C[J_];                                        \
+            acc += v_;                                                           \
+            aacc += fabs(v_);                                                    \
+        } while (0)
+        ORC_ADD(Ia, Ib);
+        /* alpha replacements of rank 1 and 2, each combined with beta replacements of rank 0/1,
+         * and beta replacements of rank 1 and 2 with the alpha string fixed */
+        const uint64_t occa = Ia, vira = full & ~Ia, occb = Ib, virb = full & ~Ib;
+        for (uint64_t oi = occa; oi; oi &= oi - 1) {
+            const int i = __builtin_ctzll(oi);
+            for (uint64_t va = vira; va; va &= va - 1) {
+                const int a = __builtin_ctzll(va);
+                const uint64_t Ja = (Ia & ~(1ull << i)) | (1ull << a);
+                ORC_ADD(Ja, Ib);
+                for (uint64_t oj = occb; oj; oj &= oj - 1) {
+                    const int j = __builtin_ctzll(oj);
+                    for (uint64_t vb = virb; vb; vb &= vb - 1) {
+                        const int b = __builtin_ctzll(vb);
+                        ORC_ADD(Ja, (Ib & ~(1ull << j)) | (1ull << b));
+                    }
+                }
+                for (uint64_t oj = oi & (oi - 1); oj; oj &= oj - 1) {
+                    const int j = __builtin_ctzll(oj);
+                    for (uint64_t vb = va & (va - 1); vb; vb &= vb - 1) {
+                        const int b = __builtin_ctzll(vb);
+                        ORC_ADD((Ja & ~(1ull << j)) | (1ull << b), Ib);
+                    }
+                }
+            }
+        }
+        for (uint64_t oi = occb; oi; oi &= oi - 1) {
+            const int i = __builtin_ctzll(oi);
+            for (uint64_t vb = virb; vb; vb &= vb - 1) {
+                const int b = __builtin_ctzll(vb);
+                const uint64_t Jb = (Ib & ~(1ull << i)) | (1ull << b);
+                ORC_ADD(Ia, Jb);
+                for (uint64_t oj = oi & (oi - 1); oj; oj &= oj - 1) {
+                    const int j = __builtin_ctzll(oj);
+                    for (uint64_t vc = vb & (vb - 1); vc; vc &= vc - 1) {
+                        const int d = __builtin_ctzll(vc);
+                        ORC_ADD(Ia, (Jb & ~(1ull << j)) | (1ull << d));
+                    }
+                }
+            }
+        }
+#undef ORC_ADD
+        out[t] = acc;
+        if (abs_out) abs_out[t] = aacc;
+    }
+    free(sa); free(sb); free(addr); free(addr_b);
+    return 0;
+}
+
 /* spin2(lhs, rhs) (forte/sparse_ci/determinant.hpp:910-958) */
 static double det_spin2(uint64_t Ia, uint64_t Ib, uint64_t Ja, uint64_t Jb, int nmo) {
     if (popc(Ia) != popc(Ja) || popc(Ib) != popc(Jb)) return 0.0;

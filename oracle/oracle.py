@@ -56,6 +56,8 @@ def lib():
         L.orc_spin2.restype = C.c_double
         L.orc_spin2.argtypes = [vp, dp]
         L.orc_rdms.argtypes = [vp, dp, dp, C.c_int, dp, dp, dp, dp, dp]
+        L.orc_sigma_rows.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, dp, dp, dp, dp, dp, dp, C.c_int64,
+                                     C.POINTER(C.c_int64), dp, dp]
         L.orc_rdms3.argtypes = [vp, dp, dp, dp, dp, dp, dp]
         L.orc_last_error.restype = C.c_char_p
         _LIB = L
@@ -175,6 +177,23 @@ class Oracle:
         if lib().orc_rdms3(self.h, _dp(cl), _dp(cr), *[_dp(out[k]) for k in ("g3aaa", "g3aab", "g3abb", "g3bbb")]) < 0:
             raise RuntimeError(lib().orc_last_error().decode())
         return out
+
+
+def sigma_rows(ints, na, nb, c, rows):
+    """Rows ``rows`` (C1 determinant indices) of sigma = H c from the Slater rules over each row's
+    connected determinants; returns (sigma rows, sum of |H_IJ c_J| per row).  Works at any size the
+    vector fits in host memory (no substitution lists)."""
+    c = np.ascontiguousarray(c, dtype=np.float64)
+    rows = np.ascontiguousarray(rows, dtype=np.int64)
+    arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in
+            (ints.oei_a, ints.oei_b, ints.tei_aa, ints.tei_ab, ints.tei_bb)]
+    out = np.zeros(len(rows))
+    aout = np.zeros(len(rows))
+    L = lib()
+    if L.orc_sigma_rows(int(ints.n), na, nb, float(ints.scalar), *[_dp(x) for x in arrs], _dp(c), len(rows),
+                        rows.ctypes.data_as(C.POINTER(C.c_int64)), _dp(out), _dp(aout)) != 0:
+        raise RuntimeError(L.orc_last_error().decode())
+    return out, aout
 
 
 def jacobi(A):

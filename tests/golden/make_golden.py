@@ -1,6 +1,6 @@
 """Generates the golden fixtures in this folder from the reference's own test inputs.
 
-Run in a container where the Forte checkout is mounted (default path below).  Reads the
+Usage: python make_golden.py <path of a Forte checkout>.  Reads the
 FCIDUMP integral files of tests/methods/integrals-fcidump-{1..6} and stores them as compact
 npz fixtures, together with the reference energies those tests assert
 (tests/methods/integrals-fcidump-N/input.dat: ``reffci``) and the active-space settings of
@@ -13,7 +13,9 @@ import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: python make_golden.py <path of a Forte checkout>")
+REF = sys.argv[1]
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 

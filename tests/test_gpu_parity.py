@@ -142,3 +142,56 @@ def test_non_convergence_raises_when_asked():
     s.set_die_if_not_converged(True)
     with pytest.raises(RuntimeError):
         s.compute_energy()
+
+
+def _block_addresses(s, orbsym, irrep):
+    """(alpha irrep, alpha address, beta address) of every FCIVector flat position."""
+    sa = s.strings(0).astype(np.int64)
+    sb = s.strings(1).astype(np.int64)
+
+    def sym(x):
+        h = 0
+        for i, o in enumerate(orbsym):
+            if (x >> i) & 1:
+                h ^= o
+        return h
+
+    ha = np.array([sym(int(x)) for x in sa])
+    hb = np.array([sym(int(x)) for x in sb])
+    out = []
+    for h in range(8):
+        na_h = int(np.sum(ha == h))
+        nb_h = int(np.sum(hb == (h ^ irrep)))
+        for ia in range(na_h):
+            for ib in range(nb_h):
+                out.append((h, ia, ib))
+    return out
+
+
+@pytest.mark.parametrize("case", ["golden1", "c1"])
+def test_max_abs_elements_reference_order(case, capfd):
+    """FCIVector::max_abs_elements: the largest |C| first, equal values in flat order (the reference's
+    insertion keeps the first one found), each with its alpha irrep and string addresses; and the
+    PRINT >= 1 listing of FCISolver::print_solutions."""
+    if case == "golden1":
+        ints, na, nb, irrep, mult, ref = golden_cases.load(1)
+        state = StateInfo(na, nb, mult, na - nb, irrep)
+    else:
+        ints = synthetic(8, 24, 2)
+        na, nb, irrep = 4, 4, 0
+        state = StateInfo(4, 4, 1)
+    s = FCISolver(state, 2, ints, {"E_CONVERGENCE": 1e-12, "PRINT": 1})
+    s.compute_energy()
+    out = capfd.readouterr().out
+    assert "==> Root No. 0 <==" in out and "==> Root No. 1 <==" in out and "Total Energy:" in out
+    addr = _block_addresses(s, ints.orbsym, irrep if case == "golden1" else 0)
+    for root in (0, 1):
+        c = s.evecs()[root]
+        k = 40
+        got = s.max_abs_elements(k, root)
+        order = np.argsort(-np.abs(c), kind="stable")[:k]
+        assert len(got) == min(k, c.size)
+        for t, i in enumerate(order):
+            a, v, h, ia, ib = got[t]
+            assert a == abs(c[i]) and v == c[i]
+            assert (h, ia, ib) == addr[i]

@@ -110,3 +110,22 @@ def test_rdms_bruteforce():
     e += 0.25 * np.sum(ints.tei_aa * g["g2aa"]) + 0.25 * np.sum(ints.tei_bb * g["g2bb"])
     e += np.sum(ints.tei_ab * g["g2ab"])
     assert abs(e - r["energies"][0]) < 1e-10
+
+
+@pytest.mark.parametrize("n,na,nb", [(6, 3, 3), (7, 4, 2), (8, 4, 4), (6, 1, 0), (5, 0, 2)])
+def test_sigma_rows_equal_list_sigma(n, na, nb):
+    """Row-wise Slater-rule sigma (used to check CAS(16,16) rows) against the list-driven oracle
+    sigma on every row, with a nonzero scalar energy."""
+    from oracle.oracle import sigma_rows
+
+    ints = I.synthetic(n, 3 * n, 11)
+    ints.scalar = 0.37
+    o = Oracle(n, na, nb)
+    o.set_integrals(ints)
+    rng = np.random.default_rng(n * 100 + na * 10 + nb)
+    c = rng.normal(size=o.ndet)
+    full = o.sigma(c)
+    rows = np.arange(o.ndet)
+    got, scale = sigma_rows(ints, na, nb, c, rows)
+    assert np.all(scale >= np.abs(got) - 1e-12)
+    np.testing.assert_allclose(got, full, rtol=0, atol=1e-12 * max(1.0, np.abs(full).max()))

@@ -15,11 +15,38 @@ from forte_b200 import FCISolver, StateInfo, capi, synthetic
 pytestmark = pytest.mark.gpu
 
 
-def _noalloc(solver, dev_tensor):
+def _noalloc(solver, dev_tensor, stream=None):
     s2 = C.c_double()
     capi.check(capi.lib().fcib_spin2_device_noalloc(solver._h, C.c_void_p(dev_tensor.data_ptr()),
-                                                    C.byref(s2), None))
+                                                    C.byref(s2), None if stream is None else C.c_void_p(stream)))
     return s2.value
+
+
+def _c1_from_flat(solver, orbsym, irrep, flat):
+    """FCIVector flat order (alpha irrep blocks) -> the engine's C1 layout, zero outside the
+    target irrep, as a device vector must be laid out for the *_device entry points."""
+    sa = solver.strings(0).astype(np.int64)
+    sb = solver.strings(1).astype(np.int64)
+
+    def sym(s):
+        h = 0
+        for i, o in enumerate(orbsym):
+            if (s >> i) & 1:
+                h ^= o
+        return h
+
+    ha = np.array([sym(int(x)) for x in sa])
+    hb = np.array([sym(int(x)) for x in sb])
+    full = np.zeros(len(sa) * len(sb))
+    pos = 0
+    for h in range(8):
+        rows = np.nonzero(ha == h)[0]
+        cols = np.nonzero(hb == (h ^ irrep))[0]
+        for i in rows:
+            full[i * len(sb) + cols] = flat[pos:pos + len(cols)]
+            pos += len(cols)
+    assert pos == len(flat)
+    return full
 
 
 @pytest.mark.parametrize("n,na,nb", [(6, 3, 3), (8, 4, 3), (10, 5, 5)])
@@ -58,3 +85,42 @@ def test_noalloc_requires_tables():
         assert rc == capi.FCIB_ERR_ARG
     finally:
         L.fcib_destroy(h)
+
+
+def test_noalloc_on_caller_stream():
+    """The caller passes the stream that produced the vector (here torch's current stream, a
+    non-default one), so the reduction is ordered after the copy that filled it."""
+    import torch
+
+    ints = synthetic(8, 24, 5)
+    s = FCISolver(StateInfo(4, 4, 0), 1, ints)
+    rng = np.random.default_rng(3)
+    c = rng.normal(size=s.size())
+    c /= np.linalg.norm(c)
+    ref = s.compute_spin2(c)
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        d = torch.from_numpy(c).pin_memory().to("cuda", non_blocking=True)
+        got = [_noalloc(s, d, torch.cuda.current_stream().cuda_stream) for _ in range(2)]
+    assert got == [ref, ref]
+
+
+def test_noalloc_with_symmetry_golden_c2v():
+    """C2v golden CAS (784 determinants in the A1 block): the device vector is in the C1 layout
+    with zeros outside the target irrep; the value equals fcib_spin2 on the flat-order vector."""
+    import torch
+
+    import golden_cases
+
+    ints, na, nb, irrep, mult, ref_e = golden_cases.load(1)
+    s = FCISolver(StateInfo(na, nb, mult, na - nb, irrep), 1, ints)
+    s.compute_energy()
+    flat = s.evecs()[0]
+    assert flat.size == 784
+    ref = s.compute_spin2(flat)
+    full = _c1_from_flat(s, ints.orbsym, irrep, flat)
+    d = torch.from_numpy(full).cuda()
+    torch.cuda.synchronize()
+    got = [_noalloc(s, d) for _ in range(2)]
+    assert got == [ref, ref]
+    assert abs(ref - 0.25 * (mult * mult - 1)) < 1e-6
