@@ -27,6 +27,7 @@ class BatchSolver:
         o.r_convergence = float(opts["R_CONVERGENCE"])
         o.subspace_per_root = int(opts["DL_SUBSPACE_PER_ROOT"])
         o.collapse_per_root = int(opts["DL_COLLAPSE_PER_ROOT"])
+        o.precision = capi.PREC_FP64 if str(opts.get("FCI_PRECISION", "FP64")).upper() == "FP64" else capi.PREC_MIXED
         self.ninst = len(instances)
         self.nroot = nroot
         k = self.ninst
@@ -68,9 +69,12 @@ class BatchSolver:
         return e, it, cv.astype(bool), ms.value
 
     def tune(self):
+        """Autotuner: opposite-spin sigma tile (pairs per work item) x launch shape; keeps the fastest."""
         t = C.c_int()
         c = C.c_int()
-        shapes = np.zeros(4)
-        capi.check(capi.lib().fcib_batch_tune(self._h, C.byref(t), C.byref(c), capi.dptr(shapes)))
-        return {"threads": t.value, "ctas_per_sm": c.value,
-                "shapes_ms": dict(zip(["256x1", "512x1", "256x2", "128x2"], shapes.tolist()))}
+        p = C.c_int()
+        times = np.zeros(12)
+        capi.check(capi.lib().fcib_batch_tune(self._h, C.byref(t), C.byref(c), C.byref(p), capi.dptr(times)))
+        names = [f"tile{tile}_{shape}" for tile in (8, 16, 32) for shape in ("256x1", "512x1", "256x2", "128x2")]
+        return {"threads": t.value, "ctas_per_sm": c.value, "pair_tile": p.value,
+                "times_ms": dict(zip(names, times.tolist()))}

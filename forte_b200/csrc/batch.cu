@@ -2,19 +2,25 @@
 // (no counterpart in the reference, whose FCISolver handles one instance per call).
 //
 // k_batch_dl is persistent: each CTA takes the next instance from an atomic counter (instances
-// are ordered largest first) and runs the whole Davidson-Liu solve for it in FP64.  All of an
-// instance's iterations run inside this one kernel:
-//   sigma:   opposite-spin + one-body (folded into the pair matrix V, the engine's formulation):
-//              s[Ia,Ib] = sum_{k in conn(Ia)} sum_{m in conn(Ib)} s_k s_m V[P_k][R_m] c[J_k,J_m]
-//            then the alpha and beta same-spin terms over the (N-2)-electron groups,
-//              s[I_i] += s_i sum_j M[lab_i][lab_j] s_j c[I_j],
-//            with one thread owning each column (alpha) or row (beta), so no atomics are needed;
+// are ordered largest first) and runs the whole Davidson-Liu solve for it.  All of an instance's
+// iterations run inside this one kernel:
+//   sigma:   opposite-spin + one-body (folded into the pair matrix V, the engine's formulation),
+//            one target alpha row at a time: B[k][R] = s_k V[P_k][R] in shared memory, every
+//            (beta string, pair tile) work item forms T[Jb][R] = sum_k c[J_k][Jb] B[k][R] in
+//            registers and adds it to the row at the beta replacement F_R Jb (FP64 shared-memory
+//            atomics); then the alpha and beta same-spin terms over the (N-2)-electron groups,
+//              s[I_i] += s_i sum_j W[i][j] s_j c[I_j],   W[i][j] = M[lab_i][lab_j] in shared memory,
+//            with one thread owning each column (alpha) or row (beta), so no atomics are needed.
+//            Products and sums in FP32 (mixed phase) or FP64; vectors always FP64.  The pair tile
+//            (8, 16 or 32 pairs per work item) and the launch shape are autotuned.
 //   subspace: G = B S^T (FP64), eigenpairs by a warp-parallel cyclic Jacobi in shared memory;
 //   residuals r_k = sum_j a_jk (s_j - lambda_k b_j), diagonal corrections r/(lambda - H_II)
 //            (0 when |lambda - H_II| <= 1e-6), normalised, two-pass Gram-Schmidt, discarded
 //            below 1e-7 (the reference's thresholds, davidson_liu_solver.cc:432-687);
 //   collapse to collapse_per_root * nroot Ritz vectors when the subspace is full.
-// Convergence needs |dlambda| < e_convergence and ||r|| < r_convergence for every root.
+// Convergence needs |dlambda| < e_convergence and ||r|| < r_convergence for every root; in mixed
+// precision the FP32 iteration's convergence triggers a restart from the nroot Ritz vectors with
+// FP64 sigma, and only the FP64 iteration's convergence ends the solve.
 // Guess: unit vectors on the 2 * nroot lowest diagonal elements (no spin selection).
 #include <algorithm>
 #include <memory>
@@ -34,6 +40,8 @@ struct BatchInst {
     double scalar;
     const uint32_t *stra, *strb, *conna, *connb, *g2ra, *g2rb;
     const uint16_t *g2la, *g2lb;
+    const int32_t* tgtb;              // beta F_R J -> I | sign << 31 (kNoTarget: none), row stride nppb
+    int nppb;
     const double *V, *Ma, *Mb, *dg;  // dg: da[n] db[n] Aaa[n*n] Abb[n*n] Aab[n*n]
     double* vec;                      // hd[N] | B[msub][N] | S[msub][N] | R[nroot][N]
 };
@@ -41,6 +49,7 @@ struct BatchInst {
 struct BatchOpts {
     int nroot, maxiter;
     double e_conv, r_conv;
+    int mixed;  // FP32 sigma until converged, then FP64 sigma from the Ritz vectors to convergence
 };
 
 struct BatchShared {  // per-CTA shared scalars
@@ -88,71 +97,80 @@ __device__ void bdots(const double* __restrict__ x, const double* __restrict__ B
     bsum(acc, nb, S);
 }
 
-// sigma of one instance by the whole CTA (see the file comment).  X: shared-memory scratch of
-// xcap doubles; grp: shared staging of a same-spin group's rows and labels (2 * kBMaxG ints).
+// sigma of one instance by the whole CTA, FP64 in and out, products and sums in T (float in the
+// mixed phase, double otherwise).  scratch: shared memory for the pair block B[k][R] (T), the sigma
+// row (double) and the row's connections; grp: a same-spin group's rows and labels.
+//   opposite spin + folded one-body terms, one target alpha row Ia at a time:
+//     B[k][R] = s_k V[P_k][R] for the row's connections k;  every (Jb, 16-pair chunk) work item forms
+//     T[Jb][R] = sum_k c[J_k][Jb] B[k][R] in registers and adds s_R T[Jb][R] to the sigma row at
+//     F_R Jb (FP64 shared-memory atomics); the row then goes to global memory.
+//   same spin: per (N-2)-electron group, W[i][j] = M[lab_i][lab_j] in shared memory, every thread
+//     owns a column (alpha) or row (beta) line and applies W to the group's rows of its line.
+// RC: pairs per work item in the opposite-spin term (the autotuned sigma tile: 8, 16 or 32)
+template <typename T, int RC>
 __device__ void bsigma(const BatchInst& P, const double* __restrict__ V, const double* __restrict__ Ma,
                        const double* __restrict__ Mb, const double* __restrict__ c, double* __restrict__ s,
-                       double* __restrict__ X, int xcap, int* __restrict__ grp) {
-    const int nbs = P.nbs, nas = P.nas, npp = P.npp, npl = P.npl, s1a = P.s1a, s1b = P.s1b;
+                       unsigned char* __restrict__ scratch, int* __restrict__ grp) {
+    const int nbs = P.nbs, nas = P.nas, npp = P.npp, npl = P.npl, s1a = P.s1a;
     const int tid = threadIdx.x, nth = blockDim.x;
-    // opposite spin + folded one-body terms, one target alpha row at a time:
-    //   X[R][Jb] = sum_k s_k V[P_k][R] c[J_k][Jb] for a chunk of pairs R, then
-    //   s[Ia][Ib] += sum_m s_m X[R_m][J_m] over the beta connections of Ib
-    const int rc = max(1, min(npp, xcap / nbs));
-    const int tpc = max(1, nth / nbs);  // threads per column in the X build
-    const int part = tid / nbs, col0 = tid - part * nbs;
+    const int nch = (npp + RC - 1) / RC;
+    const int ldb = nch * RC;  // B rows padded to whole chunks (zeros)
+    T* Bt = reinterpret_cast<T*>(scratch);
+    double* srow = reinterpret_cast<double*>(scratch + (((size_t)s1a * ldb * sizeof(T) + 15) / 16) * 16);
+    uint32_t* cs = reinterpret_cast<uint32_t*>(srow + nbs);
     for (int ia = 0; ia < nas; ia++) {
-        const uint32_t* ca = P.conna + (size_t)ia * s1a;
-        for (int r0 = 0; r0 < npp; r0 += rc) {
-            const int rn = min(rc, npp - r0);
-            if (part < tpc) {
-                for (int col = col0; col < nbs; col += (tpc == 1 ? nth : nbs)) {
-                    // chunks of kBKC alpha connections held in registers; X accumulates in shared memory
-                    for (int k0 = 0; k0 < s1a; k0 += kBKC) {
-                        const int kn = min(kBKC, s1a - k0);
-                        double ck[kBKC];
-                        int pk[kBKC];
-#pragma unroll
-                        for (int k = 0; k < kBKC; k++) {
-                            ck[k] = 0.0;
-                            pk[k] = 0;
-                            if (k < kn) {
-                                const uint32_t e = ca[k0 + k];
-                                const double v = c[(size_t)(e & kConnIdxMask) * nbs + col];
-                                ck[k] = (e >> 31) ? -v : v;
-                                pk[k] = (int)((e >> 21) & 0x3FFu) * npp + r0;
-                            }
-                        }
-                        for (int R = part; R < rn; R += tpc) {
-                            double x = (k0 == 0) ? 0.0 : X[(size_t)R * nbs + col];
-#pragma unroll
-                            for (int k = 0; k < kBKC; k++) x = fma(V[pk[k] + R], ck[k], x);
-                            X[(size_t)R * nbs + col] = x;
-                        }
-                    }
-                    if (tpc > 1) break;
-                }
+        for (int k = tid; k < s1a; k += nth) cs[k] = P.conna[(size_t)ia * s1a + k];
+        for (int j = tid; j < nbs; j += nth) srow[j] = P.scalar * c[(size_t)ia * nbs + j];
+        __syncthreads();
+        for (int idx = tid; idx < s1a * ldb; idx += nth) {
+            const int k = idx / ldb, R = idx - k * ldb;
+            double v = 0.0;
+            if (R < npp) {
+                const uint32_t e = cs[k];
+                v = V[(size_t)((e >> 21) & 0x3FFu) * npp + R];
+                if (e >> 31) v = -v;
             }
-            __syncthreads();
-            for (int ib = tid; ib < nbs; ib += nth) {
-                const size_t e = (size_t)ia * nbs + ib;
-                double acc = (r0 == 0) ? P.scalar * c[e] : s[e];
-                const uint32_t* cb = P.connb + (size_t)ib * s1b;
-                for (int m = 0; m < s1b; m++) {
-                    const uint32_t f = cb[m];
-                    const int R = (int)((f >> 21) & 0x3FFu) - r0;
-                    if (R >= 0 && R < rn) {
-                        const double x = X[(size_t)R * nbs + (f & kConnIdxMask)];
-                        acc += (f >> 31) ? -x : x;
-                    }
-                }
-                s[e] = acc;
-            }
-            __syncthreads();
+            Bt[idx] = (T)v;
         }
+        __syncthreads();
+        for (int item = tid; item < nbs * nch; item += nth) {
+            const int ch = item / nbs, jb = item - ch * nbs;
+            T acc[RC];
+#pragma unroll
+            for (int r = 0; r < RC; r++) acc[r] = (T)0;
+            const T* br = Bt + ch * RC;
+            // the gathered elements of 8 connections are loaded together, then used
+            for (int k0 = 0; k0 < s1a; k0 += 8) {
+                T a[8];
+#pragma unroll
+                for (int u = 0; u < 8; u++)
+                    a[u] = (k0 + u < s1a) ? (T)c[(size_t)(cs[k0 + u] & kConnIdxMask) * nbs + jb] : (T)0;
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    if (k0 + u < s1a) {
+#pragma unroll
+                        for (int r = 0; r < RC; r++) acc[r] = fma(a[u], br[(size_t)(k0 + u) * ldb + r], acc[r]);
+                    }
+                }
+            }
+            const int32_t* tg = P.tgtb + (size_t)jb * P.nppb + ch * RC;
+#pragma unroll
+            for (int r = 0; r < RC; r++) {
+                if (ch * RC + r < npp) {
+                    const int32_t t = tg[r];
+                    if (t != kNoTarget) {
+                        const double v = (double)acc[r];
+                        atomicAdd(&srow[t & kConnIdxMask], (t & (int32_t)kSignBit) ? -v : v);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        for (int j = tid; j < nbs; j += nth) s[(size_t)ia * nbs + j] = srow[j];
+        __syncthreads();
     }
-    // same-spin terms over the (N-2)-electron groups; a group's rows and labels are staged in
-    // shared memory, and tpc threads per column (alpha) or row (beta) split the group's rows
+    // same-spin terms over the (N-2)-electron groups
+    T* W = reinterpret_cast<T*>(scratch);  // [kBMaxG][kBMaxG], reuses the opposite-spin scratch
     for (int spin = 0; spin < 2; spin++) {
         const int ng = spin ? P.ng2b : P.ng2a;
         if (!ng) continue;
@@ -163,8 +181,6 @@ __device__ void bsigma(const BatchInst& P, const double* __restrict__ V, const d
         const int nlines = spin ? nas : nbs;   // columns (alpha) or rows (beta) owned by threads
         const size_t stride = spin ? 1 : (size_t)nbs;  // distance between consecutive strings
         const size_t lstep = spin ? (size_t)nbs : 1;   // distance between consecutive lines
-        const int tpl = max(1, nth / nlines);
-        const int pt = tid / nlines, l0 = tid - pt * nlines;
         int* rows_s = grp;
         int* labs_s = grp + kBMaxG;
         for (int g = 0; g < ng; g++) {
@@ -173,34 +189,47 @@ __device__ void bsigma(const BatchInst& P, const double* __restrict__ V, const d
                 labs_s[tid] = glabp[(size_t)g * m + tid];
             }
             __syncthreads();
-            if (pt < tpl) {
-                for (int line = l0; line < nlines; line += (tpl == 1 ? nth : nlines)) {
-                    const double* cl = c + (size_t)line * lstep;
-                    double* sl = s + (size_t)line * lstep;
-                    double x[kBMaxG];
+            for (int idx = tid; idx < m * m; idx += nth) {
+                const int i = idx / m, j = idx - i * m;
+                W[i * kBMaxG + j] = (T)M[(size_t)labs_s[i] * npl + labs_s[j]];
+            }
+            __syncthreads();
+            for (int line = tid; line < nlines; line += nth) {
+                const double* cl = c + (size_t)line * lstep;
+                double* sl = s + (size_t)line * lstep;
+                T x[kBMaxG];
 #pragma unroll
-                    for (int j = 0; j < kBMaxG; j++) {
-                        if (j < m) {
-                            const uint32_t r = (uint32_t)rows_s[j];
-                            const double v = cl[(size_t)(r & kConnIdxMask) * stride];
-                            x[j] = (r >> 31) ? -v : v;
-                        }
+                for (int j = 0; j < kBMaxG; j++) {
+                    x[j] = (T)0;
+                    if (j < m) {
+                        const uint32_t r = (uint32_t)rows_s[j];
+                        const T v = (T)cl[(size_t)(r & kConnIdxMask) * stride];
+                        x[j] = (r >> 31) ? -v : v;
                     }
-                    for (int i = pt; i < m; i += tpl) {
-                        const double* mr = M + (size_t)labs_s[i] * npl;
-                        double a = 0.0;
+                }
+                for (int i = 0; i < m; i++) {
+                    const T* wr = W + i * kBMaxG;
+                    T a = (T)0;
 #pragma unroll
-                        for (int j = 0; j < kBMaxG; j++)
-                            if (j < m) a = fma(mr[labs_s[j]], x[j], a);
-                        const uint32_t r = (uint32_t)rows_s[i];
-                        sl[(size_t)(r & kConnIdxMask) * stride] += (r >> 31) ? -a : a;
-                    }
-                    if (tpl > 1) break;
+                    for (int j = 0; j < kBMaxG; j++)
+                        if (j < m) a = fma(wr[j], x[j], a);
+                    const uint32_t r = (uint32_t)rows_s[i];
+                    const double ad = (double)a;
+                    sl[(size_t)(r & kConnIdxMask) * stride] += (r >> 31) ? -ad : ad;
                 }
             }
             __syncthreads();
         }
     }
+}
+
+// shared-memory scratch of bsigma in bytes (the larger of the opposite-spin block and the group W),
+// for the largest pair tile (32)
+__host__ __device__ inline size_t bsigma_scratch(int s1a, int npp, int nbs) {
+    const int ldb = (npp + 31) / 32 * 32;
+    const size_t opp = ((size_t)s1a * ldb * sizeof(double) + 15) / 16 * 16 + (size_t)nbs * 8 + (size_t)s1a * 4;
+    const size_t grp = (size_t)kBMaxG * kBMaxG * sizeof(double);
+    return opp > grp ? opp : grp;
 }
 
 // eigenpairs of the symmetric n x n matrix S.G (leading dimension kBMaxSub) by cyclic Jacobi
@@ -275,6 +304,7 @@ __device__ void bjacobi(BatchShared& S, int n) {
     __syncthreads();
 }
 
+template <int RC>
 __global__ void __launch_bounds__(kBMaxThreads, 1)
     k_batch_dl(const BatchInst* __restrict__ insts, const int* __restrict__ order, int ninst, int* __restrict__ counter,
                BatchOpts o, double* __restrict__ energies, int* __restrict__ iters, int* __restrict__ conv, int npp_max,
@@ -284,7 +314,7 @@ __global__ void __launch_bounds__(kBMaxThreads, 1)
     double* Vs = reinterpret_cast<double*>(batch_smem + sizeof(BatchShared));
     double* Mas = Vs + (size_t)npp_max * npp_max;
     double* Mbs = Mas + (size_t)npl_max * npl_max;
-    double* Xs = Mbs + (size_t)npl_max * npl_max;
+    unsigned char* Xs = reinterpret_cast<unsigned char*>(Mbs + (size_t)npl_max * npl_max);
     __shared__ double Gkeep[kBMaxSub * kBMaxSub];
     __shared__ int grp[2 * kBMaxG];
     __shared__ BatchInst sP;  // one copy per CTA (a per-thread copy would live in local memory)
@@ -389,11 +419,15 @@ __global__ void __launch_bounds__(kBMaxThreads, 1)
         __syncthreads();
         int it = 0;
         bool done = false;
+        bool fp64_phase = !o.mixed;  // mixed: FP32 sigma first, FP64 sigma from the restart on
         while (it < o.maxiter) {
             const int nb = S.nb;
             // sigma of the new basis vectors and the new columns of G
             for (int j = S.nsig; j < nb; j++) {
-                bsigma(P, Vs, Mas, Mbs, B + (size_t)j * N, Sg + (size_t)j * N, Xs, xcap, grp);
+                if (o.mixed && !fp64_phase)
+                    bsigma<float, RC>(P, Vs, Mas, Mbs, B + (size_t)j * N, Sg + (size_t)j * N, Xs, grp);
+                else
+                    bsigma<double, RC>(P, Vs, Mas, Mbs, B + (size_t)j * N, Sg + (size_t)j * N, Xs, grp);
                 bdots(Sg + (size_t)j * N, B, N, nb, S);
                 for (int i = tid; i < nb; i += nth) {
                     Gkeep[i * kBMaxSub + j] = S.out[i];
@@ -442,9 +476,37 @@ __global__ void __launch_bounds__(kBMaxThreads, 1)
             for (int k = 0; k < nroot; k++)
                 ok = ok && fabs(S.lam[k] - S.lam_old[k]) < o.e_conv && sqrt(S.out[k]) < o.r_conv;
             if ((size_t)nb >= N) ok = true;  // the basis spans the space: the Ritz values are exact
-            if (ok) {
+            if (ok && fp64_phase) {
                 done = true;
                 break;
+            }
+            if (ok) {
+                // mixed: the FP32 iteration has converged; restart from the nroot Ritz vectors and
+                // recompute their sigma in FP64, which alone decides convergence from here on
+                for (size_t I = tid; I < N; I += nth) {
+                    double tb[kBMaxRoot];
+#pragma unroll
+                    for (int k = 0; k < kBMaxRoot; k++) tb[k] = 0.0;
+                    for (int j = 0; j < nb; j++) {
+                        const double bj = B[(size_t)j * N + I];
+#pragma unroll
+                        for (int k = 0; k < kBMaxRoot; k++)
+                            if (k < nroot) tb[k] = fma(S.Ev[j * kBMaxSub + k], bj, tb[k]);
+                    }
+#pragma unroll
+                    for (int k = 0; k < kBMaxRoot; k++)
+                        if (k < nroot) B[(size_t)k * N + I] = tb[k];
+                }
+                __syncthreads();
+                for (int i = tid; i < kBMaxSub * kBMaxSub; i += nth) Gkeep[i] = 0.0;
+                for (int k = tid; k < nroot; k += nth) S.lam_old[k] = S.lam[k];
+                if (tid == 0) {
+                    S.nb = nroot;
+                    S.nsig = 0;
+                }
+                fp64_phase = true;
+                __syncthreads();
+                continue;
             }
             __syncthreads();
             for (int k = tid; k < nroot; k += nth) S.lam_old[k] = S.lam[k];
@@ -565,7 +627,7 @@ struct fcib_batch {
     fcib::DBuf<int> order, counter, iters, conv;
     int npp_max = 0, npl_max = 0, xcap = 0;
     size_t smem = 0;
-    int threads = 512, ctas_per_sm = 1;
+    int threads = 512, ctas_per_sm = 1, pair_tile = 16;
     cudaGraphExec_t graph = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     double last_ms = 0.0;
@@ -588,9 +650,9 @@ static void batch_capture(fcib_batch* b) {
     cudaGraph_t g;
     FCIB_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
     cudaMemsetAsync(b->counter.p, 0, sizeof(int), b->stream);
-    k_batch_dl<<<grid, b->threads, b->smem, b->stream>>>(b->insts.p, b->order.p, b->ninst, b->counter.p, b->opts,
-                                                        b->energies.p, b->iters.p, b->conv.p, b->npp_max, b->npl_max,
-                                                        b->xcap);
+    auto kern = b->pair_tile == 8 ? k_batch_dl<8> : b->pair_tile == 32 ? k_batch_dl<32> : k_batch_dl<16>;
+    kern<<<grid, b->threads, b->smem, b->stream>>>(b->insts.p, b->order.p, b->ninst, b->counter.p, b->opts,
+                                                  b->energies.p, b->iters.p, b->conv.p, b->npp_max, b->npl_max, b->xcap);
     cudaError_t le = cudaGetLastError();
     cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
     FCIB_CUDA(le);
@@ -645,7 +707,8 @@ int fcib_batch_create(fcib_batch** out, int device, int ninst, const int* n, con
         b->ninst = ninst;
         b->nroot = nroot;
         const int msub = std::min(kBMaxSub, opt->subspace_per_root * nroot);
-        b->opts = BatchOpts{nroot, opt->maxiter, opt->e_convergence, opt->r_convergence};
+        b->opts = BatchOpts{nroot, opt->maxiter, opt->e_convergence, opt->r_convergence,
+                            opt->precision != FCIB_PREC_FP64 ? 1 : 0};
         std::vector<BatchInst> hi(ninst);
         std::vector<double> pool;
         std::vector<size_t> off_V(ninst), off_Ma(ninst), off_Mb(ninst), off_dg(ninst);
@@ -695,6 +758,8 @@ int fcib_batch_create(fcib_batch** out, int device, int ninst, const int* n, con
             P.g2la = ta->g2lab.p;
             P.g2rb = tb->g2row.p;
             P.g2lb = tb->g2lab.p;
+            P.tgtb = tb->tgt.p;
+            P.nppb = tb->npair_pad;
             b->tables.push_back(std::move(ta));
             if (tbo) b->tables.push_back(std::move(tbo));
             // integrals: pair matrix with folded one-body terms, same-spin pair matrices, diagonal pieces
@@ -768,14 +833,16 @@ int fcib_batch_create(fcib_batch** out, int device, int ninst, const int* n, con
         const size_t statics = sizeof(double) * kBMaxSub * kBMaxSub + sizeof(int) * 2 * kBMaxG + 1024;
         FCIB_CHECK(fixed + statics + 8 * 2048 <= (size_t)b->smem_optin, FCIB_ERR_UNSUPPORTED,
                    "fcib_batch_create: integral blocks exceed shared memory");
-        // pair-chunk scratch of the opposite-spin term: as much as fits, at most a full row block
+        // sigma scratch: the largest instance's pair block, sigma row and connections
         size_t want = 0;
-        for (const BatchInst& P : hi) want = std::max(want, (size_t)P.npp * P.nbs);
-        b->xcap = (int)std::min(want, ((size_t)b->smem_optin - fixed - statics) / 8);
+        for (const BatchInst& P : hi) want = std::max(want, bsigma_scratch(P.s1a, P.npp, P.nbs));
+        FCIB_CHECK(fixed + statics + want <= (size_t)b->smem_optin, FCIB_ERR_UNSUPPORTED,
+                   "fcib_batch_create: sigma scratch exceeds shared memory");
+        b->xcap = (int)((want + 7) / 8);
         b->smem = fixed + 8 * (size_t)b->xcap;
-        for (const BatchInst& P : hi)
-            FCIB_CHECK(b->xcap >= P.nbs, FCIB_ERR_UNSUPPORTED, "fcib_batch_create: beta strings exceed shared memory");
-        FCIB_CUDA(cudaFuncSetAttribute(k_batch_dl, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
+        FCIB_CUDA(cudaFuncSetAttribute(k_batch_dl<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
+        FCIB_CUDA(cudaFuncSetAttribute(k_batch_dl<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
+        FCIB_CUDA(cudaFuncSetAttribute(k_batch_dl<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
         FCIB_CUDA(cudaStreamSynchronize(b->stream));
     });
     if (rc != FCIB_OK) {
@@ -810,41 +877,50 @@ int fcib_batch_solve(fcib_batch* b, double* energies, int* iterations, int* conv
 // Autotuner: times the whole batch for each launch shape (threads per CTA x CTAs per SM) and keeps
 // the fastest; the choice is re-captured into the solve graph.  shapes_ms[8] (may be NULL)
 // receives the time of each candidate (0 when a shape does not fit).
-int fcib_batch_tune(fcib_batch* b, int* threads, int* ctas_per_sm, double* shapes_ms) {
+int fcib_batch_tune(fcib_batch* b, int* threads, int* ctas_per_sm, int* pair_tile, double* times_ms) {
     if (!b) { fcib::set_error("null batch"); return FCIB_ERR_ARG; }
     return fcib::guarded(nullptr, [&] {
         FCIB_CUDA(cudaSetDevice(b->device));
+        // launch shapes (threads per CTA x CTAs per SM) x opposite-spin sigma tiles (pairs per work item)
         const int cand[4][2] = {{256, 1}, {512, 1}, {256, 2}, {128, 2}};
+        const int tiles[3] = {8, 16, 32};
         double best = 1e300;
-        int bt = b->threads, bc = b->ctas_per_sm;
-        for (int i = 0; i < 4; i++) {
-            if (shapes_ms) shapes_ms[i] = 0.0;
-            int per_sm = 0;
-            FCIB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fcib::k_batch_dl, cand[i][0], b->smem));
-            if (per_sm < cand[i][1]) continue;
-            b->threads = cand[i][0];
-            b->ctas_per_sm = cand[i][1];
-            if (b->graph) {
-                cudaGraphExecDestroy(b->graph);
-                b->graph = nullptr;
-            }
-            fcib::batch_run(b);  // capture + warm
-            const double ms = fcib::batch_run(b);
-            if (shapes_ms) shapes_ms[i] = ms;
-            if (ms < best) {
-                best = ms;
-                bt = cand[i][0];
-                bc = cand[i][1];
+        int bt = b->threads, bc = b->ctas_per_sm, bp = b->pair_tile;
+        for (int ti = 0; ti < 3; ti++) {
+            auto kern = tiles[ti] == 8 ? fcib::k_batch_dl<8> : tiles[ti] == 32 ? fcib::k_batch_dl<32> : fcib::k_batch_dl<16>;
+            for (int i = 0; i < 4; i++) {
+                if (times_ms) times_ms[ti * 4 + i] = 0.0;
+                int per_sm = 0;
+                FCIB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, cand[i][0], b->smem));
+                if (per_sm < cand[i][1]) continue;
+                b->threads = cand[i][0];
+                b->ctas_per_sm = cand[i][1];
+                b->pair_tile = tiles[ti];
+                if (b->graph) {
+                    cudaGraphExecDestroy(b->graph);
+                    b->graph = nullptr;
+                }
+                fcib::batch_run(b);  // capture + warm
+                const double ms = fcib::batch_run(b);
+                if (times_ms) times_ms[ti * 4 + i] = ms;
+                if (ms < best) {
+                    best = ms;
+                    bt = cand[i][0];
+                    bc = cand[i][1];
+                    bp = tiles[ti];
+                }
             }
         }
         b->threads = bt;
         b->ctas_per_sm = bc;
+        b->pair_tile = bp;
         if (b->graph) {
             cudaGraphExecDestroy(b->graph);
             b->graph = nullptr;
         }
         if (threads) *threads = bt;
         if (ctas_per_sm) *ctas_per_sm = bc;
+        if (pair_tile) *pair_tile = bp;
     });
 }
 

@@ -160,7 +160,7 @@ struct Context {
     bool fold_h = true;
     DBuf<uint8_t> mask;   // determinant in target irrep (only when nirrep > 1)
     // work vectors
-    DBuf<double> ct, st;  // transposed C and sigma for beta same-spin terms
+    DBuf<double> ct;      // transposed C for the beta same-spin terms
     DBuf<uint16_t> tgtR16; // beta replacement targets [column/8][string][column%8] for the tensor-core kernel
     DBuf<int> tc_perm;     // pair of each tensor-core column: off-diagonal pairs, then the diagonal ones
     DBuf<float> tf_hi;        // interleaved (tf32 hi, tf32 lo) pairs of the sigma input (mixed path)
@@ -222,9 +222,10 @@ struct Context {
 
 // counter slots: 0 opposite-spin row counter, 1 its timeout flag, 2 CUDA-core group counter,
 // 3 bits of max|C| of the sigma input, 4 tensor-core group counter, 5 its timeout flag,
-// 6 exponent el of the mixed same-spin fixed-point grid 2^-el
+// 6 exponent el of the same-spin fixed-point grid 2^-el, 7 bits of max|C| of an FP64 sigma input
 constexpr int kSlotCmax = 3;
 constexpr int kSlotSameGrid = 6;
+constexpr int kSlotCmax64 = 7;
 // the work counters and error flags of the persistent kernels, zeroed when first allocated
 inline void ensure_counter(Context& c) {
     if (c.counter.p) return;
@@ -237,6 +238,7 @@ void prepare_integrals(Context& c);
 // csf.cu: v <- its projection onto the spin sector of the target multiplicity
 void csf_project(Context& c, double* v);
 void sigma_fp64(Context& c, const double* C, double* S);
+float host_vmax(Context& c);  // max |V| (pair matrix) with a small margin, from a host copy
 void sigma_mixed(Context& c, const double* C, double* S, bool three);
 void apply_mask(Context& c, double* v);
 void export_list(int n, int k, int kind, int p, int q, int r, int s, std::vector<int8_t>& sign,

@@ -113,13 +113,29 @@ __device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
         : "d"(a), "d"(b));
 }
 
+// One FP64 value rounded to the fixed-point grid 2^-el (scale = 2^el) as a two's-complement u64
+__device__ __forceinline__ unsigned long long fixed64d(double v, double scale) {
+    return (unsigned long long)__double2ll_rn(v * scale);
+}
+
+// the FP64 sigma's 62-bit grids from max|C| (bits in *cmax_bits): the opposite-spin row sums are at
+// most |e0| max|C| + s1b kpad max|C| max|V|, so 2^el of that stays below 2^62
+__device__ __forceinline__ int grid_el_fp64(const unsigned int* cmax_bits, double bound_per_c) {
+    const double b = fmax(1.01 * bound_per_c * (double)__uint_as_float(*cmax_bits), 1e-300);
+    return min(1000, (int)floor(62.0 - log2(b)));
+}
+
 __global__ void __launch_bounds__(kDmThreads, 1) k_ab_fp64(
     const double* __restrict__ C, double* __restrict__ S, const uint32_t* __restrict__ connA, int s1a, int kpad,
     const int32_t* __restrict__ tgtB, int npp, int npair, const double* __restrict__ V, int nas, int nbs, double e0,
-    int* __restrict__ row_counter) {
+    int* __restrict__ row_counter, const unsigned int* __restrict__ cmax_bits, double bound_per_c) {
     extern __shared__ __align__(16) unsigned char smem[];
-    double* srow = reinterpret_cast<double*>(smem);
-    double* Bs = srow + ((nbs + 1) & ~1);           // [kpad][kDmLdB]: (k, R) at k*kDmLdB + (R ^ ((k & 1) << 3))
+    // the sigma row in 64-bit fixed point: every product is rounded once to the grid and the integer
+    // sum does not depend on the order of the atomics (a repeated sigma is bit-identical)
+    unsigned long long* srow = reinterpret_cast<unsigned long long*>(smem);
+    const int el = grid_el_fp64(cmax_bits, bound_per_c);
+    const double scale = ldexp(1.0, el), inv_scale = ldexp(1.0, -el);
+    double* Bs = reinterpret_cast<double*>(srow + ((nbs + 1) & ~1));  // [kpad][kDmLdB]: (k, R) at k*kDmLdB + (R ^ ((k & 1) << 3))
     double* As = Bs + (size_t)kpad * kDmLdB;        // [kpad][kDmTM]: (k, Jb) at k*kDmTM + (Jb ^ ((k & 1) << 3))
     uint32_t* cs = reinterpret_cast<uint32_t*>(As + (size_t)kpad * kDmTM);
     __shared__ int s_row;
@@ -139,7 +155,7 @@ __global__ void __launch_bounds__(kDmThreads, 1) k_ab_fp64(
         if (Ia >= nas) break;
         for (int k = tid; k < kpad; k += kDmThreads) cs[k] = k < s1a ? connA[(size_t)Ia * s1a + k] : 0u;
         const double* Crow = C + (size_t)Ia * nbs;
-        for (int j = tid; j < nbs; j += kDmThreads) srow[j] = e0 * Crow[j];
+        for (int j = tid; j < nbs; j += kDmThreads) srow[j] = fixed64d(e0 * Crow[j], scale);
         __syncthreads();
         for (int idx = tid; idx < kpad * kDmLdB; idx += kDmThreads) {
             const int k = idx / kDmLdB, R = idx - k * kDmLdB;
@@ -215,11 +231,11 @@ __global__ void __launch_bounds__(kDmThreads, 1) k_ab_fp64(
                         const int2 tg = *reinterpret_cast<const int2*>(tgtB + (size_t)jb * npp + R);
                         if (tg.x != kNoTarget) {
                             const double v = acc[j][0];
-                            atomicAdd(&srow[tg.x & kConnIdxMask], (tg.x & (int)kSignBit) ? -v : v);
+                            atomicAdd(&srow[tg.x & kConnIdxMask], fixed64d((tg.x & (int)kSignBit) ? -v : v, scale));
                         }
                         if (tg.y != kNoTarget) {
                             const double v = acc[j][1];
-                            atomicAdd(&srow[tg.y & kConnIdxMask], (tg.y & (int)kSignBit) ? -v : v);
+                            atomicAdd(&srow[tg.y & kConnIdxMask], fixed64d((tg.y & (int)kSignBit) ? -v : v, scale));
                         }
                     }
                 }
@@ -227,8 +243,18 @@ __global__ void __launch_bounds__(kDmThreads, 1) k_ab_fp64(
         }
         __syncthreads();
         double* Srow = S + (size_t)Ia * nbs;
-        for (int j = tid; j < nbs; j += kDmThreads) Srow[j] = srow[j];
+        for (int j = tid; j < nbs; j += kDmThreads) Srow[j] = (double)(long long)srow[j] * inv_scale;
     }
+}
+
+// bits of max|C| (rounded up) into *cmax_bits (zeroed before the launch)
+__global__ void k_absmax(const double* __restrict__ C, size_t n, unsigned int* __restrict__ cmax_bits) {
+    float mx = 0.f;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        mx = fmaxf(mx, (float)fabs(C[i]));
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    // non-negative floats order like their bit patterns; two ulps up cover the rounding to float
+    if ((threadIdx.x & 31) == 0) atomicMax(cmax_bits, mx > 0.f ? __float_as_uint(mx) + 2u : 0u);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -248,10 +274,6 @@ constexpr int kGrLoads = 16;  // X elements per thread per item (G*kGrTN/threads
 
 template <typename T>
 struct GroupOut {
-    using type = double;
-};
-template <>
-struct GroupOut<float> {
     using type = unsigned long long;
 };
 
@@ -266,7 +288,7 @@ __global__ void __launch_bounds__(1024) k_group(
     const uint32_t* __restrict__ rows, const uint16_t* __restrict__ labs, int G, int Gp,
     const double* __restrict__ M, int ldm, int ngroups, int nchunks, int* __restrict__ counter, int m_in_smem,
     const int* __restrict__ grid_el) {
-    const float scale = grid_el ? ldexpf(1.0f, *grid_el) : 1.0f;
+    const T scale = (T)ldexp(1.0, *grid_el);
     using T2 = typename std::conditional<std::is_same<T, double>::value, double2, float2>::type;
     extern __shared__ __align__(16) unsigned char smem[];
     T* Ms = reinterpret_cast<T*>(smem);       // [ldm][ldm] when m_in_smem (else M is read from L2)
@@ -363,12 +385,111 @@ __global__ void __launch_bounds__(1024) k_group(
                     const T a0 = (e & kSignBit) ? -acc[i][0] : acc[i][0];
                     const T a1 = (e & kSignBit) ? -acc[i][1] : acc[i][1];
                     if constexpr (std::is_same<T, double>::value) {
-                        if (col < ncols) atomicAdd(dst, a0);
-                        if (col + 1 < ncols) atomicAdd(dst + 1, a1);
+                        if (col < ncols) atomicAdd(dst, fixed64d(a0, scale));
+                        if (col + 1 < ncols) atomicAdd(dst + 1, fixed64d(a1, scale));
                     } else {
                         if (col < ncols) atomicAdd(dst, fixed64(a0, scale));
                         if (col + 1 < ncols) atomicAdd(dst + 1, fixed64(a1, scale));
                     }
+                }
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// FP64 same-spin groups on the FP64 tensor cores (mma.sync m8n8k4 f64).  Persistent CTAs take
+// (group, 128-column chunk) items in chunk-major order like k_group; per item
+//     D[i][col] = sum_j W[i][j] X[j][col],  W[i][j] = M[lab_i][lab_j],  X[j][col] = s_j C[row_j][c0 + col],
+// then s_i D[i][col] is rounded to the sigma's same-spin grid 2^-el and added to S[row_i][c0 + col]
+// (an int64 buffer) with 64-bit integer reductions, so the sum does not depend on the group order.  8 warps: warp w owns columns
+// 16w..16w+15 (two n8 tiles) for all G rows (up to six m8 tiles), so an item is 12 accumulators per
+// warp over K = G padded to 4.  W rows are 52 doubles apart (416 B, 32 B past a multiple of 128) and
+// X columns are XOR-swizzled by the parity of the row, so fragment loads take two wavefronts.
+// ------------------------------------------------------------------------------------------
+constexpr int kGdTN = 128;
+constexpr int kGdThreads = 256;
+constexpr int kGdMaxG = 48;
+constexpr int kGdLdW = 52;
+
+__global__ void __launch_bounds__(kGdThreads) k_group_dmma(
+    const double* __restrict__ C, unsigned long long* __restrict__ S, int ncols, const uint32_t* __restrict__ rows,
+    const uint16_t* __restrict__ labs, int G, const double* __restrict__ M, int ldm, int ngroups, int nchunks,
+    int* __restrict__ counter, const int* __restrict__ grid_el) {
+    const double scale = ldexp(1.0, *grid_el);  // the sigma's same-spin fixed-point grid
+    extern __shared__ __align__(16) unsigned char gd_smem[];
+    double* Ws = reinterpret_cast<double*>(gd_smem);      // W[i][j] at i*kGdLdW + j
+    double* Xs = Ws + kGdMaxG * kGdLdW;                    // X[j][col] at j*kGdTN + (col ^ ((j & 1) << 3))
+    uint32_t* rs = reinterpret_cast<uint32_t*>(Xs + kGdMaxG * kGdTN);
+    uint16_t* ls = reinterpret_cast<uint16_t*>(rs + kGdMaxG);
+    __shared__ int s_item;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int fr = lane >> 2, fk = lane & 3;
+    const int Gp = (G + 7) / 8 * 8;       // rows padded to whole m8 tiles
+    const int Kp = (G + 3) / 4 * 4;       // K padded to whole k4 steps
+    const int nmt = Gp / 8, nks = Kp / 4;
+    const int total = ngroups * nchunks;
+    while (true) {
+        __syncthreads();
+        if (tid == 0) s_item = atomicAdd(counter, 1);
+        __syncthreads();
+        const int item = s_item;
+        if (item >= total) break;
+        const int chunk = item / ngroups, g = item - chunk * ngroups;
+        const int c0 = chunk * kGdTN;
+        for (int i = tid; i < kGdMaxG; i += kGdThreads) {
+            rs[i] = i < G ? rows[(size_t)g * G + i] : 0u;
+            ls[i] = i < G ? labs[(size_t)g * G + i] : (uint16_t)0;
+        }
+        __syncthreads();
+        for (int idx = tid; idx < Gp * Kp; idx += kGdThreads) {
+            const int i = idx / Kp, j = idx - i * Kp;
+            Ws[i * kGdLdW + j] = (i < G && j < G) ? M[(size_t)ls[i] * ldm + ls[j]] : 0.0;
+        }
+        for (int idx = tid; idx < Kp * kGdTN; idx += kGdThreads) {
+            const int j = idx / kGdTN, col = idx - j * kGdTN;
+            double v = 0.0;
+            if (j < G && c0 + col < ncols) {
+                const uint32_t r = rs[j];
+                v = C[(size_t)(r & kConnIdxMask) * ncols + c0 + col];
+                if (r & kSignBit) v = -v;
+            }
+            Xs[j * kGdTN + (col ^ ((j & 1) << 3))] = v;
+        }
+        __syncthreads();
+        double acc[6][2][2];
+#pragma unroll
+        for (int m = 0; m < 6; m++)
+#pragma unroll
+            for (int t = 0; t < 2; t++) acc[m][t][0] = acc[m][t][1] = 0.0;
+        for (int ks = 0; ks < nks; ks++) {
+            const int k = 4 * ks + fk;
+            const int sw = (k & 1) << 3;
+            double b[2];
+#pragma unroll
+            for (int t = 0; t < 2; t++) b[t] = Xs[k * kGdTN + (((2 * warp + t) * 8 + fr) ^ sw)];
+#pragma unroll
+            for (int m = 0; m < 6; m++) {
+                if (m < nmt) {
+                    const double a = Ws[(m * 8 + fr) * kGdLdW + k];
+                    dmma_8x8x4(acc[m][0], a, b[0]);
+                    dmma_8x8x4(acc[m][1], a, b[1]);
+                }
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < 6; m++) {
+            const int i = m * 8 + fr;
+            if (m < nmt && i < G) {
+                const uint32_t r = rs[i];
+                unsigned long long* srow = S + (size_t)(r & kConnIdxMask) * ncols;
+#pragma unroll
+                for (int t = 0; t < 2; t++) {
+                    const int col = c0 + (2 * warp + t) * 8 + 2 * fk;
+                    const double d0 = (r & kSignBit) ? -acc[m][t][0] : acc[m][t][0];
+                    const double d1 = (r & kSignBit) ? -acc[m][t][1] : acc[m][t][1];
+                    if (col < ncols) atomicAdd(srow + col, fixed64d(d0, scale));
+                    if (col + 1 < ncols) atomicAdd(srow + col + 1, fixed64d(d1, scale));
                 }
             }
         }
@@ -401,9 +522,23 @@ static void launch_group_t(Context& c, const T* C, typename GroupOut<T>::type* S
     FCIB_KCHECK();
 }
 
-static void launch_group(Context& c, const double* C, double* S, int ncols, int ngroups, int G,
+static void launch_group(Context& c, const double* C, unsigned long long* S, int ncols, int ngroups, int G,
                          const uint32_t* rows, const uint16_t* labs, const double* M, int ldm) {
-    launch_group_t<double>(c, C, S, ncols, ngroups, G, rows, labs, M, ldm, nullptr);
+    if (ngroups == 0 || G == 0) return;
+    if (G <= kGdMaxG) {
+        // FP64 tensor cores; three CTAs per SM (69 KB of shared memory each)
+        const int nchunks = (ncols + kGdTN - 1) / kGdTN;
+        const int grid = std::min(ngroups * nchunks, 3 * c.num_sms);
+        const size_t smem = sizeof(double) * (kGdMaxG * kGdLdW + kGdMaxG * kGdTN) + kGdMaxG * 6;
+        FCIB_CUDA(cudaFuncSetAttribute(k_group_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        ensure_counter(c);
+        FCIB_CUDA(cudaMemsetAsync(c.counter.p + 2, 0, sizeof(int), c.stream));
+        k_group_dmma<<<grid, kGdThreads, smem, c.stream>>>(C, S, ncols, rows, labs, G, M, ldm, ngroups, nchunks,
+                                                           c.counter.p + 2, c.counter.p + kSlotSameGrid);
+        FCIB_KCHECK();
+        return;
+    }
+    launch_group_t<double>(c, C, S, ncols, ngroups, G, rows, labs, M, ldm, c.counter.p + kSlotSameGrid);
 }
 static void launch_group(Context& c, const float* C, unsigned long long* S, int ncols, int ngroups, int G,
                          const uint32_t* rows, const uint16_t* labs, const double* M, int ldm) {
@@ -426,23 +561,6 @@ __global__ void k_transpose(const double* __restrict__ in, double* __restrict__ 
     for (int j = threadIdx.y; j < 32; j += blockDim.y) {
         int oy = blockIdx.x * 32 + j;
         if (ox < rows && oy < cols) out[(size_t)oy * rows + ox] = tile[threadIdx.x][j];
-    }
-}
-
-// out[r][c] += in[c][r]; in is [cols][rows]
-__global__ void k_transpose_add(const double* __restrict__ in, double* __restrict__ out, int rows, int cols) {
-    __shared__ double tile[32][33];
-    int x = blockIdx.x * 32 + threadIdx.x;  // index into in's columns (= out rows)
-    int y0 = blockIdx.y * 32;               // in's rows (= out cols)
-    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
-        int y = y0 + j;
-        if (x < rows && y < cols) tile[j][threadIdx.x] = in[(size_t)y * rows + x];
-    }
-    __syncthreads();
-    int oc = y0 + threadIdx.x;
-    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
-        int orow = blockIdx.x * 32 + j;
-        if (orow < rows && oc < cols) out[(size_t)orow * cols + oc] += tile[threadIdx.x][j];
     }
 }
 
@@ -520,13 +638,6 @@ static void transpose(Context& c, const double* in, double* out, int rows, int c
     k_transpose<<<grid, block, 0, c.stream>>>(in, out, rows, cols);
     FCIB_KCHECK();
 }
-// out[rows][cols] += transpose(in[cols][rows])
-static void transpose_add(Context& c, const double* in, double* out, int rows, int cols) {
-    dim3 grid((rows + 31) / 32, (cols + 31) / 32), block(32, 8);
-    k_transpose_add<<<grid, block, 0, c.stream>>>(in, out, rows, cols);
-    FCIB_KCHECK();
-}
-
 void apply_mask(Context& c, double* v) {
     if (c.nirrep <= 1 || !c.mask.p) return;
     k_apply_mask<<<4 * c.num_sms, 256, 0, c.stream>>>(v, c.mask.p, (size_t)c.ndet);
@@ -553,24 +664,41 @@ static void sigma_same_spin(Context& c, const double* C, double* S, bool fp32) {
     const size_t N = (size_t)c.ndet;
     const int np2 = c.n * (c.n - 1) / 2;
     const bool a_g1 = !c.fold_h && c.A.ng1, b_g1 = !c.fold_h && c.B.ng1;
-    if (!fp32) {
-        if (a_g1) launch_group(c, C, S, nbs, c.A.ng1, c.A.g1, c.A.g1row.p, c.A.g1lab.p, c.Ha.p, c.n);
-        if (c.A.ng2) launch_group(c, C, S, nbs, c.A.ng2, c.A.g2, c.A.g2row.p, c.A.g2lab.p, c.M2a.p, np2);
-        if (c.B.ng2 || b_g1) {
-            c.ct.alloc(N);
-            c.st.alloc(N);
-            transpose(c, C, c.ct.p, nas, nbs);
-            FCIB_CUDA(cudaMemsetAsync(c.st.p, 0, N * sizeof(double), c.stream));
-            if (b_g1) launch_group(c, c.ct.p, c.st.p, nas, c.B.ng1, c.B.g1, c.B.g1row.p, c.B.g1lab.p, c.Hb.p, c.n);
-            if (c.B.ng2) launch_group(c, c.ct.p, c.st.p, nas, c.B.ng2, c.B.g2, c.B.g2row.p, c.B.g2lab.p, c.M2b.p, np2);
-            transpose_add(c, c.st.p, S, nas, nbs);
-        }
-        return;
-    }
-    // mixed: FP32 copy of C (written by the tensor-core split when it ran), FP32 accumulation
     const bool any_a = a_g1 || c.A.ng2, any_b = b_g1 || c.B.ng2;
     if (!any_a && !any_b) return;
     ensure_counter(c);
+    // both precisions sum the same-spin results in int64 on a per-sigma fixed-point grid (the alpha
+    // part row-major, the beta part transposed) and add them to S at the end
+    auto same_grid = [&](const unsigned int* cmax_bits) {
+        auto kb = [&](const SpinTables& t, bool g1, int ne) {
+            double v = (double)t.ng2 > 0 ? (double)ne * (ne - 1) / 2 * ((t.g2 + 15) / 16 * 16) : 0.0;
+            if (g1 && t.ng1) v += (double)ne * ((t.g1 + 15) / 16 * 16);
+            return v;
+        };
+        const double kbound = std::max(kb(c.A, a_g1, c.na), kb(c.B, b_g1, c.nb));
+        k_same_grid<<<1, 1, 0, c.stream>>>(cmax_bits, (float)(kbound * c.same_mmax), c.counter.p + kSlotSameGrid);
+        FCIB_KCHECK();
+        c.s64a.alloc(N);
+        c.st64.alloc(N);
+        FCIB_CUDA(cudaMemsetAsync(c.s64a.p, 0, N * sizeof(unsigned long long), c.stream));
+        FCIB_CUDA(cudaMemsetAsync(c.st64.p, 0, N * sizeof(unsigned long long), c.stream));
+    };
+    dim3 grid2((nas + 31) / 32, (nbs + 31) / 32), block2(32, 8);
+    if (!fp32) {
+        same_grid(reinterpret_cast<unsigned int*>(c.counter.p + kSlotCmax64));  // max|C| from sigma_fp64
+        if (a_g1) launch_group(c, C, c.s64a.p, nbs, c.A.ng1, c.A.g1, c.A.g1row.p, c.A.g1lab.p, c.Ha.p, c.n);
+        if (c.A.ng2) launch_group(c, C, c.s64a.p, nbs, c.A.ng2, c.A.g2, c.A.g2row.p, c.A.g2lab.p, c.M2a.p, np2);
+        if (any_b) {
+            c.ct.alloc(N);
+            transpose(c, C, c.ct.p, nas, nbs);
+            if (b_g1) launch_group(c, c.ct.p, c.st64.p, nas, c.B.ng1, c.B.g1, c.B.g1row.p, c.B.g1lab.p, c.Hb.p, c.n);
+            if (c.B.ng2) launch_group(c, c.ct.p, c.st64.p, nas, c.B.ng2, c.B.g2, c.B.g2row.p, c.B.g2lab.p, c.M2b.p, np2);
+        }
+        k_add_same_fixed<<<grid2, block2, 0, c.stream>>>(S, c.s64a.p, c.st64.p, nas, nbs, c.counter.p + kSlotSameGrid);
+        FCIB_KCHECK();
+        return;
+    }
+    // mixed: FP32 copy of C (written by the tensor-core split when it ran), FP32 accumulation
     unsigned int* cmax_bits = reinterpret_cast<unsigned int*>(c.counter.p + kSlotCmax);
     if (!c.c32_ready) {
         c.c32.alloc(N);
@@ -580,32 +708,18 @@ static void sigma_same_spin(Context& c, const double* C, double* S, bool fp32) {
     }
     c.c32_ready = false;
     // fixed-point grid from max|C| (just computed on the device) and the host bound kbound * max|M|
-    {
-        auto kb = [&](const SpinTables& t, bool g1, int ne) {
-            double v = (double)t.ng2 > 0 ? (double)ne * (ne - 1) / 2 * ((t.g2 + 15) / 16 * 16) : 0.0;
-            if (g1 && t.ng1) v += (double)ne * ((t.g1 + 15) / 16 * 16);
-            return v;
-        };
-        const double kbound = std::max(kb(c.A, a_g1, c.na), kb(c.B, b_g1, c.nb));
-        k_same_grid<<<1, 1, 0, c.stream>>>(cmax_bits, (float)(kbound * c.same_mmax), c.counter.p + kSlotSameGrid);
-        FCIB_KCHECK();
-    }
+    same_grid(cmax_bits);
     FCIB_CUDA(cudaMemsetAsync(c.counter.p + 5, 0, sizeof(int), c.stream));  // tensor-core group timeout flag
-    c.s64a.alloc(N);
-    c.st64.alloc(N);
-    FCIB_CUDA(cudaMemsetAsync(c.s64a.p, 0, N * sizeof(unsigned long long), c.stream));
-    FCIB_CUDA(cudaMemsetAsync(c.st64.p, 0, N * sizeof(unsigned long long), c.stream));
     if (a_g1) launch_group(c, c.c32.p, c.s64a.p, nbs, c.A.ng1, c.A.g1, c.A.g1row.p, c.A.g1lab.p, c.Ha.p, c.n);
     if (c.A.ng2) launch_group_same_f32(c, c.c32.p, c.s64a.p, nbs, c.A.ng2, c.A.g2, c.A.g2row.p, c.A.g2lab.p, c.M2a.p, np2);
     if (any_b) {
         c.ct32.alloc(N);
-        dim3 grid((nbs + 31) / 32, (nas + 31) / 32), block(32, 8);
-        k_transpose_f32<<<grid, block, 0, c.stream>>>(c.c32.p, c.ct32.p, nas, nbs);
+        dim3 gridt((nbs + 31) / 32, (nas + 31) / 32), blockt(32, 8);
+        k_transpose_f32<<<gridt, blockt, 0, c.stream>>>(c.c32.p, c.ct32.p, nas, nbs);
         FCIB_KCHECK();
         if (b_g1) launch_group(c, c.ct32.p, c.st64.p, nas, c.B.ng1, c.B.g1, c.B.g1row.p, c.B.g1lab.p, c.Hb.p, c.n);
         if (c.B.ng2) launch_group_same_f32(c, c.ct32.p, c.st64.p, nas, c.B.ng2, c.B.g2, c.B.g2row.p, c.B.g2lab.p, c.M2b.p, np2);
     }
-    dim3 grid2((nas + 31) / 32, (nbs + 31) / 32), block2(32, 8);
     k_add_same_fixed<<<grid2, block2, 0, c.stream>>>(S, c.s64a.p, c.st64.p, nas, nbs, c.counter.p + kSlotSameGrid);
     FCIB_KCHECK();
 }
@@ -644,6 +758,11 @@ void sigma_fp64(Context& c, const double* C, double* S) {
     ensure_counter(c);
     SigmaEvents ev;
     FCIB_CUDA(cudaEventRecord(ev.e[0], c.stream));
+    // max|C| for the fixed-point grids of the opposite-spin rows and the same-spin groups
+    unsigned int* cmax64 = reinterpret_cast<unsigned int*>(c.counter.p + kSlotCmax64);
+    FCIB_CUDA(cudaMemsetAsync(cmax64, 0, sizeof(unsigned int), c.stream));
+    k_absmax<<<4 * c.num_sms, 256, 0, c.stream>>>(C, N, cmax64);
+    FCIB_KCHECK();
     if (c.fold_h) {
         const int s1a = c.A.s1, npp = c.A.npair_pad;
         const int kpad = (s1a + 7) / 8 * 8;
@@ -657,8 +776,10 @@ void sigma_fp64(Context& c, const double* C, double* S) {
         per_sm = std::min(per_sm, 2048 / kDmThreads);
         int grid = std::min(nas, per_sm * c.num_sms);
         FCIB_CUDA(cudaMemsetAsync(c.counter.p, 0, sizeof(int), c.stream));
+        if (c.vmax <= 0.0f) c.vmax = host_vmax(c);
+        const double bound = std::fabs(c.scalar) + (double)c.B.s1 * kpad * (double)c.vmax;
         k_ab_fp64<<<grid, kDmThreads, smem, c.stream>>>(C, S, c.A.conn.p, s1a, kpad, c.B.tgt.p, npp, c.A.npair, c.V.p,
-                                                        nas, nbs, c.scalar, c.counter.p);
+                                                        nas, nbs, c.scalar, c.counter.p, cmax64, bound);
         FCIB_KCHECK();
     } else {
         k_scale_copy<<<4 * c.num_sms, 256, 0, c.stream>>>(C, S, c.scalar, N);

@@ -81,7 +81,8 @@ __global__ void __launch_bounds__(kGtThreads, 2)
                const double* __restrict__ M, int ldm, int ngroups, int* __restrict__ counter,
                int* __restrict__ err, const int* __restrict__ grid_el) {
     const float scale = ldexpf(1.0f, *grid_el);  // fixed-point grid 2^-el of this sigma
-    extern __shared__ __align__(128) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char gt_smem[];
+    unsigned char* smem = gt_smem;
     const GtLayout L = gt_layout(G);
     unsigned char* Bhi = smem + L.off_bhi;
     unsigned char* Blo = smem + L.off_blo;
@@ -171,15 +172,12 @@ __global__ void __launch_bounds__(kGtThreads, 2)
         prefetch(0);
         for (int t = 0; t <= ntiles; t++) {
             const int cur = t & 1, prv = cur ^ 1;
-            // (a) the TMEM X buffer is free once the previous tile's MMAs completed (one waiter)
-            if (t >= 1 && tid == 0) {
-                if (!mbar_wait_bounded(&bars[prv], (mma_count[prv] - 1) & 1)) {
-                    atomicCAS(err, 0, kErrTimeoutGroupMma);
-                    s_abort = 1;
-                }
+            // (a) the TMEM X buffer and accumulator prv are ready once the previous tile's MMAs
+            // completed; every thread waits on the barrier itself (no block barrier here)
+            if (t >= 1 && !mbar_wait_bounded(&bars[prv], (mma_count[prv] - 1) & 1)) {
+                atomicCAS(err, 0, kErrTimeoutGroupMma);
+                s_abort = 1;
             }
-            __syncthreads();
-            if (s_abort) break;
             tc_fence_after();
             // (b) registers -> X hi/lo in tensor memory
             if (t < ntiles) {
@@ -199,6 +197,7 @@ __global__ void __launch_bounds__(kGtThreads, 2)
             }
             tc_fence_before();
             __syncthreads();
+            if (s_abort) break;
             tc_fence_after();
             // (c) one thread issues the tile's MMAs into accumulator `cur`
             if (t < ntiles && tid == 0) {

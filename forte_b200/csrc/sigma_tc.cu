@@ -150,14 +150,28 @@ __device__ __forceinline__ uint32_t kmaj_off(int row, int k, int rows) {
 __device__ __forceinline__ void red_add_u32(uint32_t saddr, uint32_t v) {
     asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(saddr), "r"(v));
 }
-// both words of one fixed-point contribution (the low word kAccLoOff bytes above the high word),
-// predicated on the 16-bit target entry g holding a target (g != 0xFFFF): no branch, so the slots of
-// a chunk form straight-line code the compiler can interleave
-__device__ __forceinline__ void red_pair_if(uint32_t saddr, uint32_t hi, uint32_t lo, uint32_t g) {
-    asm volatile(
-        "{\n .reg .pred p;\n setp.ne.u32 p, %3, 65535;\n"
-        " @p red.shared.add.u32 [%0], %1;\n @p red.shared.add.u32 [%0+65536], %2;\n}\n" ::"r"(saddr),
-        "r"(hi), "r"(lo), "r"(g));
+// both words of one fixed-point contribution (the low word kAccLoOff bytes above the high word), for
+// target entries g that hold a target (g != 0xFFFF)
+__device__ __forceinline__ void red_pair(uint32_t saddr, uint32_t hi, uint32_t lo, uint32_t g) {
+    if (g != 0xFFFFu) {
+        asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(saddr), "r"(hi));
+        asm volatile("red.shared.add.u32 [%0+65536], %1;" ::"r"(saddr), "r"(lo));
+    }
+}
+
+// Two fixed-point splits at once with the paired FP32 instructions of sm_100 (f32x2): for each y
+// (|y| < 2^44, the grid already folded in), hi = round(y 2^-22) as the bits of 1.5 * 2^23 + hi and
+// lo = y - hi 2^22 (exact) as the bits of 1.5 * 2^23 + round(lo)
+__device__ __forceinline__ void split_fixed2(float y0, float y1, uint32_t& h0, uint32_t& h1, uint32_t& l0,
+                                             uint32_t& l1) {
+    asm("{\n .reg .b64 y, t, h, l;\n mov.b64 y, {%4, %5};\n"
+        " fma.rn.f32x2 t, y, %6, %7;\n sub.rn.f32x2 h, t, %7;\n"
+        " fma.rn.f32x2 l, h, %8, y;\n add.rn.f32x2 l, l, %7;\n"
+        " mov.b64 {%0, %1}, t;\n mov.b64 {%2, %3}, l;\n}"
+        : "=r"(h0), "=r"(h1), "=r"(l0), "=r"(l1)
+        : "f"(y0), "f"(y1), "l"(0x3480000034800000ull),  // (2^-22, 2^-22)
+          "l"(0x4B4000004B400000ull),                     // (1.5 * 2^23, 1.5 * 2^23)
+          "l"(0xCA800000CA800000ull));                    // (-2^22, -2^22)
 }
 
 __device__ __forceinline__ void mma_tf32_ta(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc, uint32_t idesc,
@@ -210,7 +224,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             int npair, const int* __restrict__ perm, int noff8, int n, const uint32_t* __restrict__ bstr, int kb,
             const double* __restrict__ V, int ldv, float vmax, const unsigned int* __restrict__ cmax_bits,
             int nas, int nbs, int ncontrib, double e0, int* __restrict__ row_counter, int* __restrict__ err) {
-    extern __shared__ __align__(1024) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char tc_smem[];
+    unsigned char* smem = tc_smem;
     const TcLayout L = tc_layout(s1a, npair, nbs, THREE);
     unsigned char* Bhi = smem + L.off_bhi;
     unsigned char* Blo = smem + L.off_blo;
@@ -396,15 +411,19 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 auto add_fixed = [&](float ys, uint32_t a, uint32_t g) {
                     const float t1 = fmaf(ys, 2.38418579e-7f, kMagic);
                     const float lf = fmaf(t1 - kMagic, -4194304.0f, ys);
-                    red_pair_if(a, __float_as_uint(t1), __float_as_uint(lf + kMagic), g);
+                    red_pair(a, __float_as_uint(t1), __float_as_uint(lf + kMagic), g);
                 };
                 auto scatter = [&](const uint32_t (&rv)[8], const uint4& tw) {
                     const uint32_t w[4] = {tw.x, tw.y, tw.z, tw.w};
 #pragma unroll
-                    for (int u = 0; u < 8; u++) {
-                        // entry = Ib * 4 | sign (bit 0); 0xFFFF = no target
-                        const uint32_t g = (u & 1) ? (w[u >> 1] >> 16) : (w[u >> 1] & 0xFFFFu);
-                        add_fixed(__uint_as_float(rv[u] ^ (g << 31)), acc_s + (g & 0xFFFCu), g);
+                    for (int j = 0; j < 4; j++) {
+                        // two slots per 32-bit word; entry = Ib * 4 | sign (bit 0), 0xFFFF = no target
+                        const uint32_t g0 = w[j] & 0xFFFFu, g1 = w[j] >> 16;
+                        uint32_t h0, h1, l0, l1;
+                        split_fixed2(__uint_as_float(rv[2 * j] ^ (g0 << 31)), __uint_as_float(rv[2 * j + 1] ^ (g1 << 31)),
+                                     h0, h1, l0, l1);
+                        red_pair(acc_s + (g0 & 0xFFFCu), h0, l0, g0);
+                        red_pair(acc_s + (g1 & 0xFFFCu), h1, l1, g1);
                     }
                 };
                 uint4 tg2 = load_tg(3);
@@ -516,9 +535,17 @@ __global__ void k_split_tf32(const double* __restrict__ C, float2* __restrict__ 
 
 size_t tc_smem_bytes(int s1a, int npair, int nbs, bool three) { return tc_layout(s1a, npair, nbs, three).total; }
 
+float host_vmax(Context& c) {
+    std::vector<double> hv(c.V.n);
+    FCIB_CUDA(cudaMemcpy(hv.data(), c.V.p, sizeof(double) * c.V.n, cudaMemcpyDeviceToHost));
+    double m = 0.0;
+    for (double x : hv) m = std::max(m, std::fabs(x));
+    return (float)(m * (1.0 + 1e-6)) + 1e-30f;
+}
+
 void ab_tc(Context& c, const double* C, double* S, bool three) {
     const int nas = (int)c.nas, nbs = (int)c.nbs;
-    const int s1a = c.A.s1, npair = c.A.npair;
+    const int s1a = c.A.s1;
     FCIB_CHECK(nbs <= kMaxBetaStrings, FCIB_ERR_UNSUPPORTED, "tensor-core opposite-spin kernel: too many beta strings");
     // columns: the n(n-1)/2 off-diagonal pairs in pair order (padded to a multiple of 8), then the n
     // diagonal pairs (r,r)
@@ -546,13 +573,7 @@ void ab_tc(Context& c, const double* C, double* S, bool three) {
                                                           c.tc_perm.p, noff8, L.npad);
         FCIB_KCHECK();
     }
-    if (c.vmax <= 0.0f) {
-        std::vector<double> hv(c.V.n);
-        FCIB_CUDA(cudaMemcpy(hv.data(), c.V.p, sizeof(double) * c.V.n, cudaMemcpyDeviceToHost));
-        double m = 0.0;
-        for (double x : hv) m = std::max(m, std::fabs(x));
-        c.vmax = (float)(m * (1.0 + 1e-6)) + 1e-30f;
-    }
+    if (c.vmax <= 0.0f) c.vmax = host_vmax(c);
     c.tf_hi.alloc(2 * (size_t)nas * ldp);  // interleaved hi/lo pairs
     ensure_counter(c);
     FCIB_CUDA(cudaMemsetAsync(c.counter.p, 0, 3 * sizeof(int), c.stream));

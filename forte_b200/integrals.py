@@ -49,13 +49,17 @@ def from_chemist(h: np.ndarray, eri: np.ndarray, scalar: float = 0.0, orbsym=Non
                                 list(orbsym) if orbsym is not None else [0] * n)
 
 
-def synthetic(n: int, L: int, seed: int, gap: float = 0.0) -> ActiveSpaceIntegrals:
+def synthetic(n: int, L: int, seed: int, gap: float = 0.0, orbsym=None) -> ActiveSpaceIntegrals:
     """Seeded synthetic integrals.
 
     h: symmetric, diagonal ~ U[-2, +1] Eh, off-diagonal ~ N(0, 0.1).
     (pq|rs) = sum_L B^L_pq B^L_rs with symmetric B^L ~ N(0, 0.15): 8-fold symmetric, PSD.
     ``gap`` > 0: the diagonal of h is sorted ascending and ``gap`` is added to h_pp for
     p >= n/2, opening a gap between orbitals n/2-1 and n/2.  Generator: numpy PCG64(seed).
+    ``orbsym`` (irreps of an abelian point group, XOR products): h_pq is kept only when p and q
+    share an irrep, and each B^L carries an irrep g_L = L mod 8 and keeps B^L_pq only when
+    orbsym[p] ^ orbsym[q] = g_L, so (pq|rs) vanishes unless the four irreps multiply to the
+    totally symmetric one; the draws are the same as without symmetry.
     """
     rng = np.random.Generator(np.random.PCG64(seed))
     h = rng.normal(0.0, 0.1, size=(n, n))
@@ -69,8 +73,14 @@ def synthetic(n: int, L: int, seed: int, gap: float = 0.0) -> ActiveSpaceIntegra
     B = rng.normal(0.0, 0.15, size=(L, n, n))
     B = np.triu(B)
     B = B + np.transpose(np.triu(B, 1), (0, 2, 1))
+    if orbsym is not None:
+        sym = np.asarray(orbsym, dtype=np.int64)
+        pair = sym[:, None] ^ sym[None, :]
+        h = np.where(pair == 0, h, 0.0)
+        for l in range(L):
+            B[l] = np.where(pair == (l % 8), B[l], 0.0)
     eri = np.einsum("lpq,lrs->pqrs", B, B)
-    return from_chemist(h, eri, 0.0)
+    return from_chemist(h, eri, 0.0, orbsym)
 
 
 def read_fcidump(path: str) -> dict:

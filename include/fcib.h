@@ -199,10 +199,12 @@ int fcib_captured_residual(fcib_ctx* ctx, int index, double* r, double* lambda, 
 /* ---- batched solver (no counterpart in the reference) ------------------------------------
  * Many independent CAS instances (2..12 orbitals, >= 1 electron of each spin, C1, no spin
  * selection) solved in one persistent launch: one CTA per instance at a time, largest first,
- * every Davidson-Liu iteration on the device in FP64.  Per instance: n, na, nb, scalar and the
- * integral arrays in the layouts of fcib_set_integrals.  Options used: maxiter, e_convergence,
- * r_convergence, subspace_per_root, collapse_per_root.  The launch is captured in a CUDA graph
- * on the first solve and replayed. */
+ * every Davidson-Liu iteration on the device.  Per instance: n, na, nb, scalar and the integral
+ * arrays in the layouts of fcib_set_integrals.  Options used: maxiter, e_convergence,
+ * r_convergence, subspace_per_root, collapse_per_root, precision (FCIB_PREC_FP64: FP64 sigma;
+ * otherwise FP32 sigma with FP64 subspace, residuals and vectors until converged, then a restart
+ * from the Ritz vectors with FP64 sigma, which alone decides convergence).  The launch is captured
+ * in a CUDA graph on the first solve and replayed. */
 typedef struct fcib_batch fcib_batch;
 int fcib_batch_create(fcib_batch** batch, int device, int ninst, const int* n, const int* na, const int* nb,
                       const double* scalar, const double* const* oei_a, const double* const* oei_b,
@@ -212,9 +214,10 @@ int fcib_batch_destroy(fcib_batch* batch);
 /* energies[ninst * nroot] (instance-major), iterations[ninst], converged[ninst], device_ms = device
  * time of the launch; any output may be NULL */
 int fcib_batch_solve(fcib_batch* batch, double* energies, int* iterations, int* converged, double* device_ms);
-/* autotuner: times the whole batch for each launch shape (threads per CTA x CTAs per SM: 256x1,
- * 512x1, 256x2, 128x2), keeps the fastest for later solves; shapes_ms[4] may be NULL */
-int fcib_batch_tune(fcib_batch* batch, int* threads, int* ctas_per_sm, double* shapes_ms);
+/* autotuner: times the whole batch for each opposite-spin sigma tile (8, 16 or 32 pairs per work item)
+ * and launch shape (threads per CTA x CTAs per SM: 256x1, 512x1, 256x2, 128x2), keeps the fastest
+ * for later solves; times_ms[12] (tile-major, 0 for shapes that do not fit) may be NULL */
+int fcib_batch_tune(fcib_batch* batch, int* threads, int* ctas_per_sm, int* pair_tile, double* times_ms);
 
 /* String tables for parity checks.  spin 0 = alpha, 1 = beta. */
 int fcib_num_strings(fcib_ctx* ctx, int spin, int64_t* count);

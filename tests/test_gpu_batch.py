@@ -50,8 +50,8 @@ def test_batch_autotuner_keeps_a_valid_shape():
     b = BatchSolver(inst, nroot=4, options=OPTS)
     e0, _, cv0, _ = b.solve()
     t = b.tune()
-    assert t["threads"] in (128, 256, 512) and t["ctas_per_sm"] in (1, 2)
-    assert any(v > 0 for v in t["shapes_ms"].values())
+    assert t["threads"] in (128, 256, 512) and t["ctas_per_sm"] in (1, 2) and t["pair_tile"] in (8, 16, 32)
+    assert any(v > 0 for v in t["times_ms"].values())
     e1, _, cv1, _ = b.solve()
     assert cv0.all() and cv1.all() and np.max(np.abs(e1 - e0)) < 1e-8
 
@@ -61,3 +61,21 @@ def test_batch_rejects_unsupported_instances():
         BatchSolver([(synthetic(13, 39, 1), 6, 6)], nroot=2, options=OPTS)
     with pytest.raises(RuntimeError):
         BatchSolver([(synthetic(6, 18, 1), 3, 0)], nroot=2, options=OPTS)
+
+
+@pytest.mark.parametrize("tile_seed", [0, 1])
+def test_batch_mixed_precision_matches_fp64(tile_seed):
+    """FP32 sigma with FP64 subspace and residuals, then the FP64 restart: the energies agree with the
+    FP64 batch and with the single-instance FP64 solver at the mixed tolerance (1e-8 Eh)."""
+    inst = _instances([6, 8, 7, 10, 9, 6, 8, 10], 300 + 17 * tile_seed)
+    f = BatchSolver(inst, nroot=4, options=dict(OPTS, FCI_PRECISION="FP64"))
+    m = BatchSolver(inst, nroot=4, options=dict(OPTS, FCI_PRECISION="MIXED"))
+    ef, _, cf, _ = f.solve()
+    em, itm, cm, _ = m.solve()
+    assert cf.all() and cm.all(), itm
+    assert np.max(np.abs(em - ef)) < 1e-8
+    for i in (0, 3):
+        ints, na, nb = inst[i]
+        s = FCISolver(StateInfo(na, nb, 0), 4, ints, dict(OPTS, E_CONVERGENCE=1e-12, R_CONVERGENCE=1e-8))
+        s.compute_energy()
+        assert np.max(np.abs(em[i] - np.array(s.energies()))) < 1e-8

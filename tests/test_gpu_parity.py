@@ -195,3 +195,31 @@ def test_max_abs_elements_reference_order(case, capfd):
             a, v, h, ia, ib = got[t]
             assert a == abs(c[i]) and v == c[i]
             assert (h, ia, ib) == addr[i]
+
+
+@pytest.mark.parametrize("n,na,nb", [(10, 5, 5), (9, 5, 3), (12, 6, 6), (6, 3, 0)])
+def test_fp64_sigma_is_deterministic(n, na, nb):
+    """The FP64 sigma sums in 64-bit fixed point (opposite-spin rows in shared memory, same-spin groups
+    in global memory) on grids set from max|C|, so repeated builds of one vector are bit-identical."""
+    ints = synthetic(n, 3 * n, 9)
+    s = FCISolver(StateInfo(na, nb, 0, na - nb), 1, ints)
+    rng = np.random.default_rng(n + 3 * na + nb)
+    c = rng.normal(size=s.size())
+    c /= np.linalg.norm(c)
+    first = s.sigma(c)
+    for _ in range(3):
+        assert np.array_equal(s.sigma(c), first)
+
+
+@pytest.mark.parametrize("prec", ["FP64", "MIXED"])
+def test_solves_repeat_exactly(prec):
+    """With every sigma summed in integers, a repeated Davidson solve from a fresh guess takes the
+    same iterations to the same energies, bit for bit."""
+    ints = synthetic(12, 36, 4)
+    s = FCISolver(StateInfo(6, 6, 0), 2, ints, {"FCI_PRECISION": prec, "E_CONVERGENCE": 1e-10,
+                                                 "R_CONVERGENCE": 1e-6, "DL_MAXITER": 300})
+    s.compute_energy()
+    e1, it1 = list(s.energies()), s.iterations()
+    s.reset_guess()
+    s.compute_energy()
+    assert s.iterations() == it1 and list(s.energies()) == e1
