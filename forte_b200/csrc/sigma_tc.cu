@@ -28,7 +28,7 @@
 namespace fcib {
 
 constexpr int kTcM = 128;          // beta rows per tile (MMA M)
-constexpr int kTcThreads = 512;    // 16 warps: all copy A, thread 0 issues MMAs, all scatter
+constexpr int kTcWarps = 16;       // warps of the opposite-spin kernel: all gather, one thread issues MMAs, all scatter
 constexpr uint32_t kTmemCols = 512;
 constexpr long long kWaitLimit = 1ll << 24;
 
@@ -196,11 +196,6 @@ constexpr int kErrTimeoutMma = 1;
 
 // TMEM columns: accumulators at 0 and 256 (npad <= 144), A hi at 160, A lo at 416 (kpad <= 72)
 constexpr uint32_t kColAccStride = 256, kColAhi = 160, kColAlo = 416;
-// Column groups cg = warp / 4.  Gather: A chunks c8 = cg and cg + 4, then chunk 8 + (3 - cg).
-// Epilogue: off-diagonal accumulator chunks c8 = (3 - cg) + 4 i; the diagonal-pair chunks (the
-// last ones) go to cg 0, which has one off-diagonal chunk fewer at n = 16 (15 chunks).
-constexpr int kTcGat = 3;    // 8-column A chunks per warp per tile
-constexpr int kTcEpiC = 4;   // off-diagonal accumulator chunks per warp
 constexpr int kTcMmaThread = 5 * 32;  // issues the MMAs (warp 5: two gather chunks, four epilogue chunks)
 constexpr int kFixLoBits = 22;
 constexpr float kMagic = 12582912.0f;       // 1.5 * 2^23: x + kMagic rounds |x| < 2^22 to an integer
@@ -217,8 +212,17 @@ constexpr int kMagicBits = 0x4B400000;      // bit pattern of kMagic
 // Plane rows are padded to whole tiles (zeros) and the target table to whole tiles (no target), so
 // neither the gather nor the scatter checks bounds.  Per tile: one mbarrier wait and one block
 // barrier.
-template <bool THREE>
-__global__ void __launch_bounds__(kTcThreads, 1)
+// NW warps: NW / 4 column groups per TMEM lane quarter.  Gather chunks of column group cg: cg + NCG j
+// (at 16 warps the third round goes to group 3 - cg, which holds one epilogue chunk fewer);
+// off-diagonal epilogue chunks: (NCG - 1 - cg) + NCG i; the diagonal chunks go to group 0.
+template <int NW>
+__device__ __forceinline__ int tc_gather_chunk(int cg, int j) {
+    constexpr int NCG = NW / 4;
+    return (NCG == 4 && j == 2) ? 8 + (3 - cg) : cg + NCG * j;
+}
+
+template <bool THREE, int NW>
+__global__ void __launch_bounds__(NW * 32, 1)
     k_ab_tc(const float2* __restrict__ Phl, int ldp, const double* __restrict__ C,
             double* __restrict__ S, const uint32_t* __restrict__ connA, int s1a, const uint16_t* __restrict__ tgtR,
             int npair, const int* __restrict__ perm, int noff8, int n, const uint32_t* __restrict__ bstr, int kb,
@@ -242,6 +246,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const int warp = tid >> 5, lane = tid & 31;
     const int kpad = L.kpad, npad = L.npad;
     const int q = warp & 3, cg = warp >> 2;  // TMEM lane quarter and column group of this warp
+    constexpr int NCG = NW / 4;
+    constexpr int GJ = (9 + NCG - 1) / NCG;        // gather chunks per warp (kpad <= 72)
+    constexpr int EI = (15 + NCG - 1) / NCG;       // off-diagonal epilogue chunks per warp (n <= 16)
+    constexpr int EB = EI < 3 ? EI : 3;            // chunks of the first epilogue batch
+    const int ec0 = NCG - 1 - cg;                  // first epilogue chunk of this warp
 
     if (tid == 0) {
         mbar_init(&bars[0], 1);
@@ -285,14 +294,14 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const int ndc = (n + 7) / 8;      // accumulator chunks of the diagonal pairs (r,r), after them
     const unsigned char* pbase = reinterpret_cast<const unsigned char*>(Phl);
 
-    float gh[kTcGat][8], gl[kTcGat][8];
+    float gh[GJ][8], gl[GJ][8];
     // A-tile gather: the thread owning tile row m = 32q + lane loads A[m][k] = plane[J_k][jb0 + m] for
     // the 8-column chunks c8 = cg + 4j (coalesced across lanes)
     auto gather = [&](int tt) {
         const unsigned char* pj = pbase + (size_t)(tt * kTcM + 32 * q + lane) * sizeof(float2);
 #pragma unroll
-        for (int j = 0; j < kTcGat; j++) {
-            const int c8 = j < 2 ? cg + 4 * j : 8 + (3 - cg);
+        for (int j = 0; j < GJ; j++) {
+            const int c8 = tc_gather_chunk<NW>(cg, j);
             if (c8 < nk8) {
                 const uint4 o0 = *reinterpret_cast<const uint4*>(koff + 8 * c8);
                 const uint4 o1 = *reinterpret_cast<const uint4*>(koff + 8 * c8 + 4);
@@ -347,14 +356,14 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             // pairs past npair hold no target
             const int jb_epi = (t - 1) * kTcM + 32 * q + lane;
             auto load_tg = [&](int i) {
-                const int c8 = (3 - cg) + 4 * i;
+                const int c8 = ec0 + NCG * i;
                 return (t >= 1 && c8 < nn8)
                            ? __ldg(reinterpret_cast<const uint4*>(tgtR + ((size_t)c8 * ntiles * kTcM + jb_epi) * 8))
                            : make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
             };
-            uint4 tg[3];
+            uint4 tg[EB];
 #pragma unroll
-            for (int i = 0; i < 3; i++) tg[i] = load_tg(i);
+            for (int i = 0; i < EB; i++) tg[i] = load_tg(i);
             const uint32_t occ_epi = (cg == 0 && t >= 1 && jb_epi < nbs) ? __ldg(bstr + jb_epi) : 0u;
             // (a) the TMEM A buffer and accumulator prv are ready once tile t-1's MMAs completed
             if (t >= 1 && !mbar_wait_bounded(&bars[prv], (mma_count[prv] - 1) & 1)) {
@@ -365,8 +374,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             // (b) registers -> A in tensor memory
             if (t < ntiles) {
 #pragma unroll
-                for (int j = 0; j < kTcGat; j++) {
-                    const int c8 = j < 2 ? cg + 4 * j : 8 + (3 - cg);
+                for (int j = 0; j < GJ; j++) {
+                    const int c8 = tc_gather_chunk<NW>(cg, j);
                     if (c8 < nk8) {
                         tmem_st8(tmem_base + tlane + kColAhi + 8 * c8, gh[j]);
                         if (THREE) tmem_st8(tmem_base + tlane + kColAlo + 8 * c8, gl[j]);
@@ -426,24 +435,24 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                         red_pair(acc_s + (g1 & 0xFFFCu), h1, l1, g1);
                     }
                 };
-                uint4 tg2 = load_tg(3);
+                uint4 tg2 = load_tg(EB);
                 {
-                    uint32_t rv[3][8];
+                    uint32_t rv[EB][8];
 #pragma unroll
-                    for (int i = 0; i < 3; i++) {
-                        const int c8 = (3 - cg) + 4 * i;
+                    for (int i = 0; i < EB; i++) {
+                        const int c8 = ec0 + NCG * i;
                         if (c8 < nn8) tmem_ld8_async(tbase + (uint32_t)(c8 * 8), rv[i]);
                     }
                     tmem_wait_ld8(rv[0]);
-                    reg_after(rv[1]);
-                    reg_after(rv[2]);
 #pragma unroll
-                    for (int i = 0; i < 3; i++)
-                        if ((3 - cg) + 4 * i < nn8) scatter(rv[i], tg[i]);
+                    for (int i = 1; i < EB; i++) reg_after(rv[i]);
+#pragma unroll
+                    for (int i = 0; i < EB; i++)
+                        if (ec0 + NCG * i < nn8) scatter(rv[i], tg[i]);
                 }
-                if ((3 - cg) + 12 < nn8) {
+                if (EB < EI && ec0 + NCG * EB < nn8) {
                     uint32_t rv[8];
-                    tmem_ld8_async(tbase + (uint32_t)(((3 - cg) + 12) * 8), rv);
+                    tmem_ld8_async(tbase + (uint32_t)((ec0 + NCG * EB) * 8), rv);
                     tmem_wait_ld8(rv);
                     scatter(rv, tg2);
                 }
@@ -553,7 +562,7 @@ void ab_tc(Context& c, const double* C, double* S, bool three) {
     const int noff = n * (n - 1) / 2, noff8 = (noff + 7) / 8 * 8;
     const int ncol = noff8 + n;
     TcLayout L = tc_layout(s1a, ncol, nbs, three);
-    FCIB_CHECK(L.npad <= 144 && L.kpad <= 72 && noff8 / 8 <= 4 * kTcEpiC - 1 && n <= 16 && L.kpad / 8 <= 9,
+    FCIB_CHECK(L.npad <= 144 && L.kpad <= 72 && noff8 / 8 <= 15 && n <= 16 && L.kpad / 8 <= 9,
                FCIB_ERR_UNSUPPORTED, "tensor-core kernel: more than 16 active orbitals");
     const int ntiles = (nbs + kTcM - 1) / kTcM;
     const int ldp = ntiles * kTcM;  // plane rows padded to whole tiles (zeros)
@@ -584,13 +593,13 @@ void ab_tc(Context& c, const double* C, double* S, bool three) {
     k_split_tf32<<<8 * c.num_sms, 256, 0, c.stream>>>(C, hl, c.c32.p, nas, nbs, ldp, cmax_bits);
     FCIB_KCHECK();
     c.c32_ready = true;
-    auto kern = three ? k_ab_tc<true> : k_ab_tc<false>;
+    auto kern = three ? k_ab_tc<true, kTcWarps> : k_ab_tc<false, kTcWarps>;
     FCIB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int grid = std::min(nas, c.num_sms);
     c.tc_ev.ensure();
     FCIB_CUDA(cudaEventRecord(c.tc_ev.e[0], c.stream));
     const int kb = c.nb;
-    kern<<<grid, kTcThreads, smem, c.stream>>>(hl, ldp, C, S, c.A.conn.p, s1a, c.tgtR16.p, ncol, c.tc_perm.p, noff8,
+    kern<<<grid, kTcWarps * 32, smem, c.stream>>>(hl, ldp, C, S, c.A.conn.p, s1a, c.tgtR16.p, ncol, c.tc_perm.p, noff8,
                                               n, c.B.str.p, kb, c.V.p, c.A.npair_pad, c.vmax, cmax_bits, nas, nbs,
                                               kb * (n - kb) + 1, c.scalar, c.counter.p, c.counter.p + 1);
     FCIB_KCHECK();
