@@ -48,6 +48,7 @@ class FcibOptions(C.Structure):
         ("mixed_switch", C.c_double),
         ("same_spin_kernel", C.c_int),
         ("spin_adapt", C.c_int),
+        ("sym_blocked", C.c_int),
     ]
 
 

@@ -33,7 +33,7 @@ static int guarded(fcib_ctx* ctx, F&& f) {
 
 static void build_mask_and_maps(Context& c) {
     c.block_to_c1.clear();
-    if (c.nirrep <= 1) {
+    if (c.nirrep <= 1 || c.sym.on) {  // C1, or the blocked layout (its vectors are in flat order)
         c.mask.release();
         return;
     }
@@ -80,8 +80,9 @@ void ensure_setup(Context& c) {
     c.ndet = c.nas * c.nbs;
     FCIB_CUDA(cudaStreamSynchronize(c.stream));
     prepare_integrals(c);
+    build_sym_space(c);
     build_mask_and_maps(c);
-    c.hdiag.alloc((size_t)c.ndet);
+    c.hdiag.alloc((size_t)c.nvec);
     compute_hdiag(c, c.hdiag.p);
     FCIB_CUDA(cudaStreamSynchronize(c.stream));
     c.tables_ready = true;
@@ -94,10 +95,10 @@ void sigma_dispatch(Context& c, const double* b, double* s, int precision) {
     else throw Error{FCIB_ERR_ARG, "unknown sigma precision"};
 }
 
-// host flat (FCIVector order) <-> device C1 layout
+// host flat (FCIVector order) <-> device layout (C1, flat order itself when blocked, or C1 with a mask)
 static void upload_flat(Context& c, const double* flat, double* dev) {
-    if (c.nirrep <= 1) {
-        FCIB_CUDA(cudaMemcpyAsync(dev, flat, sizeof(double) * c.ndet, cudaMemcpyHostToDevice, c.stream));
+    if (c.nirrep <= 1 || c.sym.on) {
+        FCIB_CUDA(cudaMemcpyAsync(dev, flat, sizeof(double) * c.nvec, cudaMemcpyHostToDevice, c.stream));
         return;
     }
     std::vector<double> full((size_t)c.ndet, 0.0);
@@ -106,8 +107,8 @@ static void upload_flat(Context& c, const double* flat, double* dev) {
     FCIB_CUDA(cudaStreamSynchronize(c.stream));
 }
 static void download_flat(Context& c, const double* dev, double* flat) {
-    if (c.nirrep <= 1) {
-        FCIB_CUDA(cudaMemcpyAsync(flat, dev, sizeof(double) * c.ndet, cudaMemcpyDeviceToHost, c.stream));
+    if (c.nirrep <= 1 || c.sym.on) {
+        FCIB_CUDA(cudaMemcpyAsync(flat, dev, sizeof(double) * c.nvec, cudaMemcpyDeviceToHost, c.stream));
         FCIB_CUDA(cudaStreamSynchronize(c.stream));
         return;
     }
@@ -147,7 +148,7 @@ static void rdms_to_outputs(const RdmBlocks& b, int level, int spin_free, double
     (void)n4;
 }
 static int64_t flat_size(const Context& c) {
-    return c.nirrep <= 1 ? c.ndet : (int64_t)c.block_to_c1.size();
+    return (c.nirrep <= 1 || c.sym.on) ? c.nvec : (int64_t)c.block_to_c1.size();
 }
 
 }  // namespace fcib
@@ -172,6 +173,7 @@ void fcib_default_options(fcib_options* o) {
     o->mixed_switch = 1.0e-4;
     o->same_spin_kernel = FCIB_SAME_TC;
     o->spin_adapt = 0;
+    o->sym_blocked = 1;
 }
 
 const char* fcib_last_error(void) { return g_last_error.c_str(); }
@@ -306,7 +308,14 @@ int fcib_set_options(fcib_ctx* ctx, const fcib_options* o) {
                    "bad preconditioner");
         FCIB_CHECK(o->same_spin_kernel == FCIB_SAME_TC || o->same_spin_kernel == FCIB_SAME_CUDA_CORES, FCIB_ERR_ARG,
                    "bad same-spin kernel");
-        ctx->c.opt = *o;
+        Context& c = ctx->c;
+        if ((o->sym_blocked != 0) != (c.opt.sym_blocked != 0)) {
+            // the vector layout changes: tables, stored vectors and the restart state go
+            c.tables_ready = false;
+            c.solved = false;
+            c.dl_prev = false;
+        }
+        c.opt = *o;
     });
 }
 
@@ -351,8 +360,8 @@ int fcib_solve(fcib_ctx* ctx, double* energies, double* spin2, int* iterations) 
 // their irreps); slots past the nonzero elements hold zeros, as the reference's preset tuples do.
 static void max_abs_elements(Context& c, int root, int num_dets, std::vector<double>& absv, std::vector<double>& val,
                              std::vector<int>& irr, std::vector<int64_t>& ia, std::vector<int64_t>& ib) {
-    const int64_t N = c.ndet;
-    const int64_t nflat = c.nirrep <= 1 ? N : (int64_t)c.block_to_c1.size();
+    const int64_t N = c.nvec;
+    const int64_t nflat = (c.nirrep <= 1 || c.sym.on) ? N : (int64_t)c.block_to_c1.size();
     num_dets = (int)std::min<int64_t>(num_dets, nflat);
     absv.assign(num_dets, 0.0);
     val.assign(num_dets, 0.0);
@@ -386,10 +395,25 @@ static void max_abs_elements(Context& c, int root, int num_dets, std::vector<dou
         for (int h = 0; h < 8; h++) blk[h + 1] = blk[h] + cnta[h] * cntb[h ^ (c.nirrep > 1 ? c.irrep : 0)];
         for (int64_t i = 0; i < c.nas; i++) pa[i] = blk[ha[i]] + ra[i] * cntb[ha[i] ^ (c.nirrep > 1 ? c.irrep : 0)];
     }
-    std::vector<std::pair<std::pair<double, int64_t>, int64_t>> order;  // ((-|C|, flat), c1)
+    // vector index -> (FCIVector flat position, alpha irrep, addresses within the irrep blocks)
+    auto locate = [&](int64_t idx, int64_t& flat, int& h, int64_t& ai, int64_t& bi) {
+        if (c.sym.on) {  // the blocked layout is the flat order
+            flat = idx;
+            sym_host_locate(c, idx, h, ai, bi);
+            return;
+        }
+        const int64_t i = idx / c.nbs, j = idx % c.nbs;
+        flat = pa[i] + rb[j];
+        h = ha[i];
+        ai = ra[i];
+        bi = rb[j];
+    };
+    std::vector<std::pair<std::pair<double, int64_t>, int64_t>> order;  // ((-|C|, flat), vector index)
     for (auto& e : sel) {
-        const int64_t i = e.second / c.nbs, j = e.second % c.nbs;
-        order.push_back({{e.first, pa[i] + rb[j]}, e.second});
+        int64_t flat, ai, bi;
+        int h;
+        locate(e.second, flat, h, ai, bi);
+        order.push_back({{e.first, flat}, e.second});
     }
     std::sort(order.begin(), order.end());
     std::vector<double> h(order.size());
@@ -399,12 +423,14 @@ static void max_abs_elements(Context& c, int root, int num_dets, std::vector<dou
     for (int t = 0; t < num_dets && t < (int)order.size(); t++) {
         const double a = -order[t].first.first;
         if (!(a > 0.0)) break;
-        const int64_t i = order[t].second / c.nbs, j = order[t].second % c.nbs;
+        int64_t flat, ai, bi;
+        int hh;
+        locate(order[t].second, flat, hh, ai, bi);
         absv[t] = a;
         val[t] = h[t];
-        irr[t] = ha[i];
-        ia[t] = ra[i];
-        ib[t] = rb[j];
+        irr[t] = hh;
+        ia[t] = ai;
+        ib[t] = bi;
     }
 }
 
@@ -490,7 +516,7 @@ int fcib_get_vector(fcib_ctx* ctx, int root, double* out) {
         Context& c = ctx->c;
         FCIB_CHECK(c.solved, FCIB_ERR_STATE, "no solution available");
         FCIB_CHECK(root >= 0 && root < c.nroot, FCIB_ERR_ARG, "root out of range");
-        download_flat(c, c.b.p + (size_t)root * c.ndet, out);
+        download_flat(c, c.b.p + (size_t)root * c.nvec, out);
     });
 }
 
@@ -500,8 +526,8 @@ int fcib_sigma(fcib_ctx* ctx, const double* b, double* sigma) {
         Context& c = ctx->c;
         ensure_setup(c);
         DBuf<double> db, ds;
-        db.alloc(c.ndet);
-        ds.alloc(c.ndet);
+        db.alloc(c.nvec);
+        ds.alloc(c.nvec);
         upload_flat(c, b, db.p);
         sigma_dispatch(c, db.p, ds.p, c.opt.precision);
         download_flat(c, ds.p, sigma);
@@ -539,8 +565,7 @@ int fcib_spin2(fcib_ctx* ctx, const double* cvec, double* s2) {
         Context& c = ctx->c;
         ensure_setup(c);
         DBuf<double> d;
-        d.alloc(c.ndet);
-        if (c.nirrep > 1) FCIB_CUDA(cudaMemsetAsync(d.p, 0, sizeof(double) * c.ndet, c.stream));
+        d.alloc(c.nvec);
         upload_flat(c, cvec, d.p);
         *s2 = spin2_device(c, d.p);
     });
@@ -561,7 +586,10 @@ int fcib_rdms(fcib_ctx* ctx, int root_left, int root_right, int level, int spin_
         if (level <= 0) return;
         level = std::min(level, 2);  // the three-body blocks come from fcib_rdms3
         RdmBlocks blk;
-        compute_rdms(c, c.b.p + (size_t)root_left * c.ndet, c.b.p + (size_t)root_right * c.ndet, level, blk);
+        DBuf<double> xl, xr;
+        const double* L = c1_view(c, c.b.p + (size_t)root_left * c.nvec, xl);
+        const double* R = root_right == root_left ? L : c1_view(c, c.b.p + (size_t)root_right * c.nvec, xr);
+        compute_rdms(c, L, R, level, blk);
         rdms_to_outputs(blk, level, spin_free, g1a, g1b, g2aa, g2ab, g2bb);
     });
 }
@@ -577,7 +605,7 @@ int fcib_transition_rdms(fcib_ctx* left, int root_left, fcib_ctx* right, int roo
     if (!left || !right) { set_error("null context"); return FCIB_ERR_ARG; }
     return guarded(left, [&] {
         Context& c = left->c;
-        const Context& r = right->c;
+        Context& r = right->c;
         FCIB_CHECK(c.solved && r.solved, FCIB_ERR_STATE, "FCIVector is not assigned. Cannot compute RDMs.");
         FCIB_CHECK(level <= 3 && level >= 1, FCIB_ERR_ARG, "Invalid max_rdm_level, required 1 <= max_rdm_level <= 3.");
         FCIB_CHECK(root_left >= 0 && root_right >= 0, FCIB_ERR_ARG, "negative root index");
@@ -599,9 +627,13 @@ int fcib_transition_rdms(fcib_ctx* left, int root_left, fcib_ctx* right, int roo
         // the reference returns empty blocks when the left state has no alpha electrons, for both
         // spins (compute_1rdm_different_irrep takes nb from the alpha address), and so does this call
         if (c.na >= 1) {
+            // both vectors in the C1 layout, which does not depend on the irrep
+            DBuf<double> xl, xr;
+            const double* L = c1_view(c, c.b.p + (size_t)root_left * c.nvec, xl);
+            const double* R = c1_view(r, r.b.p + (size_t)root_right * r.nvec, xr);
             FCIB_CUDA(cudaStreamSynchronize(r.stream));
             RdmBlocks blk;
-            compute_rdms(c, c.b.p + (size_t)root_left * c.ndet, r.b.p + (size_t)root_right * r.ndet, 1, blk);
+            compute_rdms(c, L, R, 1, blk);
             a = blk.g1a;
             b = blk.g1b;
         }
@@ -624,17 +656,18 @@ int fcib_compute_rdms(fcib_ctx* ctx, const double* left, const double* right, in
         FCIB_CHECK(level <= 3, FCIB_ERR_UNSUPPORTED, "RDMs of order higher than 3 are not available");
         if (level <= 0) return;
         level = std::min(level, 2);  // the three-body blocks come from fcib_compute_rdms3
-        DBuf<double> dl, dr;
-        dl.alloc(c.ndet);
+        DBuf<double> dl, dr, xl, xr;
+        dl.alloc(c.nvec);
         upload_flat(c, left, dl.p);
-        const double* R = dl.p;
+        const double* L = c1_view(c, dl.p, xl);
+        const double* R = L;
         if (right && right != left) {
-            dr.alloc(c.ndet);
+            dr.alloc(c.nvec);
             upload_flat(c, right, dr.p);
-            R = dr.p;
+            R = c1_view(c, dr.p, xr);
         }
         RdmBlocks blk;
-        compute_rdms(c, dl.p, R, level, blk);
+        compute_rdms(c, L, R, level, blk);
         rdms_to_outputs(blk, level, spin_free, g1a, g1b, g2aa, g2ab, g2bb);
     });
 }
@@ -681,7 +714,10 @@ int fcib_rdms3(fcib_ctx* ctx, int root_left, int root_right, int spin_free, doub
                                           std::to_string(root_right) + "> (0-based) because nroot = " +
                                           std::to_string(c.nroot)};
         Rdm3Blocks blk;
-        compute_rdms3(c, c.b.p + (size_t)root_left * c.ndet, c.b.p + (size_t)root_right * c.ndet, blk);
+        DBuf<double> xl, xr;
+        const double* L = c1_view(c, c.b.p + (size_t)root_left * c.nvec, xl);
+        const double* R = root_right == root_left ? L : c1_view(c, c.b.p + (size_t)root_right * c.nvec, xr);
+        compute_rdms3(c, L, R, blk);
         rdms3_to_outputs(blk, spin_free, g3aaa, g3aab, g3abb, g3bbb);
     });
 }
@@ -692,17 +728,18 @@ int fcib_compute_rdms3(fcib_ctx* ctx, const double* left, const double* right, i
     return guarded(ctx, [&] {
         Context& c = ctx->c;
         ensure_setup(c);
-        DBuf<double> dl, dr;
-        dl.alloc(c.ndet);
+        DBuf<double> dl, dr, xl, xr;
+        dl.alloc(c.nvec);
         upload_flat(c, left, dl.p);
-        const double* R = dl.p;
+        const double* L = c1_view(c, dl.p, xl);
+        const double* R = L;
         if (right && right != left) {
-            dr.alloc(c.ndet);
+            dr.alloc(c.nvec);
             upload_flat(c, right, dr.p);
-            R = dr.p;
+            R = c1_view(c, dr.p, xr);
         }
         Rdm3Blocks blk;
-        compute_rdms3(c, dl.p, R, blk);
+        compute_rdms3(c, L, R, blk);
         rdms3_to_outputs(blk, spin_free, g3aaa, g3aab, g3abb, g3bbb);
     });
 }

@@ -73,7 +73,7 @@ static void csf_coupling(int N, int twoS, int twoMs, std::vector<double>& O, std
 // one configuration, so the scatter has no conflicts.
 __global__ void k_csf_project(double* __restrict__ v, const uint32_t* __restrict__ conf, int nconf, int N, int nd,
                               int f, const uint32_t* __restrict__ pats, const double* __restrict__ O, int n,
-                              int nbs) {
+                              int nbs, SymDev sd) {
     extern __shared__ __align__(16) unsigned char csf_smem[];
     double* x = reinterpret_cast<double*>(csf_smem);  // [nd]
     double* z = x + nd;                               // [f]
@@ -90,7 +90,9 @@ __global__ void k_csf_project(double* __restrict__ v, const uint32_t* __restrict
                 if (pat >> k & 1u) a |= bit;
                 else b |= bit;
             }
-            const int id = (int)(d_rank(a, n) * (uint32_t)nbs + d_rank(b, n));
+            // the determinant's index in the engine layout (C1, or the target irrep's blocks)
+            const uint32_t ra = d_rank(a, n), rb = d_rank(b, n);
+            const int id = sd.nirrep > 1 ? (int)sym_encode(sd, a, (int)ra, (int)rb) : (int)(ra * (uint32_t)nbs + rb);
             idx[m] = id;
             x[m] = v[id];
         }
@@ -167,7 +169,7 @@ static void ensure_csf(Context& c) {
     c.csf_twoS = twoS;
 }
 
-// v <- projection of v onto the spin-S sector (C1 layout)
+// v <- projection of v onto the spin-S sector (engine layout)
 void csf_project(Context& c, double* v) {
     // k_csf_project keeps determinant indices as int in shared memory
     FCIB_CHECK(c.ndet < ((int64_t)1 << 31), FCIB_ERR_UNSUPPORTED,
@@ -180,7 +182,8 @@ void csf_project(Context& c, double* v) {
         FCIB_CUDA(cudaFuncSetAttribute(k_csf_project, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         const int grid = std::min(g.nconf, 8 * c.num_sms);
         k_csf_project<<<grid, g.nd > 64 ? 256 : 64, smem, c.stream>>>(v, g.conf.p, g.nconf, g.N, g.nd, g.f, g.pats.p,
-                                                                       g.f > 0 ? g.O.p : nullptr, c.n, (int)c.nbs);
+                                                                       g.f > 0 ? g.O.p : nullptr, c.n, (int)c.nbs,
+                                                                       sym_dev(c));
         FCIB_KCHECK();
     }
 }

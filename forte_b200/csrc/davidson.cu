@@ -357,15 +357,24 @@ __global__ void k_collect_le(const double* __restrict__ hd, const uint8_t* __res
 // per determinant: doubly occupied orbitals (r = s) and alpha/beta open-shell swaps.
 // ------------------------------------------------------------------------------------------
 
+// C in the engine layout: C1 (sd.nirrep = 1, nas * nbs elements) or the blocked layout of sd (N elements)
 __global__ void __launch_bounds__(kRedThreads) k_spin2(const double* __restrict__ C, const uint32_t* __restrict__ sa,
                                                        const uint32_t* __restrict__ sb, int nas, int nbs, int n,
-                                                       double* __restrict__ partial) {
+                                                       double* __restrict__ partial, SymDev sd, size_t N) {
     double acc = 0.0;
-    const size_t N = (size_t)nas * nbs;
+    const bool blocked = sd.nirrep > 1;
+    if (!blocked) N = (size_t)nas * nbs;
     for (size_t I = blockIdx.x * (size_t)blockDim.x + threadIdx.x; I < N; I += (size_t)gridDim.x * blockDim.x) {
         double ci = C[I];
         if (ci == 0.0) continue;
-        uint32_t Ia = sa[I / nbs], Ib = sb[I % nbs];
+        int ia, ib;
+        if (blocked) {
+            sym_decode(sd, (int64_t)I, ia, ib);
+        } else {
+            ia = (int)(I / nbs);
+            ib = (int)(I % nbs);
+        }
+        uint32_t Ia = sa[ia], Ib = sb[ib];
         double t = (double)__popc(Ia & Ib) * ci;
         uint32_t oa = Ia & ~Ib, ob = Ib & ~Ia;
         // alpha electron s -> r and beta electron r -> s with s in oa, r in ob
@@ -378,7 +387,8 @@ __global__ void __launch_bounds__(kRedThreads) k_spin2(const double* __restrict_
                 int lo = r < s ? r : s, hi = r < s ? s : r;
                 uint32_t m = (hi - lo < 2) ? 0u : (((1u << hi) - 1u) & ~((2u << lo) - 1u));
                 int par = (__popc(Ia & m) + __popc(Ib & m)) & 1;
-                double cj = C[(size_t)d_rank(Ja, n) * nbs + d_rank(Jb, n)];
+                const int ja = (int)d_rank(Ja, n), jb = (int)d_rank(Jb, n);
+                double cj = C[blocked ? (size_t)sym_encode(sd, Ja, ja, jb) : (size_t)ja * nbs + jb];
                 t += par ? -cj : cj;
             }
         }
@@ -405,7 +415,7 @@ struct Ops {
     DBuf<double> partial, out;
     std::vector<double> hout;
     explicit Ops(Context& cc) : c(cc) {
-        N = (size_t)c.ndet;
+        N = (size_t)c.nvec;
         nblk = std::max(1, std::min(4 * c.num_sms, (int)((N + kRedThreads - 1) / kRedThreads)));
         partial.alloc((size_t)nblk * kSlots);
         out.alloc(kSlots);
@@ -606,7 +616,8 @@ static void project_out(Context& c, std::vector<SparseDev>& bad, std::vector<dou
 
 double spin2_device(Context& c, const double* C) {
     Ops ops(c);
-    k_spin2<<<ops.nblk, kRedThreads, 0, c.stream>>>(C, c.A.str.p, c.B.str.p, (int)c.nas, (int)c.nbs, c.n, ops.partial.p);
+    k_spin2<<<ops.nblk, kRedThreads, 0, c.stream>>>(C, c.A.str.p, c.B.str.p, (int)c.nas, (int)c.nbs, c.n, ops.partial.p,
+                                                    sym_dev(c), (size_t)c.nvec);
     FCIB_KCHECK();
     ops.fetch(1);
     double s = ops.hout[0];
@@ -619,8 +630,8 @@ double spin2_device(Context& c, const double* C) {
 // the `count` smallest keys[] of the determinants in the target irrep with their C1 indices, sorted by
 // (key, index); ties at the boundary are resolved by the index
 std::vector<std::pair<double, int64_t>> lowest_keys(Context& c, const double* keys, int count) {
-    const size_t N = (size_t)c.ndet;
-    const uint8_t* mask = (c.nirrep > 1) ? c.mask.p : nullptr;
+    const size_t N = (size_t)c.nvec;
+    const uint8_t* mask = (c.nirrep > 1 && !c.sym.on) ? c.mask.p : nullptr;
     DBuf<unsigned int> hist;
     hist.alloc(256);
     uint64_t prefix = 0, pmask = 0;
@@ -685,9 +696,9 @@ static double now_ms() {
 enum class Phase { LowPrecision, Refine, FP64Only };
 
 void dl_solve(Context& c) {
-    const int64_t N = c.ndet;
+    const int64_t N = c.nvec;
     int64_t Neff = N;
-    if (c.nirrep > 1) {
+    if (c.nirrep > 1 && !c.sym.on) {
         std::vector<uint8_t> hm(N);
         FCIB_CUDA(cudaMemcpy(hm.data(), c.mask.p, N, cudaMemcpyDeviceToHost));
         Neff = 0;
@@ -785,9 +796,19 @@ void dl_solve(Context& c) {
         const int n = c.n;
         GuessResult gr;
         try {
+            // vector index <-> determinant in the engine layout (C1 or the target irrep's blocks)
             gr = make_guess(
-                hi, lowest, [&](int64_t I) { return Det{sa[I / nbs], sbv[I % nbs]}; },
-                [&](const Det& d) { return (int64_t)host_rank((uint32_t)d.a, n) * nbs + host_rank((uint32_t)d.b, n); },
+                hi, lowest,
+                [&](int64_t I) {
+                    if (!c.sym.on) return Det{sa[I / nbs], sbv[I % nbs]};
+                    int64_t ia, ib;
+                    sym_host_decode(c, I, ia, ib);
+                    return Det{sa[ia], sbv[ib]};
+                },
+                [&](const Det& d) {
+                    const int64_t ia = host_rank((uint32_t)d.a, n), ib = host_rank((uint32_t)d.b, n);
+                    return c.sym.on ? sym_host_encode(c, ia, ib) : ia * nbs + ib;
+                },
                 num_guess_states, c.multiplicity);
         } catch (std::exception& e) {
             throw Error{FCIB_ERR_ARG, e.what()};

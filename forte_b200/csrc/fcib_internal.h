@@ -111,6 +111,99 @@ struct SpinTables {
 };
 void build_spin_tables(SpinTables& t, int n, int k, bool need_g1, cudaStream_t s);
 
+// ------------------------------------------------------------------------------------------
+// irrep-blocked determinant space (symblock.cu)
+// ------------------------------------------------------------------------------------------
+// With point-group symmetry the engine's vectors hold only the determinants of the target irrep,
+// in FCIVector flat order (forte/fci/fci_vector.cc:86-169): alpha irrep blocks h, each the alpha
+// strings of irrep h (string order) x the beta strings of irrep h ^ irrep.  The beta same-spin
+// terms work on the transposed blocks: beta irrep h x the alpha strings of irrep h ^ irrep.
+constexpr uint32_t kNullRow = 0x7FFFFFFFu;  // padding member of a same-spin group (no string)
+
+// device view of the blocked layout, passed to kernels by value
+struct SymDev {
+    int nirrep = 1, irrep = 0;
+    uint32_t irrbit[3] = {0u, 0u, 0u};  // orbitals whose irrep label has bit b set
+    int64_t blk[9] = {};                // alpha-major block offsets
+    int32_t bcol[8] = {};               // row length of alpha block h (beta strings of irrep h ^ irrep)
+    int32_t aoff[8] = {}, boff[8] = {}; // first position of each irrep in the irrep-sorted string lists
+    const int32_t* asrc = nullptr;      // irrep-sorted position -> string index
+    const int32_t* bsrc = nullptr;
+    const int32_t* aloc = nullptr;      // string index -> position among the strings of its irrep
+    const int32_t* bloc = nullptr;
+};
+
+__host__ __device__ inline int sym_irrep_of(const SymDev& d, uint32_t s) {
+#ifdef __CUDA_ARCH__
+    return (__popc(s & d.irrbit[0]) & 1) | ((__popc(s & d.irrbit[1]) & 1) << 1) | ((__popc(s & d.irrbit[2]) & 1) << 2);
+#else
+    return (__builtin_popcount(s & d.irrbit[0]) & 1) | ((__builtin_popcount(s & d.irrbit[1]) & 1) << 1) |
+           ((__builtin_popcount(s & d.irrbit[2]) & 1) << 2);
+#endif
+}
+// blocked index -> (alpha string index, beta string index)
+__device__ __forceinline__ void sym_decode(const SymDev& d, int64_t I, int& ia, int& ib) {
+    int h = 0;
+    for (int x = 1; x < d.nirrep; x++)
+        if (I >= d.blk[x]) h = x;  // an empty block x shares its offset with x + 1, which wins
+    const int64_t r = I - d.blk[h];
+    const int64_t col = d.bcol[h];
+    const int64_t i = r / col;
+    ia = d.asrc[d.aoff[h] + i];
+    ib = d.bsrc[d.boff[h ^ d.irrep] + (int)(r - i * col)];
+}
+// (alpha string sa with index ia, beta string index ib) of the target irrep -> blocked index
+__device__ __forceinline__ int64_t sym_encode(const SymDev& d, uint32_t sa, int ia, int ib) {
+    const int h = sym_irrep_of(d, sa);
+    return d.blk[h] + (int64_t)d.aloc[ia] * d.bcol[h] + d.bloc[ib];
+}
+
+// one opposite-spin sub-problem of the blocked sigma: target alpha irrep ha, pair irrep g.  Rows are
+// the alpha strings of irrep ha; their connections through pairs of irrep g reach alpha strings of
+// irrep ha ^ g, whose rows hold the beta strings of irrep ha ^ irrep ^ g (the source columns); the
+// beta replacements of irrep g take those to the target columns (beta irrep ha ^ irrep).
+struct AbSub {
+    int ha = 0, g = 0, src = 0;  // target alpha irrep, pair irrep, source alpha irrep ha ^ g
+    int rows = 0, ns = 0, nt = 0;
+    int kmax = 0;                // connections per row (short rows padded with the zero pair)
+    size_t conn = 0, tgt32 = 0, tgt16 = 0, mag = 0;  // offsets into the SymSpace tables
+};
+// same-spin groups whose strings lie in one irrep (padded to G members with kNullRow)
+struct GroupSub {
+    int ngroups = 0, G = 0, ncols = 0;
+    int64_t blk = 0;   // block offset: alpha-major for alpha groups, transposed for beta groups
+    size_t off = 0;    // into SymSpace::grow / glab
+};
+struct SymSpace {
+    bool on = false;
+    SymDev d;
+    int64_t blkT[9] = {};
+    int acnt[8] = {}, bcnt[8] = {};
+    std::vector<int> airr, birr;                      // irrep of each string
+    std::vector<int32_t> asrc_h, bsrc_h, aloc_h, bloc_h;
+    DBuf<int32_t> asrc, bsrc, aloc, bloc;
+    DBuf<uint32_t> bstr_sorted;                       // beta strings in irrep-sorted order
+    // opposite spin
+    std::vector<AbSub> ab;                            // per target irrep: g = 0 first
+    int npp = 0;                                      // rows of V; the zero pair is row npp
+    std::vector<int> np_g, npg, noff8_g, ndiag_g;     // per pair irrep: pairs, FP64 columns (x8), tensor-core layout
+    std::vector<size_t> vg_off, perm_off;
+    DBuf<double> Vg;    // per g: (npp + 1) x npg[g], column j = pair j of irrep g
+    DBuf<double> Vz;    // the pair matrix with the zero pair row appended, (npp + 1) x npp
+    DBuf<int> perm;     // per g: tensor-core columns -> pair (off-diagonal pairs, then the diagonal ones)
+    DBuf<uint32_t> conn;
+    DBuf<int32_t> tgt32;
+    DBuf<uint16_t> tgt16;
+    DBuf<uint8_t> mag;
+    std::vector<size_t> plane_off;                    // TF32 plane of each alpha block (float2 units)
+    std::vector<int> ldp;
+    size_t plane_total = 0;
+    // same spin
+    std::vector<GroupSub> a2, a1, b2, b1;
+    DBuf<uint32_t> grow;
+    DBuf<uint16_t> glab;
+};
+
 // a pair of CUDA events owned by the context (created on first use)
 struct EventPair {
     cudaEvent_t e[2] = {nullptr, nullptr};
@@ -153,7 +246,9 @@ struct Context {
     // device tables
     SpinTables A, B;
     bool tables_ready = false;
-    int64_t nas = 0, nbs = 0, ndet = 0;
+    int64_t nas = 0, nbs = 0, ndet = 0;  // ndet = nas * nbs (the C1 layout)
+    int64_t nvec = 0;     // length of the engine's vectors: ndet, or the target irrep's blocks
+    SymSpace sym;         // the blocked layout (sym.on) when the state has point-group symmetry
     DBuf<double> V;       // [npair_pad_a x npair_pad_b] pair-pair (pq|rs) (+ folded h)
     DBuf<double> M2a, M2b;  // same-spin <pq||rs> over pairs p>q, r>s
     DBuf<double> Ha, Hb;  // one-body matrices (used when h is not folded)
@@ -220,6 +315,9 @@ struct Context {
     std::vector<double> cap_lambda;  // iteration, ms, lambda_0, max residual, fp64 basis
 };
 
+// the blocked layout's device view for kernels that decode vector indices (nirrep = 1: C1 layout)
+inline SymDev sym_dev(const Context& c) { return c.sym.on ? c.sym.d : SymDev{}; }
+
 // counter slots: 0 opposite-spin row counter, 1 its timeout flag, 2 CUDA-core group counter,
 // 3 bits of max|C| of the sigma input, 4 tensor-core group counter, 5 its timeout flag,
 // 6 exponent el of the same-spin fixed-point grid 2^-el, 7 bits of max|C| of an FP64 sigma input
@@ -260,6 +358,16 @@ struct Rdm3Blocks {
 void compute_rdms3(Context& c, const double* L, const double* R, Rdm3Blocks& out);
 // mlp.cu: learned preconditioner, in place on a diagonal correction t
 void mlp_apply(Context& c, double* t, double lambda, double rnorm, double tnorm);
+// symblock.cu: blocked-layout tables of the target irrep (c.sym.on when nirrep > 1 and blocking is on)
+void build_sym_space(Context& c);
+// v (engine layout) in the C1 layout: v itself without blocking, else expanded into buf
+const double* c1_view(Context& c, const double* v, DBuf<double>& buf);
+// engine layout <- C1 layout (blocked: the target irrep's elements)
+void from_c1(Context& c, const double* c1, double* v);
+// host view of a blocked index: (alpha irrep, positions within the irrep blocks) / string indices
+void sym_host_locate(const Context& c, int64_t I, int& h, int64_t& ia_loc, int64_t& ib_loc);
+void sym_host_decode(const Context& c, int64_t I, int64_t& ia, int64_t& ib);
+int64_t sym_host_encode(const Context& c, int64_t ia, int64_t ib);
 // davidson.cu
 void dl_solve(Context& c);
 std::vector<std::pair<double, int64_t>> lowest_keys(Context& c, const double* keys, int count);

@@ -91,7 +91,7 @@ struct MlpSmem {
     __nv_bfloat16 w3[kMlpH * kW2Ld];
 };
 
-struct EngineSource {  // determinant I of a C1 vector: diagonal correction t rescaled in place
+struct EngineSource {  // determinant I of an engine-layout vector: diagonal correction t rescaled in place
     double* t;
     const double* hd;
     const float* tabA;  // [nas][64]
@@ -100,10 +100,18 @@ struct EngineSource {  // determinant I of a C1 vector: diagonal correction t re
     double lambda;
     float inv_rnorm;
     float skip;  // tiles whose |t_I| are all below this keep the diagonal rule
+    SymDev sd;   // the blocked layout (sd.nirrep > 1) or C1
     __device__ bool load(size_t I, uint32_t& a, uint32_t& b, float& u, float& rr, double& tv) const {
-        const unsigned Iu = (unsigned)I;
-        a = Iu / nbs;
-        b = Iu - a * nbs;
+        if (sd.nirrep > 1) {
+            int ia, ib;
+            sym_decode(sd, (int64_t)I, ia, ib);
+            a = (uint32_t)ia;
+            b = (uint32_t)ib;
+        } else {
+            const unsigned Iu = (unsigned)I;
+            a = Iu / nbs;
+            b = Iu - a * nbs;
+        }
         const double h = hd[I];
         tv = t[I];
         u = (float)(h - lambda);
@@ -476,10 +484,10 @@ void mlp_apply(Context& c, double* t, double lambda, double rnorm, double tnorm)
         c.mlp_tables_ready = true;
     }
     EngineSource src{t, c.hdiag.p, c.mlp_tabA.p, c.mlp_tabB.p, (unsigned)c.nbs, lambda,
-                     (float)(rnorm > 0.0 ? 1.0 / rnorm : 0.0), (float)(kMlpSkip * tnorm)};
+                     (float)(rnorm > 0.0 ? 1.0 / rnorm : 0.0), (float)(kMlpSkip * tnorm), sym_dev(c)};
     const size_t smem = sizeof(MlpSmem);
     FCIB_CUDA(cudaFuncSetAttribute(k_mlp_apply<EngineSource>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const size_t N = (size_t)c.ndet;
+    const size_t N = (size_t)c.nvec;
     const int grid = (int)std::min<size_t>((size_t)6 * c.num_sms, (N + 127) / 128);
     k_mlp_apply<EngineSource><<<grid, 256, smem, c.stream>>>(src, N, MlpDevice{c.mlp_w.p});
     FCIB_KCHECK();
@@ -563,14 +571,14 @@ int fcib_precondition(fcib_ctx* ctx, const double* r, double lambda, double* out
         for (int64_t i = 0; i < nf; i++) rn += r[i] * r[i];
         rn = std::sqrt(rn);
         DBuf<double> d;
-        d.alloc(c.ndet);
-        if (c.nirrep > 1) FCIB_CUDA(cudaMemsetAsync(d.p, 0, sizeof(double) * c.ndet, c.stream));
+        d.alloc(c.nvec);
+        if (c.nirrep > 1 && !c.sym.on) FCIB_CUDA(cudaMemsetAsync(d.p, 0, sizeof(double) * c.nvec, c.stream));
         upload_flat(c, r, d.p);
-        k_diag_correction<<<4 * c.num_sms, 256, 0, c.stream>>>(d.p, c.hdiag.p, lambda, (size_t)c.ndet);
+        k_diag_correction<<<4 * c.num_sms, 256, 0, c.stream>>>(d.p, c.hdiag.p, lambda, (size_t)c.nvec);
         FCIB_KCHECK();
         if (c.opt.preconditioner == FCIB_PRECOND_MLP) {
-            std::vector<double> h((size_t)c.ndet);
-            FCIB_CUDA(cudaMemcpyAsync(h.data(), d.p, sizeof(double) * c.ndet, cudaMemcpyDeviceToHost, c.stream));
+            std::vector<double> h((size_t)c.nvec);
+            FCIB_CUDA(cudaMemcpyAsync(h.data(), d.p, sizeof(double) * c.nvec, cudaMemcpyDeviceToHost, c.stream));
             FCIB_CUDA(cudaStreamSynchronize(c.stream));
             double tn = 0.0;
             for (double x : h) tn += x * x;

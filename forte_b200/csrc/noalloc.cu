@@ -97,7 +97,7 @@ extern "C" int fcib_spin2_device_noalloc(fcib_ctx* ctx, const double* d_c, doubl
         FCIB_CHECK(c.has_ints && c.has_state && c.tables_ready, FCIB_ERR_STATE,
                    "fcib_spin2_device_noalloc: string tables not built (call fcib_size, fcib_solve or "
                    "fcib_spin2 on this context first)");
-        const size_t N = (size_t)c.ndet;
+        const size_t N = (size_t)c.nvec;
         const int nblk = std::max(1, std::min(4 * c.num_sms, (int)((N + kRedThreads - 1) / kRedThreads)));
         FCIB_CHECK(nblk <= kNoAllocMaxBlocks, FCIB_ERR_UNSUPPORTED,
                    "fcib_spin2_device_noalloc: launch needs more partial-sum blocks than the static "
@@ -105,7 +105,8 @@ extern "C" int fcib_spin2_device_noalloc(fcib_ctx* ctx, const double* d_c, doubl
         double* partial = noalloc_scratch(c.device);
         double* out = partial + (size_t)kNoAllocMaxBlocks * kSlots;
         cudaStream_t st = stream ? (cudaStream_t)stream : c.stream;
-        k_spin2<<<nblk, kRedThreads, 0, st>>>(d_c, c.A.str.p, c.B.str.p, (int)c.nas, (int)c.nbs, c.n, partial);
+        k_spin2<<<nblk, kRedThreads, 0, st>>>(d_c, c.A.str.p, c.B.str.p, (int)c.nas, (int)c.nbs, c.n, partial,
+                                              sym_dev(c), (size_t)c.nvec);
         FCIB_KCHECK();
         k_final_reduce<<<1, 256, 0, st>>>(partial, nblk, out);
         FCIB_KCHECK();

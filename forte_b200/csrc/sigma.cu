@@ -125,17 +125,23 @@ __device__ __forceinline__ int grid_el_fp64(const unsigned int* cmax_bits, doubl
     return min(1000, (int)floor(62.0 - log2(b)));
 }
 
+// Source rows (the connected strings J) are rows of Csrc with ns columns (row stride lds); target rows
+// Ia have nt columns (C for the E0 term and S, row stride nt).  tgtB rows hold the targets of the
+// source columns (row stride ldt), V rows the pair-matrix columns (row stride ldv).  accumulate = 1
+// adds to S instead of writing E0 C + the product (the blocked sigma's later pair irreps).  In the C1
+// layout Csrc = C, ns = lds = nt = nbs.
 __global__ void __launch_bounds__(kDmThreads, 1) k_ab_fp64(
-    const double* __restrict__ C, double* __restrict__ S, const uint32_t* __restrict__ connA, int s1a, int kpad,
-    const int32_t* __restrict__ tgtB, int npp, int npair, const double* __restrict__ V, int nas, int nbs, double e0,
-    int* __restrict__ row_counter, const unsigned int* __restrict__ cmax_bits, double bound_per_c) {
+    const double* __restrict__ Csrc, int lds, int ns, const double* __restrict__ C, double* __restrict__ S, int nt,
+    int accumulate, const uint32_t* __restrict__ connA, int s1a, int kpad, const int32_t* __restrict__ tgtB, int ldt,
+    int npair, const double* __restrict__ V, int ldv, int nas, double e0, int* __restrict__ row_counter,
+    const unsigned int* __restrict__ cmax_bits, double bound_per_c) {
     extern __shared__ __align__(16) unsigned char smem[];
     // the sigma row in 64-bit fixed point: every product is rounded once to the grid and the integer
     // sum does not depend on the order of the atomics (a repeated sigma is bit-identical)
     unsigned long long* srow = reinterpret_cast<unsigned long long*>(smem);
     const int el = grid_el_fp64(cmax_bits, bound_per_c);
     const double scale = ldexp(1.0, el), inv_scale = ldexp(1.0, -el);
-    double* Bs = reinterpret_cast<double*>(srow + ((nbs + 1) & ~1));  // [kpad][kDmLdB]: (k, R) at k*kDmLdB + (R ^ ((k & 1) << 3))
+    double* Bs = reinterpret_cast<double*>(srow + ((nt + 1) & ~1));  // [kpad][kDmLdB]: (k, R) at k*kDmLdB + (R ^ ((k & 1) << 3))
     double* As = Bs + (size_t)kpad * kDmLdB;        // [kpad][kDmTM]: (k, Jb) at k*kDmTM + (Jb ^ ((k & 1) << 3))
     uint32_t* cs = reinterpret_cast<uint32_t*>(As + (size_t)kpad * kDmTM);
     __shared__ int s_row;
@@ -154,15 +160,16 @@ __global__ void __launch_bounds__(kDmThreads, 1) k_ab_fp64(
         const int Ia = s_row;
         if (Ia >= nas) break;
         for (int k = tid; k < kpad; k += kDmThreads) cs[k] = k < s1a ? connA[(size_t)Ia * s1a + k] : 0u;
-        const double* Crow = C + (size_t)Ia * nbs;
-        for (int j = tid; j < nbs; j += kDmThreads) srow[j] = fixed64d(e0 * Crow[j], scale);
+        const double* Crow = C + (size_t)Ia * nt;
+        double* Srow = S + (size_t)Ia * nt;
+        for (int j = tid; j < nt; j += kDmThreads) srow[j] = fixed64d(accumulate ? Srow[j] : e0 * Crow[j], scale);
         __syncthreads();
         for (int idx = tid; idx < kpad * kDmLdB; idx += kDmThreads) {
             const int k = idx / kDmLdB, R = idx - k * kDmLdB;
             double v = 0.0;
             if (k < s1a && R < npair) {
                 const uint32_t e = cs[k];
-                v = V[(size_t)((e >> 21) & 1023) * npp + R];
+                v = V[(size_t)((e >> 21) & 1023) * ldv + R];
                 if (e & kSignBit) v = -v;
             }
             Bs[(size_t)k * kDmLdB + (R ^ ((k & 1) << 3))] = v;
@@ -174,12 +181,12 @@ __global__ void __launch_bounds__(kDmThreads, 1) k_ab_fp64(
                 if (it < ng) {
                     const int e = it * kDmThreads + tid;
                     const int k = e / kDmTM, jb = jb0 + (e % kDmTM);
-                    g[it] = (jb < nbs && k < s1a) ? C[(size_t)(cs[k] & kConnIdxMask) * nbs + jb] : 0.0;
+                    g[it] = (jb < ns && k < s1a) ? Csrc[(size_t)(cs[k] & kConnIdxMask) * lds + jb] : 0.0;
                 }
             }
         };
         gather(0);
-        for (int jb0 = 0; jb0 < nbs; jb0 += kDmTM) {
+        for (int jb0 = 0; jb0 < ns; jb0 += kDmTM) {
             __syncthreads();  // the previous tile's fragment loads are done; B and cs are visible
 #pragma unroll
             for (int it = 0; it < kDmG; it++) {
@@ -190,7 +197,7 @@ __global__ void __launch_bounds__(kDmThreads, 1) k_ab_fp64(
                 }
             }
             __syncthreads();
-            if (jb0 + kDmTM < nbs) gather(jb0 + kDmTM);
+            if (jb0 + kDmTM < ns) gather(jb0 + kDmTM);
             double acc[kDmNT][2];
 #pragma unroll
             for (int j = 0; j < kDmNT; j++) acc[j][0] = acc[j][1] = 0.0;
@@ -222,13 +229,13 @@ __global__ void __launch_bounds__(kDmThreads, 1) k_ab_fp64(
             }
             // scatter T[Jb][R] over the beta single replacements into the sigma row
             const int jb = jb0 + mt * 8 + fr;
-            if (jb < nbs) {
+            if (jb < ns) {
 #pragma unroll
                 for (int j = 0; j < kDmNT; j++) {
-                    const int nt = h * kDmNT + j;
-                    if (nt < nnt) {
-                        const int R = nt * 8 + 2 * fk;
-                        const int2 tg = *reinterpret_cast<const int2*>(tgtB + (size_t)jb * npp + R);
+                    const int ntile = h * kDmNT + j;
+                    if (ntile < nnt) {
+                        const int R = ntile * 8 + 2 * fk;
+                        const int2 tg = *reinterpret_cast<const int2*>(tgtB + (size_t)jb * ldt + R);
                         if (tg.x != kNoTarget) {
                             const double v = acc[j][0];
                             atomicAdd(&srow[tg.x & kConnIdxMask], fixed64d((tg.x & (int)kSignBit) ? -v : v, scale));
@@ -242,8 +249,7 @@ __global__ void __launch_bounds__(kDmThreads, 1) k_ab_fp64(
             }
         }
         __syncthreads();
-        double* Srow = S + (size_t)Ia * nbs;
-        for (int j = tid; j < nbs; j += kDmThreads) Srow[j] = (double)(long long)srow[j] * inv_scale;
+        for (int j = tid; j < nt; j += kDmThreads) Srow[j] = (double)(long long)srow[j] * inv_scale;
     }
 }
 
@@ -327,7 +333,7 @@ __global__ void __launch_bounds__(1024) k_group(
             T v = (T)0;
             if (idx < G * kGrTN) {
                 const int j = idx / kGrTN, col = c0 + (idx - j * kGrTN);
-                if (col < ncols) v = C[(size_t)(rs[j] & kConnIdxMask) * ncols + col];
+                if (col < ncols && rs[j] != kNullRow) v = C[(size_t)(rs[j] & kConnIdxMask) * ncols + col];
             }
             xv[r] = v;
         }
@@ -378,7 +384,7 @@ __global__ void __launch_bounds__(1024) k_group(
 #pragma unroll
             for (int i = 0; i < kGrRows; i++) {
                 int ii = i0 + i;
-                if (ii < G) {
+                if (ii < G && rs[ii] != kNullRow) {
                     uint32_t e = rs[ii];
                     const size_t off = (size_t)(e & kConnIdxMask) * ncols + col;
                     auto* dst = S + off;
@@ -449,7 +455,7 @@ __global__ void __launch_bounds__(kGdThreads) k_group_dmma(
         for (int idx = tid; idx < Kp * kGdTN; idx += kGdThreads) {
             const int j = idx / kGdTN, col = idx - j * kGdTN;
             double v = 0.0;
-            if (j < G && c0 + col < ncols) {
+            if (j < G && c0 + col < ncols && rs[j] != kNullRow) {
                 const uint32_t r = rs[j];
                 v = C[(size_t)(r & kConnIdxMask) * ncols + c0 + col];
                 if (r & kSignBit) v = -v;
@@ -480,7 +486,7 @@ __global__ void __launch_bounds__(kGdThreads) k_group_dmma(
 #pragma unroll
         for (int m = 0; m < 6; m++) {
             const int i = m * 8 + fr;
-            if (m < nmt && i < G) {
+            if (m < nmt && i < G && rs[i] != kNullRow) {
                 const uint32_t r = rs[i];
                 unsigned long long* srow = S + (size_t)(r & kConnIdxMask) * ncols;
 #pragma unroll
@@ -639,7 +645,7 @@ static void transpose(Context& c, const double* in, double* out, int rows, int c
     FCIB_KCHECK();
 }
 void apply_mask(Context& c, double* v) {
-    if (c.nirrep <= 1 || !c.mask.p) return;
+    if (c.nirrep <= 1 || c.sym.on || !c.mask.p) return;
     k_apply_mask<<<4 * c.num_sms, 256, 0, c.stream>>>(v, c.mask.p, (size_t)c.ndet);
     FCIB_KCHECK();
 }
@@ -661,12 +667,13 @@ static void launch_group_same_f32(Context& c, const float* C, unsigned long long
 // same-spin (and, when not folded into the opposite-spin block, one-body) terms added to S
 static void sigma_same_spin(Context& c, const double* C, double* S, bool fp32) {
     const int nas = (int)c.nas, nbs = (int)c.nbs;
-    const size_t N = (size_t)c.ndet;
+    const size_t N = (size_t)c.nvec;
     const int np2 = c.n * (c.n - 1) / 2;
     const bool a_g1 = !c.fold_h && c.A.ng1, b_g1 = !c.fold_h && c.B.ng1;
     const bool any_a = a_g1 || c.A.ng2, any_b = b_g1 || c.B.ng2;
     if (!any_a && !any_b) return;
     ensure_counter(c);
+    const SymSpace& y = c.sym;
     // both precisions sum the same-spin results in int64 on a per-sigma fixed-point grid (the alpha
     // part row-major, the beta part transposed) and add them to S at the end
     auto same_grid = [&](const unsigned int* cmax_bits) {
@@ -683,19 +690,55 @@ static void sigma_same_spin(Context& c, const double* C, double* S, bool fp32) {
         FCIB_CUDA(cudaMemsetAsync(c.s64a.p, 0, N * sizeof(unsigned long long), c.stream));
         FCIB_CUDA(cudaMemsetAsync(c.st64.p, 0, N * sizeof(unsigned long long), c.stream));
     };
-    dim3 grid2((nas + 31) / 32, (nbs + 31) / 32), block2(32, 8);
+    // C -> its transpose: one matrix in the C1 layout, one per alpha block in the blocked layout
+    auto transpose_all = [&](const auto* in, auto* out, auto&& tr) {
+        if (!y.on) {
+            tr(in, out, nas, nbs);
+            return;
+        }
+        for (int ha = 0; ha < c.nirrep; ha++) {
+            const int hb = ha ^ c.irrep;
+            if (y.acnt[ha] && y.bcnt[hb]) tr(in + y.d.blk[ha], out + y.blkT[hb], y.acnt[ha], y.bcnt[hb]);
+        }
+    };
+    auto add_same = [&]() {
+        auto add = [&](double* Sx, const unsigned long long* A, const unsigned long long* Bt, int rows, int cols) {
+            dim3 grid2((rows + 31) / 32, (cols + 31) / 32), block2(32, 8);
+            k_add_same_fixed<<<grid2, block2, 0, c.stream>>>(Sx, A, Bt, rows, cols, c.counter.p + kSlotSameGrid);
+            FCIB_KCHECK();
+        };
+        if (!y.on) {
+            add(S, c.s64a.p, c.st64.p, nas, nbs);
+            return;
+        }
+        for (int ha = 0; ha < c.nirrep; ha++) {
+            const int hb = ha ^ c.irrep;
+            if (y.acnt[ha] && y.bcnt[hb])
+                add(S + y.d.blk[ha], c.s64a.p + y.d.blk[ha], c.st64.p + y.blkT[hb], y.acnt[ha], y.bcnt[hb]);
+        }
+    };
     if (!fp32) {
         same_grid(reinterpret_cast<unsigned int*>(c.counter.p + kSlotCmax64));  // max|C| from sigma_fp64
-        if (a_g1) launch_group(c, C, c.s64a.p, nbs, c.A.ng1, c.A.g1, c.A.g1row.p, c.A.g1lab.p, c.Ha.p, c.n);
-        if (c.A.ng2) launch_group(c, C, c.s64a.p, nbs, c.A.ng2, c.A.g2, c.A.g2row.p, c.A.g2lab.p, c.M2a.p, np2);
+        auto groups = [&](const double* X, unsigned long long* out, const std::vector<GroupSub>& subs, const SpinTables& t,
+                          bool one_body, int ncols, const double* M, int ldm) {
+            if (!y.on) {
+                if (one_body) launch_group(c, X, out, ncols, t.ng1, t.g1, t.g1row.p, t.g1lab.p, M, ldm);
+                else launch_group(c, X, out, ncols, t.ng2, t.g2, t.g2row.p, t.g2lab.p, M, ldm);
+                return;
+            }
+            for (const GroupSub& g : subs)
+                launch_group(c, X + g.blk, out + g.blk, g.ncols, g.ngroups, g.G, y.grow.p + g.off, y.glab.p + g.off, M,
+                             ldm);
+        };
+        if (a_g1) groups(C, c.s64a.p, y.a1, c.A, true, nbs, c.Ha.p, c.n);
+        if (c.A.ng2) groups(C, c.s64a.p, y.a2, c.A, false, nbs, c.M2a.p, np2);
         if (any_b) {
             c.ct.alloc(N);
-            transpose(c, C, c.ct.p, nas, nbs);
-            if (b_g1) launch_group(c, c.ct.p, c.st64.p, nas, c.B.ng1, c.B.g1, c.B.g1row.p, c.B.g1lab.p, c.Hb.p, c.n);
-            if (c.B.ng2) launch_group(c, c.ct.p, c.st64.p, nas, c.B.ng2, c.B.g2, c.B.g2row.p, c.B.g2lab.p, c.M2b.p, np2);
+            transpose_all(C, c.ct.p, [&](const double* in, double* out, int r, int cc) { transpose(c, in, out, r, cc); });
+            if (b_g1) groups(c.ct.p, c.st64.p, y.b1, c.B, true, nas, c.Hb.p, c.n);
+            if (c.B.ng2) groups(c.ct.p, c.st64.p, y.b2, c.B, false, nas, c.M2b.p, np2);
         }
-        k_add_same_fixed<<<grid2, block2, 0, c.stream>>>(S, c.s64a.p, c.st64.p, nas, nbs, c.counter.p + kSlotSameGrid);
-        FCIB_KCHECK();
+        add_same();
         return;
     }
     // mixed: FP32 copy of C (written by the tensor-core split when it ran), FP32 accumulation
@@ -710,18 +753,33 @@ static void sigma_same_spin(Context& c, const double* C, double* S, bool fp32) {
     // fixed-point grid from max|C| (just computed on the device) and the host bound kbound * max|M|
     same_grid(cmax_bits);
     FCIB_CUDA(cudaMemsetAsync(c.counter.p + 5, 0, sizeof(int), c.stream));  // tensor-core group timeout flag
-    if (a_g1) launch_group(c, c.c32.p, c.s64a.p, nbs, c.A.ng1, c.A.g1, c.A.g1row.p, c.A.g1lab.p, c.Ha.p, c.n);
-    if (c.A.ng2) launch_group_same_f32(c, c.c32.p, c.s64a.p, nbs, c.A.ng2, c.A.g2, c.A.g2row.p, c.A.g2lab.p, c.M2a.p, np2);
+    auto groups32 = [&](const float* X, unsigned long long* out, const std::vector<GroupSub>& subs, const SpinTables& t,
+                        bool one_body, int ncols, const double* M, int ldm) {
+        auto one = [&](const float* Xb, unsigned long long* Ob, int nc, int ng, int G, const uint32_t* rows,
+                       const uint16_t* labs) {
+            if (one_body) launch_group(c, Xb, Ob, nc, ng, G, rows, labs, M, ldm);
+            else launch_group_same_f32(c, Xb, Ob, nc, ng, G, rows, labs, M, ldm);
+        };
+        if (!y.on) {
+            if (one_body) one(X, out, ncols, t.ng1, t.g1, t.g1row.p, t.g1lab.p);
+            else one(X, out, ncols, t.ng2, t.g2, t.g2row.p, t.g2lab.p);
+            return;
+        }
+        for (const GroupSub& g : subs) one(X + g.blk, out + g.blk, g.ncols, g.ngroups, g.G, y.grow.p + g.off, y.glab.p + g.off);
+    };
+    if (a_g1) groups32(c.c32.p, c.s64a.p, y.a1, c.A, true, nbs, c.Ha.p, c.n);
+    if (c.A.ng2) groups32(c.c32.p, c.s64a.p, y.a2, c.A, false, nbs, c.M2a.p, np2);
     if (any_b) {
         c.ct32.alloc(N);
-        dim3 gridt((nbs + 31) / 32, (nas + 31) / 32), blockt(32, 8);
-        k_transpose_f32<<<gridt, blockt, 0, c.stream>>>(c.c32.p, c.ct32.p, nas, nbs);
-        FCIB_KCHECK();
-        if (b_g1) launch_group(c, c.ct32.p, c.st64.p, nas, c.B.ng1, c.B.g1, c.B.g1row.p, c.B.g1lab.p, c.Hb.p, c.n);
-        if (c.B.ng2) launch_group_same_f32(c, c.ct32.p, c.st64.p, nas, c.B.ng2, c.B.g2, c.B.g2row.p, c.B.g2lab.p, c.M2b.p, np2);
+        transpose_all(c.c32.p, c.ct32.p, [&](const float* in, float* out, int r, int cc) {
+            dim3 gridt((cc + 31) / 32, (r + 31) / 32), blockt(32, 8);
+            k_transpose_f32<<<gridt, blockt, 0, c.stream>>>(in, out, r, cc);
+            FCIB_KCHECK();
+        });
+        if (b_g1) groups32(c.ct32.p, c.st64.p, y.b1, c.B, true, nas, c.Hb.p, c.n);
+        if (c.B.ng2) groups32(c.ct32.p, c.st64.p, y.b2, c.B, false, nas, c.M2b.p, np2);
     }
-    k_add_same_fixed<<<grid2, block2, 0, c.stream>>>(S, c.s64a.p, c.st64.p, nas, nbs, c.counter.p + kSlotSameGrid);
-    FCIB_KCHECK();
+    add_same();
 }
 
 // events bracketing the opposite-spin and same-spin parts of a sigma build
@@ -754,7 +812,7 @@ static void sigma_timing(Context& c, SigmaEvents& ev, bool fp64) {
 
 void sigma_fp64(Context& c, const double* C, double* S) {
     const int nas = (int)c.nas, nbs = (int)c.nbs;
-    const size_t N = (size_t)c.ndet;
+    const size_t N = (size_t)c.nvec;
     ensure_counter(c);
     SigmaEvents ev;
     FCIB_CUDA(cudaEventRecord(ev.e[0], c.stream));
@@ -768,19 +826,36 @@ void sigma_fp64(Context& c, const double* C, double* S) {
         const int kpad = (s1a + 7) / 8 * 8;
         FCIB_CHECK(kpad <= kDmMaxK && c.A.npair <= 2 * kDmNT * 8 && c.B.npair_pad == npp, FCIB_ERR_UNSUPPORTED,
                    "too many orbitals for the FP64 opposite-spin kernel");
-        size_t smem = ab_fp64_smem(nbs, s1a, npp);
-        FCIB_CHECK(smem + 1024 <= (size_t)c.smem_optin, FCIB_ERR_UNSUPPORTED,
-                   "opposite-spin row block exceeds shared memory (beta string count too large)");
-        FCIB_CUDA(cudaFuncSetAttribute(k_ab_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        int per_sm = std::max(1, (int)(c.smem_per_sm / (smem + 1024)));
-        per_sm = std::min(per_sm, 2048 / kDmThreads);
-        int grid = std::min(nas, per_sm * c.num_sms);
-        FCIB_CUDA(cudaMemsetAsync(c.counter.p, 0, sizeof(int), c.stream));
         if (c.vmax <= 0.0f) c.vmax = host_vmax(c);
+        // one grid for every launch of this sigma (the blocked sub-problems have fewer connections)
         const double bound = std::fabs(c.scalar) + (double)c.B.s1 * kpad * (double)c.vmax;
-        k_ab_fp64<<<grid, kDmThreads, smem, c.stream>>>(C, S, c.A.conn.p, s1a, kpad, c.B.tgt.p, npp, c.A.npair, c.V.p,
-                                                        nas, nbs, c.scalar, c.counter.p, cmax64, bound);
-        FCIB_KCHECK();
+        auto launch = [&](const double* Csrc, int lds, int ns, const double* Ct, double* St, int nt, int acc,
+                          const uint32_t* conn, int s1, const int32_t* tgt, int ldt, int npair, const double* V,
+                          int ldv, int rows) {
+            const size_t smem = ab_fp64_smem(nt, s1, 0);
+            FCIB_CHECK(smem + 1024 <= (size_t)c.smem_optin, FCIB_ERR_UNSUPPORTED,
+                       "opposite-spin row block exceeds shared memory (beta string count too large)");
+            FCIB_CUDA(cudaFuncSetAttribute(k_ab_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            int per_sm = std::max(1, (int)(c.smem_per_sm / (smem + 1024)));
+            per_sm = std::min(per_sm, 2048 / kDmThreads);
+            const int grid = std::min(rows, per_sm * c.num_sms);
+            FCIB_CUDA(cudaMemsetAsync(c.counter.p, 0, sizeof(int), c.stream));
+            k_ab_fp64<<<grid, kDmThreads, smem, c.stream>>>(Csrc, lds, ns, Ct, St, nt, acc, conn, s1, (s1 + 7) / 8 * 8,
+                                                            tgt, ldt, npair, V, ldv, rows, c.scalar, c.counter.p, cmax64,
+                                                            bound);
+            FCIB_KCHECK();
+        };
+        if (c.sym.on) {
+            // per target alpha irrep: the g = 0 sub-problem writes the block, the others add to it
+            const SymSpace& y = c.sym;
+            for (const AbSub& u : y.ab) {
+                const int64_t sb = y.d.blk[u.src], tb = y.d.blk[u.ha];
+                launch(C + sb, u.ns, u.ns, C + tb, S + tb, u.nt, u.g != 0 ? 1 : 0, y.conn.p + u.conn, u.kmax,
+                       y.tgt32.p + u.tgt32, y.npg[u.g], y.np_g[u.g], y.Vg.p + y.vg_off[u.g], y.npg[u.g], u.rows);
+            }
+        } else {
+            launch(C, nbs, nbs, C, S, nbs, 0, c.A.conn.p, s1a, c.B.tgt.p, npp, c.A.npair, c.V.p, npp, nas);
+        }
     } else {
         k_scale_copy<<<4 * c.num_sms, 256, 0, c.stream>>>(C, S, c.scalar, N);
         FCIB_KCHECK();
@@ -796,7 +871,7 @@ void ab_tc(Context& c, const double* C, double* S, bool three);
 int tc_check_error(Context& c, bool opposite_spin);
 
 void sigma_mixed(Context& c, const double* C, double* S, bool three) {
-    const size_t N = (size_t)c.ndet;
+    const size_t N = (size_t)c.nvec;
     SigmaEvents ev;
     FCIB_CUDA(cudaEventRecord(ev.e[0], c.stream));
     if (c.fold_h) {
@@ -824,10 +899,18 @@ struct DiagInts {
 };
 __constant__ DiagInts d_diag;
 
+// out in the engine layout: C1 (sd.nirrep = 1) or the blocked layout of sd
 __global__ void k_hdiag(const uint32_t* __restrict__ sa, const uint32_t* __restrict__ sb, int nas,
-                        int nbs, int n, double e0, double* __restrict__ out, size_t N) {
+                        int nbs, int n, double e0, double* __restrict__ out, size_t N, SymDev sd) {
     for (size_t I = blockIdx.x * (size_t)blockDim.x + threadIdx.x; I < N; I += (size_t)gridDim.x * blockDim.x) {
-        uint32_t Ia = sa[I / nbs], Ib = sb[I % nbs];
+        int ia, ib;
+        if (sd.nirrep > 1) {
+            sym_decode(sd, (int64_t)I, ia, ib);
+        } else {
+            ia = (int)(I / nbs);
+            ib = (int)(I % nbs);
+        }
+        uint32_t Ia = sa[ia], Ib = sb[ib];
         double e = e0;
         uint32_t a = Ia;
         while (a) {
@@ -880,7 +963,7 @@ void compute_hdiag(Context& c, double* out) {
     }
     FCIB_CUDA(cudaMemcpyToSymbolAsync(d_diag, &d, sizeof(d), 0, cudaMemcpyHostToDevice, c.stream));
     k_hdiag<<<8 * c.num_sms, 256, 0, c.stream>>>(c.A.str.p, c.B.str.p, (int)c.nas, (int)c.nbs, n,
-                                                c.scalar, out, (size_t)c.ndet);
+                                                c.scalar, out, (size_t)c.nvec, sym_dev(c));
     FCIB_KCHECK();
 }
 

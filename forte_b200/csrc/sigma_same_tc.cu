@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(kGtThreads, 2)
 #pragma unroll
             for (int u = 0; u < 4; u++) {
                 const int j = 4 * (cg + 4 * i) + u;
-                off[i][u] = j < G ? (rs[j] & kConnIdxMask) * (uint32_t)ncols : kGtNoRow;
+                off[i][u] = (j < G && rs[j] != kNullRow) ? (rs[j] & kConnIdxMask) * (uint32_t)ncols : kGtNoRow;
             }
         // X-tile gather, one tile ahead in registers (coalesced across lanes)
         float xv[Q][4];

@@ -212,6 +212,9 @@ constexpr int kMagicBits = 0x4B400000;      // bit pattern of kMagic
 // Plane rows are padded to whole tiles (zeros) and the target table to whole tiles (no target), so
 // neither the gather nor the scatter checks bounds.  Per tile: one mbarrier wait and one block
 // barrier.
+// Source rows (plane, ns beta strings) and target rows (C, S: nt beta strings) have their own
+// lengths, so one launch also serves a sub-problem of the irrep-blocked layout; ndiag = 0 drops the
+// diagonal pairs and accumulate = 1 adds the row to S instead of writing E0 C + the product.
 // NW warps: NW / 4 column groups per TMEM lane quarter.  Gather chunks of column group cg: cg + NCG j
 // (at 16 warps the third round goes to group 3 - cg, which holds one epilogue chunk fewer);
 // off-diagonal epilogue chunks: (NCG - 1 - cg) + NCG i; the diagonal chunks go to group 0.
@@ -223,14 +226,15 @@ __device__ __forceinline__ int tc_gather_chunk(int cg, int j) {
 
 template <bool THREE, int NW>
 __global__ void __launch_bounds__(NW * 32, 1)
-    k_ab_tc(const float2* __restrict__ Phl, int ldp, const double* __restrict__ C,
-            double* __restrict__ S, const uint32_t* __restrict__ connA, int s1a, const uint16_t* __restrict__ tgtR,
-            int npair, const int* __restrict__ perm, int noff8, int n, const uint32_t* __restrict__ bstr, int kb,
+    k_ab_tc(const float2* __restrict__ Phl, int ldp, int ns, const double* __restrict__ C, double* __restrict__ S,
+            int nt, int accumulate, const uint32_t* __restrict__ connA, int s1a, const uint16_t* __restrict__ tgtR,
+            int npair, const int* __restrict__ perm, int noff8, int ndiag, const uint32_t* __restrict__ bstr, int kb,
             const double* __restrict__ V, int ldv, float vmax, const unsigned int* __restrict__ cmax_bits,
-            int nas, int nbs, int ncontrib, double e0, int* __restrict__ row_counter, int* __restrict__ err) {
+            int nas, int ncontrib, const uint8_t* __restrict__ mag, double e0, int* __restrict__ row_counter,
+            int* __restrict__ err) {
     extern __shared__ __align__(128) unsigned char tc_smem[];
     unsigned char* smem = tc_smem;
-    const TcLayout L = tc_layout(s1a, npair, nbs, THREE);
+    const TcLayout L = tc_layout(s1a, npair, nt, THREE);
     unsigned char* Bhi = smem + L.off_bhi;
     unsigned char* Blo = smem + L.off_blo;
     int* acc_hi = reinterpret_cast<int*>(smem);
@@ -277,8 +281,9 @@ __global__ void __launch_bounds__(NW * 32, 1)
     const int el = min(60, (int)floorf(44.0f - log2f(ybound)));
     const double inv_grid = ldexp(1.0, -el);
     const double grid = ldexp(1.0, el);
-    // every element receives exactly ncontrib contributions: kb (n - kb) off-diagonal ones and the
-    // diagonal sum of its own string; ncontrib * kMagicBits is removed once per element (mod 2^32)
+    // every element receives exactly ncontrib contributions (C1 layout: kb (n - kb) off-diagonal ones and
+    // the diagonal sum of its own string; blocked sub-problems: mag[element]); that many kMagicBits are
+    // removed once per element (mod 2^32)
     const unsigned magic_total = (unsigned)ncontrib * (unsigned)kMagicBits;
 
     // instruction descriptor: D f32, A/B tf32, both K-major, N = npad, M = 128
@@ -288,10 +293,10 @@ __global__ void __launch_bounds__(NW * 32, 1)
     const uint32_t acc_s = smem_u32(acc_hi);
 
     uint32_t mma_count[2] = {0u, 0u};  // commits issued per accumulator (parity tracking)
-    const int ntiles = (nbs + kTcM - 1) / kTcM;
+    const int ntiles = (ns + kTcM - 1) / kTcM;
     const int nk8 = kpad / 8;
     const int nn8 = noff8 / 8;        // accumulator chunks of off-diagonal pairs
-    const int ndc = (n + 7) / 8;      // accumulator chunks of the diagonal pairs (r,r), after them
+    const int ndc = (ndiag + 7) / 8;  // accumulator chunks of the diagonal pairs (r,r), after them
     const unsigned char* pbase = reinterpret_cast<const unsigned char*>(Phl);
 
     float gh[GJ][8], gl[GJ][8];
@@ -326,7 +331,7 @@ __global__ void __launch_bounds__(NW * 32, 1)
             cs[k] = e;
             koff[k] = (e & kConnIdxMask) * (uint32_t)ldp * (uint32_t)sizeof(float2);
         }
-        for (int j = tid; j < nbs; j += blockDim.x) {
+        for (int j = tid; j < nt; j += blockDim.x) {
             acc_hi[j] = 0;
             acc_lo[j] = 0u;
         }
@@ -364,7 +369,7 @@ __global__ void __launch_bounds__(NW * 32, 1)
             uint4 tg[EB];
 #pragma unroll
             for (int i = 0; i < EB; i++) tg[i] = load_tg(i);
-            const uint32_t occ_epi = (cg == 0 && t >= 1 && jb_epi < nbs) ? __ldg(bstr + jb_epi) : 0u;
+            const uint32_t occ_epi = (cg == 0 && ndiag > 0 && t >= 1 && jb_epi < ns) ? __ldg(bstr + jb_epi) : 0u;
             // (a) the TMEM A buffer and accumulator prv are ready once tile t-1's MMAs completed
             if (t >= 1 && !mbar_wait_bounded(&bars[prv], (mma_count[prv] - 1) & 1)) {
                 atomicCAS(err, 0, kErrTimeoutMma);
@@ -456,7 +461,7 @@ __global__ void __launch_bounds__(NW * 32, 1)
                     tmem_wait_ld8(rv);
                     scatter(rv, tg2);
                 }
-                if (cg == 0) {
+                if (cg == 0 && ndiag > 0) {
                     // diagonal pairs (r,r): F_rr Jb = Jb for every occupied r, so the string's own
                     // element receives sum_{r occupied} T[Jb][(r,r)], added in FP32 in a fixed order
                     // and reduced as one contribution
@@ -469,8 +474,8 @@ __global__ void __launch_bounds__(NW * 32, 1)
                     float d = 0.f;
 #pragma unroll
                     for (int r = 0; r < 16; r++)
-                        if (r < n && ((occ >> r) & 1u)) d += __uint_as_float(rd[r >> 3][r & 7]);
-                    add_fixed(d, acc_s + (uint32_t)jb_epi * 4u, jb_epi < nbs ? 0u : 0xFFFFu);
+                        if (r < ndiag && ((occ >> r) & 1u)) d += __uint_as_float(rd[r >> 3][r & 7]);
+                    add_fixed(d, acc_s + (uint32_t)jb_epi * 4u, jb_epi < ns ? 0u : 0xFFFFu);
                 }
             }
             tc_fence_before();
@@ -478,12 +483,13 @@ __global__ void __launch_bounds__(NW * 32, 1)
         if (s_abort) break;
         __syncthreads();
         // (e) sigma row = E0 * C row + opposite-spin part (exact fixed-point sum -> FP64)
-        const double* Crow = C + (size_t)Ia * nbs;
-        double* Srow = S + (size_t)Ia * nbs;
-        for (int j = tid; j < nbs; j += blockDim.x) {
-            const int hi = (int)((unsigned)acc_hi[j] - magic_total), lo = (int)(acc_lo[j] - magic_total);
+        const double* Crow = C + (size_t)Ia * nt;
+        double* Srow = S + (size_t)Ia * nt;
+        for (int j = tid; j < nt; j += blockDim.x) {
+            const unsigned mt = mag ? (unsigned)mag[j] * (unsigned)kMagicBits : magic_total;
+            const int hi = (int)((unsigned)acc_hi[j] - mt), lo = (int)(acc_lo[j] - mt);
             const long long tot = ((long long)hi << kFixLoBits) + (long long)lo;
-            Srow[j] = e0 * Crow[j] + (double)tot * inv_grid;
+            Srow[j] = (accumulate ? Srow[j] : e0 * Crow[j]) + (double)tot * inv_grid;
         }
     }
     // drain: wait (bounded) for any MMA still in flight before releasing tensor memory
@@ -555,22 +561,68 @@ float host_vmax(Context& c) {
 void ab_tc(Context& c, const double* C, double* S, bool three) {
     const int nas = (int)c.nas, nbs = (int)c.nbs;
     const int s1a = c.A.s1;
-    FCIB_CHECK(nbs <= kMaxBetaStrings, FCIB_ERR_UNSUPPORTED, "tensor-core opposite-spin kernel: too many beta strings");
+    const int n = c.n, kb = c.nb;
+    const SymSpace& y = c.sym;
+    if (c.vmax <= 0.0f) c.vmax = host_vmax(c);
+    ensure_counter(c);
+    FCIB_CUDA(cudaMemsetAsync(c.counter.p, 0, 3 * sizeof(int), c.stream));
+    unsigned int* cmax_bits = reinterpret_cast<unsigned int*>(c.counter.p + 3);
+    FCIB_CUDA(cudaMemsetAsync(cmax_bits, 0, sizeof(unsigned int), c.stream));
+    auto kern = three ? k_ab_tc<true, kTcWarps> : k_ab_tc<false, kTcWarps>;
+    // shared memory of one launch: one CTA per SM (it owns all tensor memory)
+    auto smem_of = [&](int s1, int ncol, int nt, int noff8, int ndiag) {
+        const TcLayout L = tc_layout(s1, ncol, nt, three);
+        FCIB_CHECK(nt <= kMaxBetaStrings, FCIB_ERR_UNSUPPORTED, "tensor-core opposite-spin kernel: too many beta strings");
+        FCIB_CHECK(L.npad <= 144 && L.kpad <= 72 && noff8 / 8 <= 15 && ndiag <= 16 && L.kpad / 8 <= 9,
+                   FCIB_ERR_UNSUPPORTED, "tensor-core kernel: more than 16 active orbitals");
+        const size_t smem = std::max<size_t>(L.total, 120 * 1024);
+        FCIB_CHECK(smem + 2048 <= (size_t)c.smem_optin, FCIB_ERR_UNSUPPORTED,
+                   "tensor-core kernel: sigma row and integral block exceed shared memory");
+        FCIB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        return smem;
+    };
+    c.tc_ev.ensure();
+    if (y.on) {
+        // blocked layout: TF32 planes per alpha block, one launch per (target irrep, pair irrep)
+        c.tf_hi.alloc(2 * std::max<size_t>(y.plane_total, 1));
+        c.c32.alloc((size_t)c.nvec);
+        float2* hl = reinterpret_cast<float2*>(c.tf_hi.p);
+        for (int h = 0; h < c.nirrep; h++) {
+            const int nb_h = y.bcnt[h ^ c.irrep];
+            if (y.acnt[h] == 0 || nb_h == 0) continue;
+            k_split_tf32<<<8 * c.num_sms, 256, 0, c.stream>>>(C + y.d.blk[h], hl + y.plane_off[h], c.c32.p + y.d.blk[h],
+                                                              y.acnt[h], nb_h, y.ldp[h], cmax_bits);
+            FCIB_KCHECK();
+        }
+        c.c32_ready = true;
+        FCIB_CUDA(cudaEventRecord(c.tc_ev.e[0], c.stream));
+        for (const AbSub& u : y.ab) {
+            const int g = u.g, noff8 = y.noff8_g[g], ndiag = y.ndiag_g[g];
+            const int ncol = noff8 + ndiag;
+            const size_t smem = smem_of(u.kmax, ncol, u.nt, noff8, ndiag);
+            FCIB_CUDA(cudaMemsetAsync(c.counter.p, 0, sizeof(int), c.stream));  // row counter (errors stay)
+            const int64_t tb = y.d.blk[u.ha];
+            kern<<<std::min(u.rows, c.num_sms), kTcWarps * 32, smem, c.stream>>>(
+                hl + y.plane_off[u.src], y.ldp[u.src], u.ns, C + tb, S + tb, u.nt, g != 0 ? 1 : 0, y.conn.p + u.conn,
+                u.kmax, y.tgt16.p + u.tgt16, ncol, y.perm.p + y.perm_off[g], noff8, ndiag,
+                y.bstr_sorted.p + y.d.boff[u.ha ^ c.irrep ^ g], kb, y.Vz.p, y.npp, c.vmax, cmax_bits, u.rows, 0,
+                y.mag.p + u.mag, c.scalar, c.counter.p, c.counter.p + 1);
+            FCIB_KCHECK();
+        }
+        FCIB_CUDA(cudaEventRecord(c.tc_ev.e[1], c.stream));
+        c.tc_recorded = true;
+        return;
+    }
     // columns: the n(n-1)/2 off-diagonal pairs in pair order (padded to a multiple of 8), then the n
     // diagonal pairs (r,r)
-    const int n = c.n;
     const int noff = n * (n - 1) / 2, noff8 = (noff + 7) / 8 * 8;
     const int ncol = noff8 + n;
-    TcLayout L = tc_layout(s1a, ncol, nbs, three);
-    FCIB_CHECK(L.npad <= 144 && L.kpad <= 72 && noff8 / 8 <= 15 && n <= 16 && L.kpad / 8 <= 9,
-               FCIB_ERR_UNSUPPORTED, "tensor-core kernel: more than 16 active orbitals");
+    const size_t smem = smem_of(s1a, ncol, nbs, noff8, n);
+    const TcLayout L = tc_layout(s1a, ncol, nbs, three);
     const int ntiles = (nbs + kTcM - 1) / kTcM;
     const int ldp = ntiles * kTcM;  // plane rows padded to whole tiles (zeros)
     FCIB_CHECK((uint64_t)nas * ldp * sizeof(float2) < (1ull << 32), FCIB_ERR_UNSUPPORTED,
                "tensor-core kernel: TF32 planes exceed the 32-bit gather offsets");
-    size_t smem = std::max<size_t>(L.total, 120 * 1024);  // one CTA per SM (owns all tensor memory)
-    FCIB_CHECK(smem + 2048 <= (size_t)c.smem_optin, FCIB_ERR_UNSUPPORTED,
-               "tensor-core kernel: sigma row and integral block exceed shared memory");
     if (!c.tgtR16.p) {
         std::vector<int> perm(L.npad, -1);
         for (int p = 0, col = 0; p < n; p++)
@@ -582,26 +634,18 @@ void ab_tc(Context& c, const double* C, double* S, bool three) {
                                                           c.tc_perm.p, noff8, L.npad);
         FCIB_KCHECK();
     }
-    if (c.vmax <= 0.0f) c.vmax = host_vmax(c);
     c.tf_hi.alloc(2 * (size_t)nas * ldp);  // interleaved hi/lo pairs
-    ensure_counter(c);
-    FCIB_CUDA(cudaMemsetAsync(c.counter.p, 0, 3 * sizeof(int), c.stream));
-    unsigned int* cmax_bits = reinterpret_cast<unsigned int*>(c.counter.p + 3);
-    FCIB_CUDA(cudaMemsetAsync(cmax_bits, 0, sizeof(unsigned int), c.stream));
     c.c32.alloc((size_t)nas * nbs);
     float2* hl = reinterpret_cast<float2*>(c.tf_hi.p);
     k_split_tf32<<<8 * c.num_sms, 256, 0, c.stream>>>(C, hl, c.c32.p, nas, nbs, ldp, cmax_bits);
     FCIB_KCHECK();
     c.c32_ready = true;
-    auto kern = three ? k_ab_tc<true, kTcWarps> : k_ab_tc<false, kTcWarps>;
-    FCIB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int grid = std::min(nas, c.num_sms);
-    c.tc_ev.ensure();
+    const int grid = std::min(nas, c.num_sms);
     FCIB_CUDA(cudaEventRecord(c.tc_ev.e[0], c.stream));
-    const int kb = c.nb;
-    kern<<<grid, kTcWarps * 32, smem, c.stream>>>(hl, ldp, C, S, c.A.conn.p, s1a, c.tgtR16.p, ncol, c.tc_perm.p, noff8,
-                                              n, c.B.str.p, kb, c.V.p, c.A.npair_pad, c.vmax, cmax_bits, nas, nbs,
-                                              kb * (n - kb) + 1, c.scalar, c.counter.p, c.counter.p + 1);
+    kern<<<grid, kTcWarps * 32, smem, c.stream>>>(hl, ldp, nbs, C, S, nbs, 0, c.A.conn.p, s1a, c.tgtR16.p, ncol,
+                                                  c.tc_perm.p, noff8, n, c.B.str.p, kb, c.V.p, c.A.npair_pad, c.vmax,
+                                                  cmax_bits, nas, kb * (n - kb) + 1, nullptr, c.scalar, c.counter.p,
+                                                  c.counter.p + 1);
     FCIB_KCHECK();
     FCIB_CUDA(cudaEventRecord(c.tc_ev.e[1], c.stream));
     c.tc_recorded = true;

@@ -45,6 +45,7 @@ DEFAULT_OPTIONS = {
     "FCI_MIXED_SWITCH": 1.0e-4,
     "FCI_SAME_SPIN": "TC",          # TC | CUDA_CORES (mixed modes)
     "CI_SPIN_ADAPT": False,         # solve in the spin sector of the state's multiplicity
+    "FCI_SYM_BLOCKED": True,        # with symmetry: vectors over the target irrep's blocks only
 }
 
 
@@ -121,6 +122,7 @@ class FCISolver:
         o.mixed_switch = float(d["FCI_MIXED_SWITCH"])
         o.same_spin_kernel = {"TC": capi.SAME_TC, "CUDA_CORES": capi.SAME_CUDA_CORES}[str(d["FCI_SAME_SPIN"]).upper()]
         o.spin_adapt = 1 if d["CI_SPIN_ADAPT"] else 0
+        o.sym_blocked = 1 if d["FCI_SYM_BLOCKED"] else 0
         if o.preconditioner == capi.PRECOND_MLP and getattr(self, "_mlp", None) is None:
             from .learned_precond import load_weights
             self.set_mlp_weights(load_weights())

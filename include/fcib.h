@@ -4,7 +4,10 @@
  * Plain C types only (no CUDA or torch types).  Every function returns FCIB_OK (0) or a
  * negative error code; fcib_last_error() returns the calling thread's last message.
  * Host-buffer entry points take and return host memory; *_device entry points take device
- * pointers in the engine's C1 layout and a CUDA stream handle passed as void*.
+ * pointers in the engine's layout and a CUDA stream handle passed as void*.  The engine's layout
+ * is the C1 layout (na_str x nb_str row-major) without point-group symmetry; with symmetry it is
+ * FCIVector flat order (fcib_size elements, the target irrep's blocks only) by default, or the C1
+ * layout with zeros outside the target irrep when fcib_options.sym_blocked = 0.
  *
  * Each entry point replaces a piece of Forte's FCISolver path (paths relative to the Forte
  * project root):
@@ -70,6 +73,8 @@ typedef struct fcib_options {
     int same_spin_kernel;      /* mixed modes: FCIB_SAME_TC (default) or FCIB_SAME_CUDA_CORES */
     int spin_adapt;            /* CI_SPIN_ADAPT: keep the Davidson space in the spin sector of the
                                   state's multiplicity (projection onto its CSFs); default 0 */
+    int sym_blocked;           /* nirrep > 1: vectors and sigma cover only the target irrep's blocks
+                                  (FCIVector flat order, default 1); 0 = the full C1 space with a mask */
 } fcib_options;
 
 typedef struct fcib_ctx fcib_ctx;
@@ -119,7 +124,7 @@ int fcib_max_abs_elements(fcib_ctx* ctx, int root, int num_dets, double* abs_c, 
                           int64_t* alfa_address, int64_t* beta_address, int* count);
 /* sigma = H b for a host vector in FCIVector flat order */
 int fcib_sigma(fcib_ctx* ctx, const double* b, double* sigma);
-/* sigma for device vectors in the engine's C1 layout (na_str x nb_str row-major), on a
+/* sigma for device vectors in the engine's layout (see the top of this file), on a
  * stream (void* = cudaStream_t, NULL = the context's stream); precision = FCIB_PREC_* */
 int fcib_sigma_device(fcib_ctx* ctx, const double* d_b, double* d_sigma, int precision, void* stream);
 /* diagonal of H in FCIVector flat order */
@@ -191,7 +196,7 @@ int fcib_mlp_train(int device, int64_t n, const uint32_t* ea, const uint32_t* eb
  * context's preconditioner option: out = r / (lambda - H_II) (0 when |lambda - H_II| <= 1e-6),
  * rescaled by the network when preconditioner = FCIB_PRECOND_MLP; host vectors in flat order */
 int fcib_precondition(fcib_ctx* ctx, const double* r, double lambda, double* out);
-/* keep the raw residual of root 0 (C1 layout) and its Ritz value at every Davidson iteration of
+/* keep the raw residual of root 0 (engine layout) and its Ritz value at every Davidson iteration of
  * later solves, up to max_vectors (0 = off); read them back by index (index < 0: count only) */
 int fcib_set_residual_capture(fcib_ctx* ctx, int max_vectors);
 int fcib_captured_residual(fcib_ctx* ctx, int index, double* r, double* lambda, int* count);
@@ -251,7 +256,7 @@ int fcib_get_profile(fcib_ctx* ctx, fcib_profile* out);
 /* the CUDA stream (cudaStream_t as void*) the engine launches on */
 int fcib_stream(fcib_ctx* ctx, void** stream);
 
-/* <S^2> of a device vector in the engine's C1 layout, allocating nothing.  For callers that
+/* <S^2> of a device vector in the engine's layout, allocating nothing.  For callers that
  * cannot call cudaMalloc: a host whose memory pool already owns the GPU, or a loop that must
  * not pay for an allocation's device synchronisation or risk its failure.  No device or host
  * buffers are created; the reduction scratch is a static per-device array of 598,600 bytes
@@ -262,8 +267,8 @@ int fcib_stream(fcib_ctx* ctx, void** stream);
  * cudaDeviceReset the module is loaded at a new address), so make the first call after a reset
  * before any capture too.  The context's string tables must already exist (FCIB_ERR_STATE
  * otherwise); a launch needing more than 1024 blocks returns FCIB_ERR_UNSUPPORTED.  Calls on one
- * device that overlap on the GPU race on the shared scratch: serialise them.  d_c is in the C1
- * layout (zeros outside the target irrep when the state has symmetry).  stream: cudaStream_t as
+ * device that overlap on the GPU race on the shared scratch: serialise them.  d_c is in the
+ * engine's layout (see the top of this file).  stream: cudaStream_t as
  * void*, NULL = the context's stream, which is a non-blocking stream and so is NOT ordered after
  * the legacy default stream or the caller's streams: either pass the stream that wrote d_c, or
  * make sure d_c is complete before the call.  The call synchronizes the stream it runs on.  No

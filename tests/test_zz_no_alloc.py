@@ -106,21 +106,23 @@ def test_noalloc_on_caller_stream():
 
 
 def test_noalloc_with_symmetry_golden_c2v():
-    """C2v golden CAS (784 determinants in the A1 block): the device vector is in the C1 layout
-    with zeros outside the target irrep; the value equals fcib_spin2 on the flat-order vector."""
+    """C2v golden CAS (784 determinants in the A1 block): with the blocked layout (the default) the
+    device vector is the flat-order vector itself; with FCI_SYM_BLOCKED off it is in the C1 layout
+    with zeros outside the target irrep.  Both equal fcib_spin2 on the flat-order vector."""
     import torch
 
     import golden_cases
 
     ints, na, nb, irrep, mult, ref_e = golden_cases.load(1)
-    s = FCISolver(StateInfo(na, nb, mult, na - nb, irrep), 1, ints)
-    s.compute_energy()
-    flat = s.evecs()[0]
-    assert flat.size == 784
-    ref = s.compute_spin2(flat)
-    full = _c1_from_flat(s, ints.orbsym, irrep, flat)
-    d = torch.from_numpy(full).cuda()
-    torch.cuda.synchronize()
-    got = [_noalloc(s, d) for _ in range(2)]
-    assert got == [ref, ref]
-    assert abs(ref - 0.25 * (mult * mult - 1)) < 1e-6
+    for blocked in (True, False):
+        s = FCISolver(StateInfo(na, nb, mult, na - nb, irrep), 1, ints, {"FCI_SYM_BLOCKED": blocked})
+        s.compute_energy()
+        flat = s.evecs()[0]
+        assert flat.size == 784
+        ref = s.compute_spin2(flat)
+        dev = flat if blocked else _c1_from_flat(s, ints.orbsym, irrep, flat)
+        d = torch.from_numpy(np.ascontiguousarray(dev)).cuda()
+        torch.cuda.synchronize()
+        got = [_noalloc(s, d) for _ in range(2)]
+        assert got == [ref, ref]
+        assert abs(ref - 0.25 * (mult * mult - 1)) < 1e-6
