@@ -555,6 +555,8 @@ def run_batch(args, world, rank, local):
     # end to end: integrals from host memory to energies back, through the public API
     t1 = time.perf_counter()
     b2 = BatchSolver(inst, nroot=4, options=opts, device=local)
+    if tuned:
+        b2.set_shape(tuned["threads"], tuned["pair_tile"], tuned["cluster"])
     e2, it2, cv2, _ = b2.solve()
     e2e_s = allmax(world, time.perf_counter() - t1)
     h2d = sum(sum(getattr(x[0], k).nbytes for k in ("oei_a", "oei_b", "tei_aa", "tei_ab", "tei_bb")) for x in inst)

@@ -68,13 +68,20 @@ class BatchSolver:
                                                cv.ctypes.data_as(C.POINTER(C.c_int)), C.byref(ms)))
         return e, it, cv.astype(bool), ms.value
 
+    def set_shape(self, threads=512, pair_tile=32, cluster=2):
+        """Launch shape of later solves: threads per CTA, opposite-spin sigma tile, CTAs per instance."""
+        capi.check(capi.lib().fcib_batch_set_shape(self._h, threads, pair_tile, cluster))
+
     def tune(self):
-        """Autotuner: opposite-spin sigma tile (pairs per work item) x launch shape; keeps the fastest."""
+        """Autotuner: opposite-spin sigma tile (pairs per work item) x launch shape (threads per CTA x
+        CTAs per instance, a thread-block cluster); keeps the fastest."""
         t = C.c_int()
         c = C.c_int()
         p = C.c_int()
+        cl = C.c_int()
         times = np.zeros(12)
-        capi.check(capi.lib().fcib_batch_tune(self._h, C.byref(t), C.byref(c), C.byref(p), capi.dptr(times)))
-        names = [f"tile{tile}_{shape}" for tile in (8, 16, 32) for shape in ("256x1", "512x1", "256x2", "128x2")]
-        return {"threads": t.value, "ctas_per_sm": c.value, "pair_tile": p.value,
+        capi.check(capi.lib().fcib_batch_tune(self._h, C.byref(t), C.byref(c), C.byref(p), C.byref(cl),
+                                              capi.dptr(times)))
+        names = [f"tile{tile}_{shape}" for tile in (8, 16, 32) for shape in ("256x1", "512x1", "256x2", "512x2")]
+        return {"threads": t.value, "ctas_per_sm": c.value, "pair_tile": p.value, "cluster": cl.value,
                 "times_ms": dict(zip(names, times.tolist()))}

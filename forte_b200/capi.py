@@ -116,7 +116,9 @@ SIGNATURES = {
                                     C.POINTER(_dp), C.POINTER(_dp), C.c_int, C.POINTER(FcibOptions)]),
     "fcib_batch_destroy": (C.c_int, [_vp]),
     "fcib_batch_solve": (C.c_int, [_vp, _dp, C.POINTER(C.c_int), C.POINTER(C.c_int), _dp]),
-    "fcib_batch_tune": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), _dp]),
+    "fcib_batch_set_shape": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int]),
+    "fcib_batch_tune": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                  C.POINTER(C.c_int), _dp]),
     "fcib_captured_residual": (C.c_int, [_vp, C.c_int, _dp, _dp, C.POINTER(C.c_int)]),
     "fcib_fp64_peak": (C.c_int, [C.c_int, _dp, _dp]),
     "fcib_transition_rdms": (C.c_int, [_vp, C.c_int, _vp, C.c_int, C.c_int, C.c_int, _dp, _dp]),

@@ -22,6 +22,15 @@
 // precision the FP32 iteration's convergence triggers a restart from the nroot Ritz vectors with
 // FP64 sigma, and only the FP64 iteration's convergence ends the solve.
 // Guess: unit vectors on the 2 * nroot lowest diagonal elements (no spin selection).
+// Several CTAs can share an instance as a thread-block cluster (csize CTAs, autotuned 1 or 2): CTA
+// crank owns the vector elements I = crank * nth + tid (mod csize * nth), every csize-th sigma row
+// and a contiguous share of the same-spin lines; partial sums are combined through distributed
+// shared memory in rank order, so every CTA of the cluster holds the same reduced values and takes
+// the same branches.  Cluster barriers separate the phases whose data cross CTAs: before each sigma
+// (basis vectors written by all CTAs), between its opposite-spin, alpha and beta same-spin parts,
+// and at every partial-sum combination.
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <memory>
 
@@ -61,10 +70,23 @@ struct BatchShared {  // per-CTA shared scalars
     double red[(kBMaxThreads / 32) * kBMaxSub];
     int chosen[2 * kBMaxRoot];
     int inst, nb, nsig, added;
+    double part[2][kBMaxSub];  // this CTA's partial sums, read by the cluster's other CTAs
 };
 
-// sum over the CTA of v[0..K) (K <= kBMaxSub); results in S.out
-__device__ __forceinline__ void bsum(double (&v)[kBMaxSub], int K, BatchShared& S) {
+// the cluster sharing an instance: size CTAs, this CTA's rank, the partial-sum buffer in turn
+struct CInfo {
+    int size, rank, pb;
+};
+// every thread of every CTA of the cluster (a block barrier when the cluster is one CTA)
+__device__ __forceinline__ void csync(const CInfo& ci) {
+    if (ci.size > 1) cooperative_groups::this_cluster().sync();
+    else __syncthreads();
+}
+
+// sum over the cluster of v[0..K) (K <= kBMaxSub); results in S.out of every CTA.  The partial
+// buffers alternate between calls: a CTA writes a buffer again only after the barrier of the next
+// call, which every other CTA reaches after reading it.
+__device__ __forceinline__ void bsum(double (&v)[kBMaxSub], int K, BatchShared& S, CInfo& ci) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
     for (int k = 0; k < kBMaxSub; k++) {
@@ -78,25 +100,39 @@ __device__ __forceinline__ void bsum(double (&v)[kBMaxSub], int K, BatchShared& 
     for (int k = threadIdx.x; k < K; k += blockDim.x) {
         double s = 0.0;
         for (int i = 0; i < nw; i++) s += S.red[i * kBMaxSub + k];
-        S.out[k] = s;
+        if (ci.size == 1) S.out[k] = s;
+        else S.part[ci.pb][k] = s;
+    }
+    if (ci.size > 1) {
+        auto cl = cooperative_groups::this_cluster();
+        cl.sync();
+        for (int k = threadIdx.x; k < K; k += blockDim.x) {
+            double t = 0.0;
+            for (int r = 0; r < ci.size; r++) t += cl.map_shared_rank(&S.part[ci.pb][0], r)[k];
+            S.out[k] = t;
+        }
+        ci.pb ^= 1;
     }
     __syncthreads();
 }
 
-// S.out[j] = <x, B_j> for j < nb
-__device__ void bdots(const double* __restrict__ x, const double* __restrict__ B, size_t N, int nb, BatchShared& S) {
+// S.out[j] = <x, B_j> for j < nb.  x may be a sigma vector that other CTAs of the cluster wrote, so
+// its loads stay coherent (not __restrict__).
+__device__ void bdots(const double* x, const double* __restrict__ B, size_t N, int nb, BatchShared& S, CInfo& ci) {
     double acc[kBMaxSub];
 #pragma unroll
     for (int j = 0; j < kBMaxSub; j++) acc[j] = 0.0;
-    for (size_t I = threadIdx.x; I < N; I += blockDim.x) {
+    for (size_t I = (size_t)ci.rank * blockDim.x + threadIdx.x; I < N; I += (size_t)ci.size * blockDim.x) {
         const double xi = x[I];
 #pragma unroll
         for (int j = 0; j < kBMaxSub; j++)
             if (j < nb) acc[j] = fma(B[(size_t)j * N + I], xi, acc[j]);
     }
-    bsum(acc, nb, S);
+    bsum(acc, nb, S, ci);
 }
 
+// c is not __restrict__: the other CTAs of a cluster write it during the kernel, so its loads must
+// stay coherent (no read-only cache path).
 // sigma of one instance by the whole CTA, FP64 in and out, products and sums in T (float in the
 // mixed phase, double otherwise).  scratch: shared memory for the pair block B[k][R] (T), the sigma
 // row (double) and the row's connections; grp: a same-spin group's rows and labels.
@@ -109,8 +145,8 @@ __device__ void bdots(const double* __restrict__ x, const double* __restrict__ B
 // RC: pairs per work item in the opposite-spin term (the autotuned sigma tile: 8, 16 or 32)
 template <typename T, int RC>
 __device__ void bsigma(const BatchInst& P, const double* __restrict__ V, const double* __restrict__ Ma,
-                       const double* __restrict__ Mb, const double* __restrict__ c, double* __restrict__ s,
-                       unsigned char* __restrict__ scratch, int* __restrict__ grp) {
+                       const double* __restrict__ Mb, const double* c, double* __restrict__ s,
+                       unsigned char* __restrict__ scratch, int* __restrict__ grp, const CInfo& ci) {
     const int nbs = P.nbs, nas = P.nas, npp = P.npp, npl = P.npl, s1a = P.s1a;
     const int tid = threadIdx.x, nth = blockDim.x;
     const int nch = (npp + RC - 1) / RC;
@@ -118,7 +154,7 @@ __device__ void bsigma(const BatchInst& P, const double* __restrict__ V, const d
     T* Bt = reinterpret_cast<T*>(scratch);
     double* srow = reinterpret_cast<double*>(scratch + (((size_t)s1a * ldb * sizeof(T) + 15) / 16) * 16);
     uint32_t* cs = reinterpret_cast<uint32_t*>(srow + nbs);
-    for (int ia = 0; ia < nas; ia++) {
+    for (int ia = ci.rank; ia < nas; ia += ci.size) {  // every csize-th row
         for (int k = tid; k < s1a; k += nth) cs[k] = P.conna[(size_t)ia * s1a + k];
         for (int j = tid; j < nbs; j += nth) srow[j] = P.scalar * c[(size_t)ia * nbs + j];
         __syncthreads();
@@ -169,11 +205,15 @@ __device__ void bsigma(const BatchInst& P, const double* __restrict__ V, const d
         for (int j = tid; j < nbs; j += nth) s[(size_t)ia * nbs + j] = srow[j];
         __syncthreads();
     }
+    csync(ci);  // every row written before the same-spin terms add to them
     // same-spin terms over the (N-2)-electron groups
     T* W = reinterpret_cast<T*>(scratch);  // [kBMaxG][kBMaxG], reuses the opposite-spin scratch
     for (int spin = 0; spin < 2; spin++) {
         const int ng = spin ? P.ng2b : P.ng2a;
-        if (!ng) continue;
+        if (!ng) {
+            csync(ci);
+            continue;
+        }
         const int m = spin ? P.g2b : P.g2a;
         const uint32_t* growp = spin ? P.g2rb : P.g2ra;
         const uint16_t* glabp = spin ? P.g2lb : P.g2la;
@@ -194,7 +234,10 @@ __device__ void bsigma(const BatchInst& P, const double* __restrict__ V, const d
                 W[i * kBMaxG + j] = (T)M[(size_t)labs_s[i] * npl + labs_s[j]];
             }
             __syncthreads();
-            for (int line = tid; line < nlines; line += nth) {
+            // this CTA's contiguous share of the lines
+            const int l0 = (int)((long long)ci.rank * nlines / ci.size);
+            const int l1 = (int)((long long)(ci.rank + 1) * nlines / ci.size);
+            for (int line = l0 + tid; line < l1; line += nth) {
                 const double* cl = c + (size_t)line * lstep;
                 double* sl = s + (size_t)line * lstep;
                 T x[kBMaxG];
@@ -220,6 +263,7 @@ __device__ void bsigma(const BatchInst& P, const double* __restrict__ V, const d
             }
             __syncthreads();
         }
+        csync(ci);  // alpha lines (columns) done before the beta lines (rows); sigma complete at the end
     }
 }
 
@@ -308,7 +352,7 @@ template <int RC>
 __global__ void __launch_bounds__(kBMaxThreads, 1)
     k_batch_dl(const BatchInst* __restrict__ insts, const int* __restrict__ order, int ninst, int* __restrict__ counter,
                BatchOpts o, double* __restrict__ energies, int* __restrict__ iters, int* __restrict__ conv, int npp_max,
-               int npl_max, int xcap) {
+               int npl_max, int xcap, int csize) {
     extern __shared__ __align__(16) unsigned char batch_smem[];
     BatchShared& S = *reinterpret_cast<BatchShared*>(batch_smem);
     double* Vs = reinterpret_cast<double*>(batch_smem + sizeof(BatchShared));
@@ -319,10 +363,14 @@ __global__ void __launch_bounds__(kBMaxThreads, 1)
     __shared__ int grp[2 * kBMaxG];
     __shared__ BatchInst sP;  // one copy per CTA (a per-thread copy would live in local memory)
     const int tid = threadIdx.x, nth = blockDim.x;
+    CInfo ci{csize, csize > 1 ? (int)cooperative_groups::this_cluster().block_rank() : 0, 0};
+    // this CTA's share of an instance's vector elements
+#define BFOR(I) for (size_t I = (size_t)ci.rank * nth + tid; I < N; I += (size_t)ci.size * nth)
     for (;;) {
-        if (tid == 0) S.inst = atomicAdd(counter, 1);
-        __syncthreads();
-        const int slot = S.inst;
+        // rank 0 takes the next instance for the cluster; the others read it from its shared memory
+        if (tid == 0 && ci.rank == 0) S.inst = atomicAdd(counter, 1);
+        csync(ci);
+        const int slot = ci.size > 1 ? *cooperative_groups::this_cluster().map_shared_rank(&S.inst, 0) : S.inst;
         if (slot >= ninst) break;
         const int id = order[slot];
         if (tid == 0) sP = insts[id];
@@ -347,7 +395,7 @@ __global__ void __launch_bounds__(kBMaxThreads, 1)
             const double* Aaa = db + n;
             const double* Abb = Aaa + n * n;
             const double* Aab = Abb + n * n;
-            for (size_t e = tid; e < N; e += nth) {
+            BFOR(e) {
                 const int ia = (int)(e / P.nbs), ib = (int)(e - (size_t)ia * P.nbs);
                 const uint32_t sa = P.stra[ia], sb = P.strb[ib];
                 double h = P.scalar;
@@ -365,7 +413,7 @@ __global__ void __launch_bounds__(kBMaxThreads, 1)
                 hd[e] = h;
             }
         }
-        __syncthreads();
+        csync(ci);  // the guess reads every diagonal element
         // guess: unit vectors on the lowest diagonal elements
         const int nguess = min(min(2 * nroot, msub), (int)N);
         for (int g = 0; g < nguess; g++) {
@@ -409,7 +457,7 @@ __global__ void __launch_bounds__(kBMaxThreads, 1)
         }
         for (int g = 0; g < nguess; g++) {
             double* bg = B + (size_t)g * N;
-            for (size_t e = tid; e < N; e += nth) bg[e] = ((int)e == S.chosen[g]) ? 1.0 : 0.0;
+            BFOR(e) bg[e] = ((int)e == S.chosen[g]) ? 1.0 : 0.0;
         }
         if (tid == 0) {
             S.nb = nguess;
@@ -422,13 +470,14 @@ __global__ void __launch_bounds__(kBMaxThreads, 1)
         bool fp64_phase = !o.mixed;  // mixed: FP32 sigma first, FP64 sigma from the restart on
         while (it < o.maxiter) {
             const int nb = S.nb;
+            csync(ci);  // the new basis vectors, written by every CTA, are read whole by sigma
             // sigma of the new basis vectors and the new columns of G
             for (int j = S.nsig; j < nb; j++) {
                 if (o.mixed && !fp64_phase)
-                    bsigma<float, RC>(P, Vs, Mas, Mbs, B + (size_t)j * N, Sg + (size_t)j * N, Xs, grp);
+                    bsigma<float, RC>(P, Vs, Mas, Mbs, B + (size_t)j * N, Sg + (size_t)j * N, Xs, grp, ci);
                 else
-                    bsigma<double, RC>(P, Vs, Mas, Mbs, B + (size_t)j * N, Sg + (size_t)j * N, Xs, grp);
-                bdots(Sg + (size_t)j * N, B, N, nb, S);
+                    bsigma<double, RC>(P, Vs, Mas, Mbs, B + (size_t)j * N, Sg + (size_t)j * N, Xs, grp, ci);
+                bdots(Sg + (size_t)j * N, B, N, nb, S, ci);
                 for (int i = tid; i < nb; i += nth) {
                     Gkeep[i * kBMaxSub + j] = S.out[i];
                     Gkeep[j * kBMaxSub + i] = S.out[i];
@@ -447,7 +496,7 @@ __global__ void __launch_bounds__(kBMaxThreads, 1)
                 double acc[kBMaxSub];
 #pragma unroll
                 for (int k = 0; k < kBMaxSub; k++) acc[k] = 0.0;
-                for (size_t I = tid; I < N; I += nth) {
+                BFOR(I) {
                     double rs[kBMaxRoot], rb[kBMaxRoot];
 #pragma unroll
                     for (int k = 0; k < kBMaxRoot; k++) rs[k] = rb[k] = 0.0;
@@ -469,7 +518,7 @@ __global__ void __launch_bounds__(kBMaxThreads, 1)
                             acc[k] = fma(r, r, acc[k]);
                         }
                 }
-                bsum(acc, nroot, S);
+                bsum(acc, nroot, S, ci);
             }
             it++;
             bool ok = true;
@@ -483,7 +532,7 @@ __global__ void __launch_bounds__(kBMaxThreads, 1)
             if (ok) {
                 // mixed: the FP32 iteration has converged; restart from the nroot Ritz vectors and
                 // recompute their sigma in FP64, which alone decides convergence from here on
-                for (size_t I = tid; I < N; I += nth) {
+                BFOR(I) {
                     double tb[kBMaxRoot];
 #pragma unroll
                     for (int k = 0; k < kBMaxRoot; k++) tb[k] = 0.0;
@@ -511,7 +560,7 @@ __global__ void __launch_bounds__(kBMaxThreads, 1)
             __syncthreads();
             for (int k = tid; k < nroot; k += nth) S.lam_old[k] = S.lam[k];
             // diagonal corrections
-            for (size_t I = tid; I < N; I += nth) {
+            BFOR(I) {
                 const double h = hd[I];
                 for (int k = 0; k < nroot; k++) {
                     const double den = S.lam[k] - h;
@@ -523,7 +572,7 @@ __global__ void __launch_bounds__(kBMaxThreads, 1)
             // collapse when the subspace would overflow
             if (nb + nroot > msub) {
                 const int ncol = min(P.ncol, nb);
-                for (size_t I = tid; I < N; I += nth) {
+                BFOR(I) {
                     double tb[2 * kBMaxRoot], ts[2 * kBMaxRoot];
 #pragma unroll
                     for (int k = 0; k < 2 * kBMaxRoot; k++) tb[k] = ts[k] = 0.0;
@@ -565,16 +614,16 @@ __global__ void __launch_bounds__(kBMaxThreads, 1)
                     double a[kBMaxSub];
 #pragma unroll
                     for (int j = 0; j < kBMaxSub; j++) a[j] = 0.0;
-                    for (size_t I = tid; I < N; I += nth) a[0] = fma(r[I], r[I], a[0]);
-                    bsum(a, 1, S);
+                    BFOR(I) a[0] = fma(r[I], r[I], a[0]);
+                    bsum(a, 1, S, ci);
                 }
                 const double nrm0 = sqrt(S.out[0]);
                 if (!(nrm0 > 0.0)) continue;
-                for (size_t I = tid; I < N; I += nth) r[I] /= nrm0;
+                BFOR(I) r[I] /= nrm0;
                 __syncthreads();
                 for (int pass = 0; pass < 2; pass++) {
-                    bdots(r, B, N, nbk, S);
-                    for (size_t I = tid; I < N; I += nth) {
+                    bdots(r, B, N, nbk, S, ci);
+                    BFOR(I) {
                         double v = r[I];
                         for (int j = 0; j < nbk; j++) v -= S.out[j] * B[(size_t)j * N + I];
                         r[I] = v;
@@ -585,13 +634,13 @@ __global__ void __launch_bounds__(kBMaxThreads, 1)
                     double a[kBMaxSub];
 #pragma unroll
                     for (int j = 0; j < kBMaxSub; j++) a[j] = 0.0;
-                    for (size_t I = tid; I < N; I += nth) a[0] = fma(r[I], r[I], a[0]);
-                    bsum(a, 1, S);
+                    BFOR(I) a[0] = fma(r[I], r[I], a[0]);
+                    bsum(a, 1, S, ci);
                 }
                 const double nrm = sqrt(S.out[0]);
                 if (!(nrm >= 1.0e-7)) continue;
                 double* bn = B + (size_t)nbk * N;
-                for (size_t I = tid; I < N; I += nth) bn[I] = r[I] / nrm;
+                BFOR(I) bn[I] = r[I] / nrm;
                 __syncthreads();
                 if (tid == 0) {
                     S.nb = nbk + 1;
@@ -601,13 +650,18 @@ __global__ void __launch_bounds__(kBMaxThreads, 1)
             }
             if (S.added == 0) break;
         }
-        if (tid < nroot) energies[(size_t)id * nroot + tid] = S.lam[tid];
-        if (tid == 0) {
-            iters[id] = it;
-            conv[id] = done ? 1 : 0;
+        if (ci.rank == 0) {
+            if (tid < nroot) energies[(size_t)id * nroot + tid] = S.lam[tid];
+            if (tid == 0) {
+                iters[id] = it;
+                conv[id] = done ? 1 : 0;
+            }
         }
         __syncthreads();
     }
+#undef BFOR
+    // no CTA leaves while another may still read its shared memory
+    if (ci.size > 1) cooperative_groups::this_cluster().sync();
 }
 
 }  // namespace fcib
@@ -627,7 +681,7 @@ struct fcib_batch {
     fcib::DBuf<int> order, counter, iters, conv;
     int npp_max = 0, npl_max = 0, xcap = 0;
     size_t smem = 0;
-    int threads = 512, ctas_per_sm = 1, pair_tile = 16;
+    int threads = 512, ctas_per_sm = 1, pair_tile = 32, cluster = 1;  // the default shape (see fcib_batch_create)
     cudaGraphExec_t graph = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     double last_ms = 0.0;
@@ -646,14 +700,30 @@ static void batch_capture(fcib_batch* b) {
         FCIB_CUDA(cudaGraphExecDestroy(b->graph));
         b->graph = nullptr;
     }
-    const int grid = std::min(b->ninst, b->ctas_per_sm * b->num_sms);
+    // clusters of b->cluster CTAs, one cluster per instance at a time, at most one cluster slot per
+    // (ctas_per_sm x SMs / cluster) and never more clusters than instances
+    const int cl = b->cluster;
+    const int grid = std::min(b->ninst, b->ctas_per_sm * b->num_sms / cl) * cl;
     cudaGraph_t g;
     FCIB_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
     cudaMemsetAsync(b->counter.p, 0, sizeof(int), b->stream);
     auto kern = b->pair_tile == 8 ? k_batch_dl<8> : b->pair_tile == 32 ? k_batch_dl<32> : k_batch_dl<16>;
-    kern<<<grid, b->threads, b->smem, b->stream>>>(b->insts.p, b->order.p, b->ninst, b->counter.p, b->opts,
-                                                  b->energies.p, b->iters.p, b->conv.p, b->npp_max, b->npl_max, b->xcap);
-    cudaError_t le = cudaGetLastError();
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(b->threads);
+    cfg.dynamicSmemBytes = b->smem;
+    cfg.stream = b->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cl;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = cl > 1 ? 1 : 0;
+    cudaError_t le = cudaLaunchKernelEx(&cfg, kern, (const BatchInst*)b->insts.p, (const int*)b->order.p, b->ninst,
+                                        b->counter.p, b->opts, b->energies.p, b->iters.p, b->conv.p, b->npp_max,
+                                        b->npl_max, b->xcap, cl);
+    if (le == cudaSuccess) le = cudaGetLastError();
     cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
     FCIB_CUDA(le);
     FCIB_CUDA(ce);
@@ -843,6 +913,25 @@ int fcib_batch_create(fcib_batch** out, int device, int ninst, const int* n, con
         FCIB_CUDA(cudaFuncSetAttribute(k_batch_dl<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
         FCIB_CUDA(cudaFuncSetAttribute(k_batch_dl<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
         FCIB_CUDA(cudaFuncSetAttribute(k_batch_dl<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
+        // default shape: 512 threads, 32-pair tiles, instances shared by clusters of two CTAs when two
+        // such CTAs can be co-scheduled (the fastest shape measured on the 256-instance batch)
+        {
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(b->num_sms / 2 * 2);
+            cfg.blockDim = dim3(512);
+            cfg.dynamicSmemBytes = b->smem;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = 2;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            int nclusters = 0;
+            if (cudaOccupancyMaxActiveClusters(&nclusters, k_batch_dl<32>, &cfg) == cudaSuccess && nclusters >= 1)
+                b->cluster = 2;
+            cudaGetLastError();
+        }
         FCIB_CUDA(cudaStreamSynchronize(b->stream));
     });
     if (rc != FCIB_OK) {
@@ -874,27 +963,67 @@ int fcib_batch_solve(fcib_batch* b, double* energies, int* iterations, int* conv
     });
 }
 
-// Autotuner: times the whole batch for each launch shape (threads per CTA x CTAs per SM) and keeps
-// the fastest; the choice is re-captured into the solve graph.  shapes_ms[8] (may be NULL)
-// receives the time of each candidate (0 when a shape does not fit).
-int fcib_batch_tune(fcib_batch* b, int* threads, int* ctas_per_sm, int* pair_tile, double* times_ms) {
+// Launch shape for later solves: threads per CTA (256 or 512), opposite-spin sigma tile (8, 16 or
+// 32 pairs per work item) and CTAs per instance (a thread-block cluster of 1, 2 or 4).
+int fcib_batch_set_shape(fcib_batch* b, int threads, int pair_tile, int cluster) {
+    if (!b) { fcib::set_error("null batch"); return FCIB_ERR_ARG; }
+    return fcib::guarded(nullptr, [&] {
+        FCIB_CHECK(threads == 256 || threads == 512, FCIB_ERR_ARG, "fcib_batch_set_shape: 256 or 512 threads");
+        FCIB_CHECK(pair_tile == 8 || pair_tile == 16 || pair_tile == 32, FCIB_ERR_ARG,
+                   "fcib_batch_set_shape: pair tile 8, 16 or 32");
+        FCIB_CHECK(cluster == 1 || cluster == 2 || cluster == 4, FCIB_ERR_ARG, "fcib_batch_set_shape: cluster 1, 2 or 4");
+        FCIB_CUDA(cudaSetDevice(b->device));
+        b->threads = threads;
+        b->ctas_per_sm = 1;
+        b->pair_tile = pair_tile;
+        b->cluster = cluster;
+        if (b->graph) {
+            cudaGraphExecDestroy(b->graph);
+            b->graph = nullptr;
+        }
+    });
+}
+
+// Autotuner: times the whole batch for each launch shape (threads per CTA x CTAs per instance, the
+// cluster size) and opposite-spin sigma tile, keeps the fastest and re-captures it into the solve
+// graph.  times_ms[12] (may be NULL) receives each candidate's time (0 when a shape does not fit),
+// tile-major: tiles 8, 16, 32 x shapes 256x1, 512x1, 256 in clusters of 2, 512 in clusters of 2.
+int fcib_batch_tune(fcib_batch* b, int* threads, int* ctas_per_sm, int* pair_tile, int* cluster, double* times_ms) {
     if (!b) { fcib::set_error("null batch"); return FCIB_ERR_ARG; }
     return fcib::guarded(nullptr, [&] {
         FCIB_CUDA(cudaSetDevice(b->device));
-        // launch shapes (threads per CTA x CTAs per SM) x opposite-spin sigma tiles (pairs per work item)
-        const int cand[4][2] = {{256, 1}, {512, 1}, {256, 2}, {128, 2}};
+        const int cand[4][2] = {{256, 1}, {512, 1}, {256, 2}, {512, 2}};  // threads, cluster size
         const int tiles[3] = {8, 16, 32};
         double best = 1e300;
-        int bt = b->threads, bc = b->ctas_per_sm, bp = b->pair_tile;
+        int bt = b->threads, bp = b->pair_tile, bcl = b->cluster;
         for (int ti = 0; ti < 3; ti++) {
             auto kern = tiles[ti] == 8 ? fcib::k_batch_dl<8> : tiles[ti] == 32 ? fcib::k_batch_dl<32> : fcib::k_batch_dl<16>;
             for (int i = 0; i < 4; i++) {
                 if (times_ms) times_ms[ti * 4 + i] = 0.0;
                 int per_sm = 0;
                 FCIB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, cand[i][0], b->smem));
-                if (per_sm < cand[i][1]) continue;
+                if (per_sm < 1) continue;
+                if (cand[i][1] > 1) {
+                    cudaLaunchConfig_t cfg = {};
+                    cfg.gridDim = dim3(b->num_sms / cand[i][1] * cand[i][1]);
+                    cfg.blockDim = dim3(cand[i][0]);
+                    cfg.dynamicSmemBytes = b->smem;
+                    cudaLaunchAttribute attr[1];
+                    attr[0].id = cudaLaunchAttributeClusterDimension;
+                    attr[0].val.clusterDim.x = cand[i][1];
+                    attr[0].val.clusterDim.y = 1;
+                    attr[0].val.clusterDim.z = 1;
+                    cfg.attrs = attr;
+                    cfg.numAttrs = 1;
+                    int nclusters = 0;
+                    if (cudaOccupancyMaxActiveClusters(&nclusters, kern, &cfg) != cudaSuccess || nclusters < 1) {
+                        cudaGetLastError();
+                        continue;
+                    }
+                }
                 b->threads = cand[i][0];
-                b->ctas_per_sm = cand[i][1];
+                b->ctas_per_sm = 1;
+                b->cluster = cand[i][1];
                 b->pair_tile = tiles[ti];
                 if (b->graph) {
                     cudaGraphExecDestroy(b->graph);
@@ -906,21 +1035,23 @@ int fcib_batch_tune(fcib_batch* b, int* threads, int* ctas_per_sm, int* pair_til
                 if (ms < best) {
                     best = ms;
                     bt = cand[i][0];
-                    bc = cand[i][1];
+                    bcl = cand[i][1];
                     bp = tiles[ti];
                 }
             }
         }
         b->threads = bt;
-        b->ctas_per_sm = bc;
+        b->ctas_per_sm = 1;
+        b->cluster = bcl;
         b->pair_tile = bp;
         if (b->graph) {
             cudaGraphExecDestroy(b->graph);
             b->graph = nullptr;
         }
         if (threads) *threads = bt;
-        if (ctas_per_sm) *ctas_per_sm = bc;
+        if (ctas_per_sm) *ctas_per_sm = 1;
         if (pair_tile) *pair_tile = bp;
+        if (cluster) *cluster = bcl;
     });
 }
 

@@ -203,8 +203,9 @@ int fcib_captured_residual(fcib_ctx* ctx, int index, double* r, double* lambda, 
 
 /* ---- batched solver (no counterpart in the reference) ------------------------------------
  * Many independent CAS instances (2..12 orbitals, >= 1 electron of each spin, C1, no spin
- * selection) solved in one persistent launch: one CTA per instance at a time, largest first,
- * every Davidson-Liu iteration on the device.  Per instance: n, na, nb, scalar and the integral
+ * selection) solved in one persistent launch: one CTA, or a thread-block cluster of CTAs sharing
+ * its rows and vector elements, per instance at a time, largest first, every Davidson-Liu
+ * iteration on the device.  Per instance: n, na, nb, scalar and the integral
  * arrays in the layouts of fcib_set_integrals.  Options used: maxiter, e_convergence,
  * r_convergence, subspace_per_root, collapse_per_root, precision (FCIB_PREC_FP64: FP64 sigma;
  * otherwise FP32 sigma with FP64 subspace, residuals and vectors until converged, then a restart
@@ -219,10 +220,16 @@ int fcib_batch_destroy(fcib_batch* batch);
 /* energies[ninst * nroot] (instance-major), iterations[ninst], converged[ninst], device_ms = device
  * time of the launch; any output may be NULL */
 int fcib_batch_solve(fcib_batch* batch, double* energies, int* iterations, int* converged, double* device_ms);
+/* launch shape of later solves: threads per CTA (256 or 512), opposite-spin sigma tile (8, 16 or 32
+ * pairs per work item), CTAs per instance (a thread-block cluster of 1, 2 or 4).  The default is
+ * 512 threads, 32-pair tiles and clusters of 2 (1 when two CTAs cannot be co-scheduled). */
+int fcib_batch_set_shape(fcib_batch* batch, int threads, int pair_tile, int cluster);
 /* autotuner: times the whole batch for each opposite-spin sigma tile (8, 16 or 32 pairs per work item)
- * and launch shape (threads per CTA x CTAs per SM: 256x1, 512x1, 256x2, 128x2), keeps the fastest
- * for later solves; times_ms[12] (tile-major, 0 for shapes that do not fit) may be NULL */
-int fcib_batch_tune(fcib_batch* batch, int* threads, int* ctas_per_sm, int* pair_tile, double* times_ms);
+ * and launch shape (threads per CTA x CTAs per instance, a thread-block cluster: 256x1, 512x1,
+ * 256x2, 512x2), keeps the fastest for later solves; ctas_per_sm is 1; times_ms[12] (tile-major,
+ * 0 for shapes that do not fit) may be NULL */
+int fcib_batch_tune(fcib_batch* batch, int* threads, int* ctas_per_sm, int* pair_tile, int* cluster,
+                    double* times_ms);
 
 /* String tables for parity checks.  spin 0 = alpha, 1 = beta. */
 int fcib_num_strings(fcib_ctx* ctx, int spin, int64_t* count);

@@ -50,7 +50,8 @@ def test_batch_autotuner_keeps_a_valid_shape():
     b = BatchSolver(inst, nroot=4, options=OPTS)
     e0, _, cv0, _ = b.solve()
     t = b.tune()
-    assert t["threads"] in (128, 256, 512) and t["ctas_per_sm"] in (1, 2) and t["pair_tile"] in (8, 16, 32)
+    assert t["threads"] in (256, 512) and t["ctas_per_sm"] == 1 and t["pair_tile"] in (8, 16, 32)
+    assert t["cluster"] in (1, 2)
     assert any(v > 0 for v in t["times_ms"].values())
     e1, _, cv1, _ = b.solve()
     assert cv0.all() and cv1.all() and np.max(np.abs(e1 - e0)) < 1e-8
@@ -79,3 +80,21 @@ def test_batch_mixed_precision_matches_fp64(tile_seed):
         s = FCISolver(StateInfo(na, nb, 0), 4, ints, dict(OPTS, E_CONVERGENCE=1e-12, R_CONVERGENCE=1e-8))
         s.compute_energy()
         assert np.max(np.abs(em[i] - np.array(s.energies()))) < 1e-8
+
+
+@pytest.mark.parametrize("cluster,prec", [(2, "FP64"), (2, "MIXED"), (4, "FP64")])
+def test_batch_cluster_matches_single_cta(cluster, prec):
+    """Instances shared by a thread-block cluster (rows, lines and vector elements split across its
+    CTAs, partial sums combined through distributed shared memory) give the single-CTA energies."""
+    inst = _instances([10, 6, 9, 7, 8, 5, 10], 1200)
+    one = BatchSolver(inst, nroot=4, options=dict(OPTS, FCI_PRECISION=prec))
+    many = BatchSolver(inst, nroot=4, options=dict(OPTS, FCI_PRECISION=prec))
+    one.set_shape(512, 16, 1)
+    many.set_shape(512, 16, cluster)
+    e1, it1, c1, _ = one.solve()
+    e2, it2, c2, _ = many.solve()
+    assert c1.all() and c2.all(), (it1, it2)
+    assert np.max(np.abs(e2 - e1)) < 1e-9
+    # the graph replays to the same answer
+    e3, _, c3, _ = many.solve()
+    assert c3.all() and np.max(np.abs(e3 - e2)) < 1e-12
