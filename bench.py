@@ -530,10 +530,15 @@ def cpu_batch_sample(instances, nroot, iterations):
 
 def run_batch(args, world, rank, local):
     """Batched CASCI: instances/s of one persistent launch over seeded CAS instances."""
+    import ctypes as C
     import torch
-    from forte_b200 import build
+    from forte_b200 import build, capi
     from forte_b200.batch import BatchSolver
-    build.build()
+    if args.phases:
+        # the profiling build: the same kernels with per-phase clock counters
+        capi.LIB_PATH = build.build(phases=True)
+    else:
+        build.build()
     torch.cuda.set_device(local)
     sizes = [int(x) for x in args.batch_sizes.split(",")]
     inst = batch_instances(args.batch_count, sizes, SEED + rank)
@@ -547,11 +552,21 @@ def run_batch(args, world, rank, local):
     for _ in range(max(0, args.warmup - 1)):
         b.solve()
     barrier(world)
+    cycles = (C.c_ulonglong * 8)()
+    if args.phases:
+        capi.check(capi.lib().fcib_batch_phase_cycles(cycles))  # reset
     ms = []
     for _ in range(args.steps):
         e, it, cv, d = b.solve()
         ms.append(d)
     step_s = allmax(world, statistics.mean(ms) / 1e3)
+    phases = None
+    if args.phases:
+        capi.check(capi.lib().fcib_batch_phase_cycles(cycles))
+        names = ["sigma_opposite_spin", "sigma_same_spin", "g_update", "subspace", "residuals", "preconditioner",
+                 "collapse", "gram_schmidt"]
+        tot = float(sum(cycles)) or 1.0
+        phases = {nm: cycles[i] / tot for i, nm in enumerate(names)}
     # end to end: integrals from host memory to energies back, through the public API
     t1 = time.perf_counter()
     b2 = BatchSolver(inst, nroot=4, options=opts, device=local)
@@ -577,6 +592,7 @@ def run_batch(args, world, rank, local):
                        "r_convergence": opts["R_CONVERGENCE"], "parallelism": f"replicas x{world}"},
             "iterations_mean": float(np.mean(it)), "iterations_max": int(np.max(it)),
             "converged_fraction": float(np.mean(cv)), "autotune": tuned, "setup_seconds": setup_s,
+            "phase_fractions": phases, "build": "profiling (phase clocks)" if args.phases else "default",
             "e2e": {"value": world * args.batch_count / e2e_s, "unit": "instances/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(e2.nbytes + it2.nbytes + cv2.nbytes)},
             "cpu_baseline": cpu, "gpu_launches": 1,
@@ -602,6 +618,8 @@ def main():
     ap.add_argument("--batch-count", type=int, default=256)
     ap.add_argument("--batch-sizes", default="6,7,8,9,10")
     ap.add_argument("--maxiter", type=int, default=0, help="batch mode: Davidson iteration cap (0 = 200)")
+    ap.add_argument("--phases", action="store_true",
+                    help="batch mode: run the profiling build and report the share of clock cycles per phase")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--mode", default="solve", choices=["solve", "sigma", "precond", "batch", "configs", "sym"],
                     help="solve: the Davidson time-to-solution metric; sigma: sigma builds/s at CAS(n,n); "

@@ -82,6 +82,7 @@ SIGNATURES = {
     "fcib_set_state": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
     "fcib_set_options": (C.c_int, [_vp, C.POINTER(FcibOptions)]),
     "fcib_size": (C.c_int, [_vp, C.POINTER(C.c_int64)]),
+    "fcib_ncsf": (C.c_int, [_vp, C.POINTER(C.c_int64)]),
     "fcib_solve": (C.c_int, [_vp, _dp, _dp, C.POINTER(C.c_int)]),
     "fcib_reset_guess": (C.c_int, [_vp]),
     "fcib_get_vector": (C.c_int, [_vp, C.c_int, _dp]),
@@ -117,6 +118,7 @@ SIGNATURES = {
     "fcib_batch_destroy": (C.c_int, [_vp]),
     "fcib_batch_solve": (C.c_int, [_vp, _dp, C.POINTER(C.c_int), C.POINTER(C.c_int), _dp]),
     "fcib_batch_set_shape": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int]),
+    "fcib_batch_phase_cycles": (C.c_int, [C.POINTER(C.c_ulonglong)]),
     "fcib_batch_tune": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
                                   C.POINTER(C.c_int), _dp]),
     "fcib_captured_residual": (C.c_int, [_vp, C.c_int, _dp, _dp, C.POINTER(C.c_int)]),

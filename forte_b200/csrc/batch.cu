@@ -36,6 +36,24 @@
 
 namespace fcib {
 
+// Phase clocks (profiling builds only, compiled with -DFCIB_BATCH_PHASES, see forte_b200/build.py):
+// thread 0 of every CTA adds the clock cycles of each phase of its solves to g_bphase, read back by
+// fcib_batch_phase_cycles.  Phases: 0 opposite-spin sigma, 1 same-spin sigma, 2 G update, 3 subspace
+// eigenproblem, 4 residuals, 5 preconditioner, 6 collapse, 7 Gram-Schmidt.
+#ifdef FCIB_BATCH_PHASES
+__device__ unsigned long long g_bphase[8];
+__device__ __forceinline__ void bphase_mark(int ph, long long& t) {
+    if (threadIdx.x == 0) {
+        const long long now = clock64();
+        atomicAdd(&g_bphase[ph], (unsigned long long)(now - t));
+        t = now;
+    }
+}
+#define FCIB_PHASE(ph) bphase_mark((ph), pt)
+#else
+#define FCIB_PHASE(ph) ((void)pt)
+#endif
+
 constexpr int kBMaxOrb = 12;
 constexpr int kBMaxRoot = 8;
 constexpr int kBMaxSub = 32;   // subspace dimension cap
@@ -146,7 +164,8 @@ __device__ void bdots(const double* x, const double* __restrict__ B, size_t N, i
 template <typename T, int RC>
 __device__ void bsigma(const BatchInst& P, const double* __restrict__ V, const double* __restrict__ Ma,
                        const double* __restrict__ Mb, const double* c, double* __restrict__ s,
-                       unsigned char* __restrict__ scratch, int* __restrict__ grp, const CInfo& ci) {
+                       unsigned char* __restrict__ scratch, int* __restrict__ grp, const CInfo& ci,
+                       long long& pt) {
     const int nbs = P.nbs, nas = P.nas, npp = P.npp, npl = P.npl, s1a = P.s1a;
     const int tid = threadIdx.x, nth = blockDim.x;
     const int nch = (npp + RC - 1) / RC;
@@ -206,6 +225,7 @@ __device__ void bsigma(const BatchInst& P, const double* __restrict__ V, const d
         __syncthreads();
     }
     csync(ci);  // every row written before the same-spin terms add to them
+    FCIB_PHASE(0);
     // same-spin terms over the (N-2)-electron groups
     T* W = reinterpret_cast<T*>(scratch);  // [kBMaxG][kBMaxG], reuses the opposite-spin scratch
     for (int spin = 0; spin < 2; spin++) {
@@ -265,6 +285,7 @@ __device__ void bsigma(const BatchInst& P, const double* __restrict__ V, const d
         }
         csync(ci);  // alpha lines (columns) done before the beta lines (rows); sigma complete at the end
     }
+    FCIB_PHASE(1);
 }
 
 // shared-memory scratch of bsigma in bytes (the larger of the opposite-spin block and the group W),
@@ -466,6 +487,10 @@ __global__ void __launch_bounds__(kBMaxThreads, 1)
         for (int k = tid; k < kBMaxRoot; k += nth) S.lam_old[k] = 0.0;
         __syncthreads();
         int it = 0;
+        long long pt = 0;
+#ifdef FCIB_BATCH_PHASES
+        pt = clock64();
+#endif
         bool done = false;
         bool fp64_phase = !o.mixed;  // mixed: FP32 sigma first, FP64 sigma from the restart on
         while (it < o.maxiter) {
@@ -474,15 +499,16 @@ __global__ void __launch_bounds__(kBMaxThreads, 1)
             // sigma of the new basis vectors and the new columns of G
             for (int j = S.nsig; j < nb; j++) {
                 if (o.mixed && !fp64_phase)
-                    bsigma<float, RC>(P, Vs, Mas, Mbs, B + (size_t)j * N, Sg + (size_t)j * N, Xs, grp, ci);
+                    bsigma<float, RC>(P, Vs, Mas, Mbs, B + (size_t)j * N, Sg + (size_t)j * N, Xs, grp, ci, pt);
                 else
-                    bsigma<double, RC>(P, Vs, Mas, Mbs, B + (size_t)j * N, Sg + (size_t)j * N, Xs, grp, ci);
+                    bsigma<double, RC>(P, Vs, Mas, Mbs, B + (size_t)j * N, Sg + (size_t)j * N, Xs, grp, ci, pt);
                 bdots(Sg + (size_t)j * N, B, N, nb, S, ci);
                 for (int i = tid; i < nb; i += nth) {
                     Gkeep[i * kBMaxSub + j] = S.out[i];
                     Gkeep[j * kBMaxSub + i] = S.out[i];
                 }
                 __syncthreads();
+                FCIB_PHASE(2);
             }
             if (tid == 0) S.nsig = nb;
             for (int i = tid; i < nb * kBMaxSub; i += nth) {
@@ -491,6 +517,7 @@ __global__ void __launch_bounds__(kBMaxThreads, 1)
             }
             __syncthreads();
             bjacobi(S, nb);
+            FCIB_PHASE(3);
             // residuals and their norms
             {
                 double acc[kBMaxSub];
@@ -520,6 +547,7 @@ __global__ void __launch_bounds__(kBMaxThreads, 1)
                 }
                 bsum(acc, nroot, S, ci);
             }
+            FCIB_PHASE(4);
             it++;
             bool ok = true;
             for (int k = 0; k < nroot; k++)
@@ -569,6 +597,7 @@ __global__ void __launch_bounds__(kBMaxThreads, 1)
                 }
             }
             __syncthreads();
+            FCIB_PHASE(5);
             // collapse when the subspace would overflow
             if (nb + nroot > msub) {
                 const int ncol = min(P.ncol, nb);
@@ -603,6 +632,7 @@ __global__ void __launch_bounds__(kBMaxThreads, 1)
                 }
                 __syncthreads();
             }
+            FCIB_PHASE(6);
             // add the normalised, orthogonalised corrections
             if (tid == 0) S.added = 0;
             __syncthreads();
@@ -648,6 +678,7 @@ __global__ void __launch_bounds__(kBMaxThreads, 1)
                 }
                 __syncthreads();
             }
+            FCIB_PHASE(7);
             if (S.added == 0) break;
         }
         if (ci.rank == 0) {
@@ -961,6 +992,22 @@ int fcib_batch_solve(fcib_batch* b, double* energies, int* iterations, int* conv
         if (iterations) FCIB_CUDA(cudaMemcpy(iterations, b->iters.p, sizeof(int) * b->ninst, cudaMemcpyDeviceToHost));
         if (converged) FCIB_CUDA(cudaMemcpy(converged, b->conv.p, sizeof(int) * b->ninst, cudaMemcpyDeviceToHost));
     });
+}
+
+// Clock cycles of each phase summed over all CTAs since the last call (then zeroed); only builds
+// compiled with -DFCIB_BATCH_PHASES count them.
+int fcib_batch_phase_cycles(unsigned long long* cycles) {
+    if (!cycles) { fcib::set_error("null argument"); return FCIB_ERR_ARG; }
+#ifdef FCIB_BATCH_PHASES
+    return fcib::guarded(nullptr, [&] {
+        FCIB_CUDA(cudaMemcpyFromSymbol(cycles, fcib::g_bphase, 8 * sizeof(unsigned long long)));
+        const unsigned long long z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        FCIB_CUDA(cudaMemcpyToSymbol(fcib::g_bphase, z, sizeof(z)));
+    });
+#else
+    fcib::set_error("fcib_batch_phase_cycles: this build has no phase clocks (build with -DFCIB_BATCH_PHASES)");
+    return FCIB_ERR_UNSUPPORTED;
+#endif
 }
 
 // Launch shape for later solves: threads per CTA (256 or 512), opposite-spin sigma tile (8, 16 or

@@ -327,6 +327,16 @@ int fcib_size(fcib_ctx* ctx, int64_t* ndet) {
     });
 }
 
+// SpinAdapter::ncsf (ci_spin_adaptation.h:81-183): CSFs of the state's multiplicity in the target irrep
+int fcib_ncsf(fcib_ctx* ctx, int64_t* ncsf) {
+    if (!ctx || !ncsf) { set_error("null argument"); return FCIB_ERR_ARG; }
+    return guarded(ctx, [&] {
+        ensure_setup(ctx->c);
+        ensure_csf(ctx->c);
+        *ncsf = ctx->c.ncsf;
+    });
+}
+
 static void print_solutions(Context& c);
 
 int fcib_solve(fcib_ctx* ctx, double* energies, double* spin2, int* iterations) {
@@ -369,8 +379,10 @@ static void max_abs_elements(Context& c, int root, int num_dets, std::vector<dou
     ia.assign(num_dets, 0);
     ib.assign(num_dets, 0);
     if (num_dets <= 0) return;
-    const double* x = c.b.p + (size_t)root * N;
-    double* keys = c.tmp.p;  // scratch once the solve has finished
+    const double* x = root_vector(c, root);
+    DBuf<double> kb;
+    kb.alloc((size_t)N);
+    double* keys = kb.p;
     k_neg_abs<<<4 * c.num_sms, 256, 0, c.stream>>>(x, keys, (size_t)N);
     FCIB_KCHECK();
     auto sel = lowest_keys(c, keys, num_dets);
@@ -516,7 +528,7 @@ int fcib_get_vector(fcib_ctx* ctx, int root, double* out) {
         Context& c = ctx->c;
         FCIB_CHECK(c.solved, FCIB_ERR_STATE, "no solution available");
         FCIB_CHECK(root >= 0 && root < c.nroot, FCIB_ERR_ARG, "root out of range");
-        download_flat(c, c.b.p + (size_t)root * c.nvec, out);
+        download_flat(c, root_vector(c, root), out);
     });
 }
 
@@ -587,8 +599,8 @@ int fcib_rdms(fcib_ctx* ctx, int root_left, int root_right, int level, int spin_
         level = std::min(level, 2);  // the three-body blocks come from fcib_rdms3
         RdmBlocks blk;
         DBuf<double> xl, xr;
-        const double* L = c1_view(c, c.b.p + (size_t)root_left * c.nvec, xl);
-        const double* R = root_right == root_left ? L : c1_view(c, c.b.p + (size_t)root_right * c.nvec, xr);
+        const double* L = c1_view(c, root_vector(c, root_left), xl);
+        const double* R = root_right == root_left ? L : c1_view(c, root_vector(c, root_right), xr);
         compute_rdms(c, L, R, level, blk);
         rdms_to_outputs(blk, level, spin_free, g1a, g1b, g2aa, g2ab, g2bb);
     });
@@ -629,8 +641,8 @@ int fcib_transition_rdms(fcib_ctx* left, int root_left, fcib_ctx* right, int roo
         if (c.na >= 1) {
             // both vectors in the C1 layout, which does not depend on the irrep
             DBuf<double> xl, xr;
-            const double* L = c1_view(c, c.b.p + (size_t)root_left * c.nvec, xl);
-            const double* R = c1_view(r, r.b.p + (size_t)root_right * r.nvec, xr);
+            const double* L = c1_view(c, root_vector(c, root_left), xl);
+            const double* R = c1_view(r, root_vector(r, root_right), xr);
             FCIB_CUDA(cudaStreamSynchronize(r.stream));
             RdmBlocks blk;
             compute_rdms(c, L, R, 1, blk);
@@ -715,8 +727,8 @@ int fcib_rdms3(fcib_ctx* ctx, int root_left, int root_right, int spin_free, doub
                                           std::to_string(c.nroot)};
         Rdm3Blocks blk;
         DBuf<double> xl, xr;
-        const double* L = c1_view(c, c.b.p + (size_t)root_left * c.nvec, xl);
-        const double* R = root_right == root_left ? L : c1_view(c, c.b.p + (size_t)root_right * c.nvec, xr);
+        const double* L = c1_view(c, root_vector(c, root_left), xl);
+        const double* R = root_right == root_left ? L : c1_view(c, root_vector(c, root_right), xr);
         compute_rdms3(c, L, R, blk);
         rdms3_to_outputs(blk, spin_free, g3aaa, g3aab, g3abb, g3bbb);
     });

@@ -1,11 +1,12 @@
 // Spin adaptation (option spin_adapt; Forte's CI_SPIN_ADAPT, SpinAdapter in
-// forte/sparse_ci/ci_spin_adaptation.h:81-183, used by fci_solver.cc:136-141,246-253).
+// forte/sparse_ci/ci_spin_adaptation.h:81-183, used by fci_solver.cc:136-141,186-262).
 //
-// The reference solves in a basis of configuration state functions (CSFs) of the target spin S.
-// This engine keeps the determinant basis and projects every new Davidson vector (guesses,
-// corrections, random fill-ins) onto the span of those CSFs.  H commutes with S^2, so the subspace
-// stays in the spin-S sector and the solver converges to the lowest roots of that sector: the
-// energies, eigenvectors and RDMs of the CSF solve.
+// Like the reference, the Davidson-Liu solver then works in a basis of configuration state
+// functions (CSFs) of the target spin S: its vectors hold CSF coefficients z, and sigma is formed
+// as z -> C = P z (determinants) -> H C -> P^T (H C) (fci_solver.cc:247-254), with the CSF
+// diagonal sum_m O_im^2 H_mm as preconditioner (form_Hdiag_csf without the full-preconditioner
+// option, fci_solver_initial_guess.cc:111-149) and unit vectors on the lowest CSF diagonal elements
+// as guess (find_initial_guess_csf, sparse_initial_guess.cc:266-327).
 //
 // CSFs of a configuration (doubly occupied set D, open-shell set O, N = |O|) are the genealogical
 // couplings of the N open shells taken in orbital order (the published construction that adds one
@@ -14,9 +15,10 @@
 // operators.  Written in this engine's determinants |D+Oa ; D+Ob> (alpha string, then beta string),
 // the coefficient of the spin pattern m over O (bit k set: the k-th open shell is alpha) is
 //     O_N[i][m] = (-1)^(number of beta open shells below an alpha open shell) * prod_k CG_k(i, m)
-// up to a sign common to the configuration.  So a configuration's projector is P = O_N^T O_N, the
-// same matrix for every configuration with N open shells, and configurations that cannot couple
-// to S (N < 2S) are projected to zero.
+// up to a sign common to the configuration.  So P restricted to a configuration is O_N^T, the same
+// matrix for every configuration with N open shells; configurations that cannot couple to S
+// (N < 2S) hold no CSF.  CSF vector layout: groups of increasing N, configuration-major, the f
+// couplings of a configuration consecutive.
 #include "fcib_internal.h"
 
 namespace fcib {
@@ -68,52 +70,66 @@ static void csf_coupling(int N, int twoS, int twoMs, std::vector<double>& O, std
         }
 }
 
-// One CTA per configuration of a group with N open shells: gather the coefficients of its nd
-// determinants, z = O x (f CSFs), scatter back x' = O^T z.  Every determinant belongs to exactly
-// one configuration, so the scatter has no conflicts.
-__global__ void k_csf_project(double* __restrict__ v, const uint32_t* __restrict__ conf, int nconf, int N, int nd,
-                              int f, const uint32_t* __restrict__ pats, const double* __restrict__ O, int n,
-                              int nbs, SymDev sd) {
+// index in the engine layout (C1, or the target irrep's blocks) of the determinant with spin
+// pattern pat (bit k: the k-th open shell in orbital order is alpha) of configuration (D, Om)
+__device__ __forceinline__ int64_t csf_det_id(uint32_t D, uint32_t Om, uint32_t pat, int N, int n, int nbs,
+                                              const SymDev& sd) {
+    uint32_t a = D, b = D, rest = Om;
+    for (int k = 0; k < N; k++) {
+        const uint32_t bit = rest & (0u - rest);
+        rest ^= bit;
+        if (pat >> k & 1u) a |= bit;
+        else b |= bit;
+    }
+    const uint32_t ra = d_rank(a, n), rb = d_rank(b, n);
+    return sd.nirrep > 1 ? sym_encode(sd, a, (int)ra, (int)rb) : (int64_t)ra * nbs + rb;
+}
+
+// One CTA per configuration (grid-stride) of a group with N open shells, nd spin patterns and f
+// couplings; its CSF coefficients are z[zoff + cf * f + i].  Every determinant belongs to exactly
+// one configuration, so the scatters have no conflicts.
+//   mode 0: x[det m] = sum_i O[i][m] z_i        (CSF -> determinants; zeros when f = 0)
+//   mode 1: z_i = sum_m O[i][m] x[det m]        (determinants -> CSF)
+//   mode 2: z_i = sum_m O[i][m]^2 x[det m]      (the CSF diagonal from the determinant diagonal x)
+template <int MODE>
+__global__ void k_csf_map(const double* __restrict__ in, double* __restrict__ out, const uint32_t* __restrict__ conf,
+                          int nconf, int N, int nd, int f, const uint32_t* __restrict__ pats,
+                          const double* __restrict__ O, int n, int nbs, SymDev sd, int64_t zoff) {
     extern __shared__ __align__(16) unsigned char csf_smem[];
-    double* x = reinterpret_cast<double*>(csf_smem);  // [nd]
-    double* z = x + nd;                               // [f]
-    int* idx = reinterpret_cast<int*>(z + f);         // [nd]
+    double* xs = reinterpret_cast<double*>(csf_smem);  // [nd] determinant values (modes 1, 2)
+    double* zs = xs + nd;                              // [f] CSF values (mode 0)
+    int64_t* idx = reinterpret_cast<int64_t*>(zs + f); // [nd]
     for (int cf = blockIdx.x; cf < nconf; cf += gridDim.x) {
         const uint32_t D = conf[2 * (size_t)cf], Om = conf[2 * (size_t)cf + 1];
+        const int64_t z0 = zoff + (int64_t)cf * f;
         __syncthreads();
         for (int m = threadIdx.x; m < nd; m += blockDim.x) {
-            const uint32_t pat = pats[m];
-            uint32_t a = D, b = D, rest = Om;
-            for (int k = 0; k < N; k++) {
-                const uint32_t bit = rest & (0u - rest);  // k-th open shell in orbital order
-                rest ^= bit;
-                if (pat >> k & 1u) a |= bit;
-                else b |= bit;
-            }
-            // the determinant's index in the engine layout (C1, or the target irrep's blocks)
-            const uint32_t ra = d_rank(a, n), rb = d_rank(b, n);
-            const int id = sd.nirrep > 1 ? (int)sym_encode(sd, a, (int)ra, (int)rb) : (int)(ra * (uint32_t)nbs + rb);
+            const int64_t id = csf_det_id(D, Om, pats[m], N, n, nbs, sd);
             idx[m] = id;
-            x[m] = v[id];
+            if (MODE != 0) xs[m] = in[id];
         }
+        if (MODE == 0)
+            for (int i = threadIdx.x; i < f; i += blockDim.x) zs[i] = in[z0 + i];
         __syncthreads();
-        for (int i = threadIdx.x; i < f; i += blockDim.x) {
-            const double* row = O + (size_t)i * nd;
-            double s = 0.0;
-            for (int m = 0; m < nd; m++) s = fma(row[m], x[m], s);
-            z[i] = s;
-        }
-        __syncthreads();
-        for (int m = threadIdx.x; m < nd; m += blockDim.x) {
-            double s = 0.0;
-            for (int i = 0; i < f; i++) s = fma(O[(size_t)i * nd + m], z[i], s);
-            v[idx[m]] = s;
+        if (MODE == 0) {
+            for (int m = threadIdx.x; m < nd; m += blockDim.x) {
+                double v = 0.0;
+                for (int i = 0; i < f; i++) v = fma(O[(size_t)i * nd + m], zs[i], v);
+                out[idx[m]] = v;
+            }
+        } else {
+            for (int i = threadIdx.x; i < f; i += blockDim.x) {
+                const double* row = O + (size_t)i * nd;
+                double v = 0.0;
+                for (int m = 0; m < nd; m++) v = fma(MODE == 2 ? row[m] * row[m] : row[m], xs[m], v);
+                out[z0 + i] = v;
+            }
         }
     }
 }
 
 // Configuration groups of the current state and target spin (rebuilt when either changes)
-static void ensure_csf(Context& c) {
+void ensure_csf(Context& c) {
     const int twoS = c.multiplicity - 1, twoMs = c.na - c.nb;
     if (c.csf_ready && c.csf_twoS == twoS) return;
     FCIB_CHECK(c.multiplicity >= 1, FCIB_ERR_ARG, "spin adaptation needs the multiplicity of the target state");
@@ -159,6 +175,7 @@ static void ensure_csf(Context& c) {
         csf_coupling(N, twoS, twoMs, O, pats, g.f, g.nd);
         g.N = N;
         g.nconf = (int)(byN[N].size() / 2);
+        g.zoff = c.ncsf;
         g.conf.upload(byN[N], c.stream);
         g.pats.upload(pats, c.stream);
         if (!O.empty()) g.O.upload(O, c.stream);
@@ -169,24 +186,31 @@ static void ensure_csf(Context& c) {
     c.csf_twoS = twoS;
 }
 
-// v <- projection of v onto the spin-S sector (engine layout)
-void csf_project(Context& c, double* v) {
-    // k_csf_project keeps determinant indices as int in shared memory
-    FCIB_CHECK(c.ndet < ((int64_t)1 << 31), FCIB_ERR_UNSUPPORTED,
-               "spin adaptation: more than 2^31 - 1 determinants");
+// one k_csf_map launch per configuration group
+template <int MODE>
+static void csf_map(Context& c, const double* in, double* out) {
     ensure_csf(c);
     for (auto& gp : c.csf) {
         CsfGroup& g = *gp;
-        const size_t smem = (size_t)g.nd * 12 + (size_t)g.f * 8;
+        if (MODE != 0 && g.f == 0) continue;  // no CSF to write
+        const size_t smem = (size_t)g.nd * 16 + (size_t)g.f * 8;
         FCIB_CHECK(smem + 1024 <= (size_t)c.smem_optin, FCIB_ERR_UNSUPPORTED, "spin adaptation: configuration too large");
-        FCIB_CUDA(cudaFuncSetAttribute(k_csf_project, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        FCIB_CUDA(cudaFuncSetAttribute(k_csf_map<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         const int grid = std::min(g.nconf, 8 * c.num_sms);
-        k_csf_project<<<grid, g.nd > 64 ? 256 : 64, smem, c.stream>>>(v, g.conf.p, g.nconf, g.N, g.nd, g.f, g.pats.p,
-                                                                       g.f > 0 ? g.O.p : nullptr, c.n, (int)c.nbs,
-                                                                       sym_dev(c));
+        k_csf_map<MODE><<<grid, g.nd > 64 ? 256 : 64, smem, c.stream>>>(
+            in, out, g.conf.p, g.nconf, g.N, g.nd, g.f, g.pats.p, g.f > 0 ? g.O.p : nullptr, c.n, (int)c.nbs,
+            sym_dev(c), g.zoff);
         FCIB_KCHECK();
     }
 }
+
+void csf_to_det(Context& c, const double* z, double* x) {
+    // the masked C1 layout also holds determinants of other irreps, which no configuration covers
+    if (c.nirrep > 1 && !c.sym.on) FCIB_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * c.nvec, c.stream));
+    csf_map<0>(c, z, x);
+}
+void det_to_csf(Context& c, const double* x, double* z) { csf_map<1>(c, x, z); }
+void csf_hdiag(Context& c, double* out) { csf_map<2>(c, c.hdiag.p, out); }
 
 }  // namespace fcib
 

@@ -411,11 +411,13 @@ __global__ void __launch_bounds__(kRedThreads) k_spin2(const double* __restrict_
 struct Ops {
     Context& c;
     size_t N;
+    const double* hd;  // diagonal of the preconditioner
     int nblk;
     DBuf<double> partial, out;
     std::vector<double> hout;
-    explicit Ops(Context& cc) : c(cc) {
-        N = (size_t)c.nvec;
+    explicit Ops(Context& cc) : Ops(cc, (size_t)cc.nvec, cc.hdiag.p) {}
+    Ops(Context& cc, size_t n, const double* diag) : c(cc), hd(diag) {
+        N = n;
         nblk = std::max(1, std::min(4 * c.num_sms, (int)((N + kRedThreads - 1) / kRedThreads)));
         partial.alloc((size_t)nblk * kSlots);
         out.alloc(kSlots);
@@ -509,7 +511,7 @@ struct Ops {
                     a.out[k] = outs[k0 + k];
                     a.lambda[k] = lambda ? lambda[k0 + k] : 0.0;
                 }
-                a.hd = c.hdiag.p;
+                a.hd = hd;
                 a.nv = nv;
                 a.nout = nout;
                 a.precond = (lambda && last) ? 1 : 0;
@@ -609,9 +611,10 @@ static void project_out(Context& c, std::vector<SparseDev>& bad, std::vector<dou
             k_project_sparse<<<1, 256, 0, c.stream>>>(V[k], b.idx.p, b.val.p, b.cnt);
             FCIB_KCHECK();
         }
-    // spin adaptation: every vector that enters the basis is kept in the target spin sector
-    if (c.opt.spin_adapt)
-        for (int k = 0; k < nvec; k++) csf_project(c, V[k]);
+}
+
+const double* root_vector(Context& c, int root) {
+    return c.csf_basis_solve ? c.evdet.p + (size_t)root * c.nvec : c.b.p + (size_t)root * c.nvec;
 }
 
 double spin2_device(Context& c, const double* C) {
@@ -630,8 +633,10 @@ double spin2_device(Context& c, const double* C) {
 // the `count` smallest keys[] of the determinants in the target irrep with their C1 indices, sorted by
 // (key, index); ties at the boundary are resolved by the index
 std::vector<std::pair<double, int64_t>> lowest_keys(Context& c, const double* keys, int count) {
-    const size_t N = (size_t)c.nvec;
-    const uint8_t* mask = (c.nirrep > 1 && !c.sym.on) ? c.mask.p : nullptr;
+    return lowest_keys(c, keys, count, (size_t)c.nvec, (c.nirrep > 1 && !c.sym.on) ? c.mask.p : nullptr);
+}
+std::vector<std::pair<double, int64_t>> lowest_keys(Context& c, const double* keys, int count, size_t N,
+                                                    const uint8_t* mask) {
     DBuf<unsigned int> hist;
     hist.alloc(256);
     uint64_t prefix = 0, pmask = 0;
@@ -696,9 +701,22 @@ static double now_ms() {
 enum class Phase { LowPrecision, Refine, FP64Only };
 
 void dl_solve(Context& c) {
-    const int64_t N = c.nvec;
+    // spin adaptation: the Davidson space is the CSF basis of the target multiplicity
+    // (fci_solver.cc:186-262); otherwise the engine's determinant layout
+    const bool csf_basis = c.opt.spin_adapt != 0;
+    if (csf_basis) {
+        FCIB_CHECK(c.opt.preconditioner != FCIB_PRECOND_MLP, FCIB_ERR_UNSUPPORTED,
+                   "the learned preconditioner works in the determinant basis (not with spin adaptation)");
+        ensure_csf(c);
+        FCIB_CHECK(c.ncsf > 0, FCIB_ERR_ARG, "Found zero FCI guesses with the requested multiplicity.");
+        c.hd_csf.alloc((size_t)c.ncsf);
+        csf_hdiag(c, c.hd_csf.p);
+        c.csf_x.alloc((size_t)c.nvec);
+        c.csf_s.alloc((size_t)c.nvec);
+    }
+    const int64_t N = csf_basis ? c.ncsf : c.nvec;
     int64_t Neff = N;
-    if (c.nirrep > 1 && !c.sym.on) {
+    if (!csf_basis && c.nirrep > 1 && !c.sym.on) {
         std::vector<uint8_t> hm(N);
         FCIB_CUDA(cudaMemcpy(hm.data(), c.mask.p, N, cudaMemcpyDeviceToHost));
         Neff = 0;
@@ -728,7 +746,18 @@ void dl_solve(Context& c) {
         tmp[i] = c.tmp.p + (size_t)i * N;
     }
     for (int k = 0; k < nroot; k++) r[k] = c.r.p + (size_t)k * N;
-    Ops ops(c);
+    Ops ops(c, (size_t)N, csf_basis ? c.hd_csf.p : c.hdiag.p);
+    // sigma of a vector of the Davidson space: in the CSF basis z -> P z -> H P z -> P^T H P z
+    // (fci_solver.cc:247-254)
+    auto space_sigma = [&](const double* bj, double* sj, int prec) {
+        if (!csf_basis) {
+            sigma_dispatch(c, bj, sj, prec);
+            return;
+        }
+        csf_to_det(c, bj, c.csf_x.p);
+        sigma_dispatch(c, c.csf_x.p, c.csf_s.p, prec);
+        det_to_csf(c, c.csf_s.p, sj);
+    };
     cudaEvent_t ev_start, e0, e1;
     FCIB_CUDA(cudaEventCreate(&ev_start));
     FCIB_CUDA(cudaEventCreate(&e0));
@@ -784,6 +813,33 @@ void dl_solve(Context& c) {
     };
     // a fresh guess (FCISolver::initial_guess_det): lowest diagonal determinants, spin-adapted
     // guess vectors and the unwanted roots to project out
+    // a fresh guess in the CSF basis (FCISolver::initial_guess_csf, find_initial_guess_csf in
+    // sparse_initial_guess.cc:266-327): unit vectors on the num_guess_states lowest CSF diagonal
+    // elements, ordered by (value, index); no roots to project out
+    auto fresh_guess_csf = [&]() -> int {
+        auto lowest = lowest_keys(c, c.hd_csf.p, num_guess_states, (size_t)N, nullptr);
+        const int nguess = (int)lowest.size();
+        c.t_guess_ms = now_ms() - t_guess0;
+        c.guess_dets = nguess;
+        FCIB_CHECK(nguess >= 1, FCIB_ERR_ARG, "Found zero FCI guesses with the requested multiplicity.");
+        FCIB_CHECK(nguess >= nroot && nguess <= m, FCIB_ERR_ARG,
+                   "DavidsonLiuSolver: number of guess vectors must be between nroot and the subspace size");
+        c.dl_bad.clear();
+        upload_bad(c.dl_bad);
+        FCIB_CUDA(cudaMemsetAsync(c.tmp.p, 0, sizeof(double) * (size_t)m * N, c.stream));
+        std::vector<int64_t> ix(nguess);
+        std::vector<double> one(nguess, 1.0);
+        for (int g = 0; g < nguess; g++) ix[g] = (int64_t)g * N + lowest[g].second;  // tmp[g][csf]
+        SparseDev sd;
+        sd.idx.upload(ix, c.stream);
+        sd.val.upload(one, c.stream);
+        k_fill_sparse<<<(nguess + 255) / 256, 256, 0, c.stream>>>(c.tmp.p, sd.idx.p, sd.val.p, nguess);
+        FCIB_KCHECK();
+        FCIB_CUDA(cudaStreamSynchronize(c.stream));
+        const int added = add_rows_orth(ops, b, 0, std::vector<double*>(tmp.begin(), tmp.begin() + nguess), nguess);
+        FCIB_CHECK(added == nguess, FCIB_ERR_NUMERIC, "DavidsonLiuSolver: guess vectors are zero or linearly dependent");
+        return added;
+    };
     auto fresh_guess = [&]() -> int {
         auto lowest = lowest_diagonal(c, ng);
         std::vector<uint32_t> sa(c.nas), sbv(c.nbs);
@@ -854,7 +910,7 @@ void dl_solve(Context& c) {
         basis = nroot;  // rows 0..nroot-1 of b hold the previous eigenvectors
         c.t_guess_ms = 0.0;
     } else {
-        basis = fresh_guess();
+        basis = csf_basis ? fresh_guess_csf() : fresh_guess();
     }
 
     const bool mixed = (o.precision != FCIB_PREC_FP64);
@@ -897,7 +953,7 @@ void dl_solve(Context& c) {
         for (int j = nsig; j < basis; j++) {
             bool fp64 = (phase == Phase::FP64Only) || (phase == Phase::Refine && j < nroot && nsig == 0);
             FCIB_CUDA(cudaEventRecord(e0, c.stream));
-            sigma_dispatch(c, b[j], sg[j], fp64 ? FCIB_PREC_FP64 : lowp);
+            space_sigma(b[j], sg[j], fp64 ? FCIB_PREC_FP64 : lowp);
             FCIB_CUDA(cudaEventRecord(e1, c.stream));
             FCIB_CUDA(cudaEventSynchronize(e1));
             float ms = 0.f;
@@ -1044,7 +1100,7 @@ void dl_solve(Context& c) {
                 FCIB_CUDA(cudaMemsetAsync(tmp[m - 1], 0, sizeof(double) * N, c.stream));
                 k_add_random<<<ops.nblk, kRedThreads, 0, c.stream>>>(tmp[m - 1], N, 0xD1B54A32D192ED03ull + rng(), 1.0);
                 FCIB_KCHECK();
-                apply_mask(c, tmp[m - 1]);
+                if (!csf_basis) apply_mask(c, tmp[m - 1]);
                 std::vector<double*> one{tmp[m - 1]};
                 project_out(c, bad, one, 1);
                 int ra = add_rows_orth(ops, b, basis, one, 1);
@@ -1080,8 +1136,14 @@ void dl_solve(Context& c) {
     c.dl_prev = true;
     c.dl_prev_space = space;
     c.dl_lambda_old = lambda;
+    if (csf_basis) {
+        // the roots in the determinant layout, for <S^2>, RDMs and the flat-order vectors
+        c.evdet.alloc((size_t)nroot * c.nvec);
+        for (int k = 0; k < nroot; k++) csf_to_det(c, c.b.p + (size_t)k * N, c.evdet.p + (size_t)k * c.nvec);
+    }
+    c.csf_basis_solve = csf_basis;
     c.spin2.resize(nroot);
-    for (int k = 0; k < nroot; k++) c.spin2[k] = spin2_device(c, c.b.p + (size_t)k * N);
+    for (int k = 0; k < nroot; k++) c.spin2[k] = spin2_device(c, root_vector(c, k));
     FCIB_CUDA(cudaStreamSynchronize(c.stream));
     cudaEventDestroy(ev_start);
     cudaEventDestroy(e0);

@@ -223,6 +223,7 @@ struct EventPair {
 // configurations with N open shells of the spin-adapted space (csf.cu)
 struct CsfGroup {
     int N = 0, f = 0, nd = 0, nconf = 0;  // open shells, CSFs and determinants per configuration
+    int64_t zoff = 0;                     // first CSF of the group in a CSF vector
     DBuf<uint32_t> conf;                  // [nconf][2]: doubly occupied mask, open-shell mask
     DBuf<uint32_t> pats;                  // [nd] spin patterns over the open shells (bit k: alpha)
     DBuf<double> O;                       // [f][nd] coupling coefficients
@@ -301,6 +302,10 @@ struct Context {
     bool csf_ready = false;
     int csf_twoS = -1;
     int64_t ncsf = 0;
+    DBuf<double> csf_x, csf_s;  // determinant-space scratch of the CSF-basis sigma
+    DBuf<double> hd_csf;        // CSF diagonal of the last spin-adapted solve
+    DBuf<double> evdet;         // spin-adapted solves: the roots in the engine's determinant layout
+    bool csf_basis_solve = false;  // the last solve ran in the CSF basis (its roots are in evdet)
     std::vector<int64_t> dl_prev_space;
     std::vector<std::vector<std::pair<int64_t, double>>> dl_bad;
     std::vector<double> dl_lambda_old;  // eigenvalues of the previous solve's last iteration
@@ -333,8 +338,12 @@ inline void ensure_counter(Context& c) {
 
 // kernels / launchers (sigma.cu)
 void prepare_integrals(Context& c);
-// csf.cu: v <- its projection onto the spin sector of the target multiplicity
-void csf_project(Context& c, double* v);
+// csf.cu: the CSF basis of the target multiplicity (the Davidson space of spin_adapt): configuration
+// groups, x = P z (CSF coefficients -> engine-layout determinants), z = P^T x, the CSF diagonal
+void ensure_csf(Context& c);
+void csf_to_det(Context& c, const double* z, double* x);
+void det_to_csf(Context& c, const double* x, double* z);
+void csf_hdiag(Context& c, double* out);
 void sigma_fp64(Context& c, const double* C, double* S);
 float host_vmax(Context& c);  // max |V| (pair matrix) with a small margin, from a host copy
 void sigma_mixed(Context& c, const double* C, double* S, bool three);
@@ -370,7 +379,12 @@ void sym_host_decode(const Context& c, int64_t I, int64_t& ia, int64_t& ib);
 int64_t sym_host_encode(const Context& c, int64_t ia, int64_t ib);
 // davidson.cu
 void dl_solve(Context& c);
+// a root of the last solve in the engine's determinant layout
+const double* root_vector(Context& c, int root);
 std::vector<std::pair<double, int64_t>> lowest_keys(Context& c, const double* keys, int count);
+// the same over N keys with an optional mask (keys whose mask byte is 0 are skipped)
+std::vector<std::pair<double, int64_t>> lowest_keys(Context& c, const double* keys, int count, size_t N,
+                                                    const uint8_t* mask);
 double spin2_device(Context& c, const double* C);
 
 }  // namespace fcib

@@ -175,6 +175,12 @@ class FCISolver:
         capi.check(capi.lib().fcib_size(self._h, C.byref(n)))
         return n.value
 
+    def ncsf(self) -> int:
+        """Size of the CSF basis of the state's multiplicity (the Davidson space with CI_SPIN_ADAPT)."""
+        n = C.c_int64()
+        capi.check(capi.lib().fcib_ncsf(self._h, C.byref(n)))
+        return n.value
+
     def compute_energy(self) -> float:
         """FCISolver::compute_energy (forte/fci/fci_solver.cc:177-314)."""
         e = np.zeros(self.nroot)

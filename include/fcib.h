@@ -100,6 +100,9 @@ int fcib_set_options(fcib_ctx* ctx, const fcib_options* opt);
 
 /* determinant-space size in FCIVector flat order (sum over irrep blocks) */
 int fcib_size(fcib_ctx* ctx, int64_t* ndet);
+/* size of the CSF basis of the state's multiplicity in the target irrep, the Davidson space of
+ * spin-adapted solves (SpinAdapter::ncsf, forte/sparse_ci/ci_spin_adaptation.h:81-183) */
+int fcib_ncsf(fcib_ctx* ctx, int64_t* ncsf);
 
 /* Runs the Davidson-Liu FCI.  energies[nroot], spin2[nroot] (either may be NULL), iterations
  * (may be NULL).  Returns FCIB_ERR_NOT_CONVERGED when the solver did not converge and
@@ -220,6 +223,12 @@ int fcib_batch_destroy(fcib_batch* batch);
 /* energies[ninst * nroot] (instance-major), iterations[ninst], converged[ninst], device_ms = device
  * time of the launch; any output may be NULL */
 int fcib_batch_solve(fcib_batch* batch, double* energies, int* iterations, int* converged, double* device_ms);
+/* clock cycles per phase of the batched solves since the last call (then reset), summed over all
+ * CTAs: opposite-spin sigma, same-spin sigma, G update, subspace eigenproblem, residuals,
+ * preconditioner, collapse, Gram-Schmidt (cycles[8]).  Only the profiling build of the library
+ * (forte_b200.build.build(phases=True), compiled with -DFCIB_BATCH_PHASES) counts them; other
+ * builds return FCIB_ERR_UNSUPPORTED. */
+int fcib_batch_phase_cycles(unsigned long long* cycles);
 /* launch shape of later solves: threads per CTA (256 or 512), opposite-spin sigma tile (8, 16 or 32
  * pairs per work item), CTAs per instance (a thread-block cluster of 1, 2 or 4).  The default is
  * 512 threads, 32-pair tiles and clusters of 2 (1 when two CTAs cannot be co-scheduled). */

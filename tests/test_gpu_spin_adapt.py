@@ -1,7 +1,8 @@
-"""CI_SPIN_ADAPT: the Davidson space is kept in the spin sector of the state's multiplicity (every
-new vector projected onto its CSFs).  Energies are checked against the dense Hamiltonian of the
-oracle restricted to the S^2 = S(S+1) sector, <S^2> of the roots against S(S+1), and the golden
-C2v singlet; FP64 tolerance 1e-9 Eh, mixed precision 1e-8 Eh."""
+"""CI_SPIN_ADAPT: the Davidson solver works in the CSF basis of the state's multiplicity, like the
+reference (sigma through P^T H P, CSF diagonal, lowest-CSF guess).  Energies are checked against
+the dense Hamiltonian of the oracle restricted to the S^2 = S(S+1) sector, the CSF count against
+that sector's dimension, <S^2> of the roots against S(S+1), and the golden C2v singlet; FP64
+tolerance 1e-9 Eh, mixed precision 1e-8 Eh."""
 import numpy as np
 import pytest
 
@@ -13,7 +14,8 @@ pytestmark = pytest.mark.gpu
 OPTS = {"E_CONVERGENCE": 1e-11, "R_CONVERGENCE": 1e-7, "CI_SPIN_ADAPT": True, "DL_MAXITER": 200}
 
 
-def _sector_energies(n, na, nb, ints, mult, nroot):
+def _sector(n, na, nb, ints, mult, nroot):
+    """(lowest nroot energies, dimension) of the S^2 = S(S+1) sector of the dense Hamiltonian."""
     o = orc.Oracle(n, na, nb)
     o.set_integrals(ints)
     H = orc.dense_hamiltonian(o)
@@ -23,7 +25,11 @@ def _sector_energies(n, na, nb, ints, mult, nroot):
     w, V = np.linalg.eigh(S2)
     S = (mult - 1) / 2
     Q = V[:, np.abs(w - S * (S + 1)) < 1e-8]
-    return np.linalg.eigvalsh(Q.T @ H @ Q)[:nroot]
+    return np.linalg.eigvalsh(Q.T @ H @ Q)[:nroot], Q.shape[1]
+
+
+def _sector_energies(n, na, nb, ints, mult, nroot):
+    return _sector(n, na, nb, ints, mult, nroot)[0]
 
 
 @pytest.mark.parametrize("n,na,nb,mult", [(6, 3, 3, 1), (6, 3, 3, 3), (6, 3, 3, 5), (7, 4, 3, 2), (7, 4, 3, 4),
@@ -31,8 +37,10 @@ def _sector_energies(n, na, nb, ints, mult, nroot):
 def test_spin_adapted_roots_match_the_spin_sector(n, na, nb, mult):
     ints = synthetic(n, 3 * n, 12)
     s = FCISolver(StateInfo(na, nb, mult, na - nb), 3, ints, OPTS)
+    s.set_die_if_not_converged(True)
     s.compute_energy()
-    ref = _sector_energies(n, na, nb, ints, mult, 3)
+    ref, dim = _sector(n, na, nb, ints, mult, 3)
+    assert s.ncsf() == dim
     assert np.max(np.abs(np.array(s.energies()) - ref)) < 1e-9
     S = (mult - 1) / 2
     assert np.max(np.abs(np.array(s.spin2()) - S * (S + 1))) < 1e-8
