@@ -51,3 +51,16 @@ def test_create_without_gpu_fails_cleanly(L):
     assert rc in (capi.FCIB_ERR_CUDA, capi.FCIB_ERR_ARG)
     assert not h.value
     assert len(L.fcib_last_error()) > 0
+
+
+def test_default_build_has_no_phase_clocks(L):
+    """The batched solver's phase clocks exist only in the profiling build (-DFCIB_BATCH_PHASES)."""
+    out = (C.c_ulonglong * 8)()
+    assert L.fcib_batch_phase_cycles(out) == capi.FCIB_ERR_UNSUPPORTED
+    assert b"FCIB_BATCH_PHASES" in L.fcib_last_error()
+    assert L.fcib_batch_phase_cycles(None) == capi.FCIB_ERR_ARG
+
+
+def test_default_options_select_the_blocked_layout(L):
+    o = capi.default_options()
+    assert o.sym_blocked == 1 and o.spin_adapt == 0
