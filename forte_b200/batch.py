@@ -82,6 +82,6 @@ class BatchSolver:
         times = np.zeros(12)
         capi.check(capi.lib().fcib_batch_tune(self._h, C.byref(t), C.byref(c), C.byref(p), C.byref(cl),
                                               capi.dptr(times)))
-        names = [f"tile{tile}_{shape}" for tile in (8, 16, 32) for shape in ("256x1", "512x1", "256x2", "512x2")]
+        names = [f"tile{tile}_{shape}" for tile in (8, 16, 32) for shape in ("512x1", "256x2", "512x2", "512x4")]
         return {"threads": t.value, "ctas_per_sm": c.value, "pair_tile": p.value, "cluster": cl.value,
                 "times_ms": dict(zip(names, times.tolist()))}

@@ -1034,12 +1034,12 @@ int fcib_batch_set_shape(fcib_batch* b, int threads, int pair_tile, int cluster)
 // Autotuner: times the whole batch for each launch shape (threads per CTA x CTAs per instance, the
 // cluster size) and opposite-spin sigma tile, keeps the fastest and re-captures it into the solve
 // graph.  times_ms[12] (may be NULL) receives each candidate's time (0 when a shape does not fit),
-// tile-major: tiles 8, 16, 32 x shapes 256x1, 512x1, 256 in clusters of 2, 512 in clusters of 2.
+// tile-major: tiles 8, 16, 32 x shapes 512x1, 256 in clusters of 2, 512 in clusters of 2 and of 4.
 int fcib_batch_tune(fcib_batch* b, int* threads, int* ctas_per_sm, int* pair_tile, int* cluster, double* times_ms) {
     if (!b) { fcib::set_error("null batch"); return FCIB_ERR_ARG; }
     return fcib::guarded(nullptr, [&] {
         FCIB_CUDA(cudaSetDevice(b->device));
-        const int cand[4][2] = {{256, 1}, {512, 1}, {256, 2}, {512, 2}};  // threads, cluster size
+        const int cand[4][2] = {{512, 1}, {256, 2}, {512, 2}, {512, 4}};  // threads, cluster size
         const int tiles[3] = {8, 16, 32};
         double best = 1e300;
         int bt = b->threads, bp = b->pair_tile, bcl = b->cluster;

@@ -234,8 +234,8 @@ int fcib_batch_phase_cycles(unsigned long long* cycles);
  * 512 threads, 32-pair tiles and clusters of 2 (1 when two CTAs cannot be co-scheduled). */
 int fcib_batch_set_shape(fcib_batch* batch, int threads, int pair_tile, int cluster);
 /* autotuner: times the whole batch for each opposite-spin sigma tile (8, 16 or 32 pairs per work item)
- * and launch shape (threads per CTA x CTAs per instance, a thread-block cluster: 256x1, 512x1,
- * 256x2, 512x2), keeps the fastest for later solves; ctas_per_sm is 1; times_ms[12] (tile-major,
+ * and launch shape (threads per CTA x CTAs per instance, a thread-block cluster: 512x1, 256x2,
+ * 512x2, 512x4), keeps the fastest for later solves; ctas_per_sm is 1; times_ms[12] (tile-major,
  * 0 for shapes that do not fit) may be NULL */
 int fcib_batch_tune(fcib_batch* batch, int* threads, int* ctas_per_sm, int* pair_tile, int* cluster,
                     double* times_ms);

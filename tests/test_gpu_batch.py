@@ -51,7 +51,7 @@ def test_batch_autotuner_keeps_a_valid_shape():
     e0, _, cv0, _ = b.solve()
     t = b.tune()
     assert t["threads"] in (256, 512) and t["ctas_per_sm"] == 1 and t["pair_tile"] in (8, 16, 32)
-    assert t["cluster"] in (1, 2)
+    assert t["cluster"] in (1, 2, 4)
     assert any(v > 0 for v in t["times_ms"].values())
     e1, _, cv1, _ = b.solve()
     assert cv0.all() and cv1.all() and np.max(np.abs(e1 - e0)) < 1e-8
