@@ -49,6 +49,7 @@ class FcibOptions(C.Structure):
         ("same_spin_kernel", C.c_int),
         ("spin_adapt", C.c_int),
         ("sym_blocked", C.c_int),
+        ("spin_adapt_full_preconditioner", C.c_int),
     ]
 
 
@@ -83,6 +84,9 @@ SIGNATURES = {
     "fcib_set_options": (C.c_int, [_vp, C.POINTER(FcibOptions)]),
     "fcib_size": (C.c_int, [_vp, C.POINTER(C.c_int64)]),
     "fcib_ncsf": (C.c_int, [_vp, C.POINTER(C.c_int64)]),
+    "fcib_csf_to_det": (C.c_int, [_vp, _dp, _dp]),
+    "fcib_det_to_csf": (C.c_int, [_vp, _dp, _dp]),
+    "fcib_csf_hdiag": (C.c_int, [_vp, C.c_int, _dp]),
     "fcib_solve": (C.c_int, [_vp, _dp, _dp, C.POINTER(C.c_int)]),
     "fcib_reset_guess": (C.c_int, [_vp]),
     "fcib_get_vector": (C.c_int, [_vp, C.c_int, _dp]),

@@ -174,6 +174,7 @@ void fcib_default_options(fcib_options* o) {
     o->same_spin_kernel = FCIB_SAME_TC;
     o->spin_adapt = 0;
     o->sym_blocked = 1;
+    o->spin_adapt_full_preconditioner = 0;
 }
 
 const char* fcib_last_error(void) { return g_last_error.c_str(); }
@@ -334,6 +335,60 @@ int fcib_ncsf(fcib_ctx* ctx, int64_t* ncsf) {
         ensure_setup(ctx->c);
         ensure_csf(ctx->c);
         *ncsf = ctx->c.ncsf;
+    });
+}
+
+// CSF <-> determinant transforms and the CSF diagonal for host vectors (flat order)
+int fcib_csf_to_det(fcib_ctx* ctx, const double* z, double* cv) {
+    if (!ctx || !z || !cv) { set_error("null argument"); return FCIB_ERR_ARG; }
+    return guarded(ctx, [&] {
+        Context& c = ctx->c;
+        ensure_setup(c);
+        ensure_csf(c);
+        DBuf<double> dz, dx;
+        dz.upload(z, (size_t)c.ncsf, c.stream);
+        dx.alloc((size_t)c.nvec);
+        csf_to_det(c, dz.p, dx.p);
+        download_flat(c, dx.p, cv);
+    });
+}
+
+int fcib_det_to_csf(fcib_ctx* ctx, const double* cv, double* z) {
+    if (!ctx || !cv || !z) { set_error("null argument"); return FCIB_ERR_ARG; }
+    return guarded(ctx, [&] {
+        Context& c = ctx->c;
+        ensure_setup(c);
+        ensure_csf(c);
+        DBuf<double> dz, dx;
+        dx.alloc((size_t)c.nvec);
+        if (c.nirrep > 1 && !c.sym.on) FCIB_CUDA(cudaMemsetAsync(dx.p, 0, sizeof(double) * c.nvec, c.stream));
+        upload_flat(c, cv, dx.p);
+        dz.alloc((size_t)c.ncsf);
+        det_to_csf(c, dx.p, dz.p);
+        FCIB_CUDA(cudaMemcpyAsync(z, dz.p, sizeof(double) * c.ncsf, cudaMemcpyDeviceToHost, c.stream));
+        FCIB_CUDA(cudaStreamSynchronize(c.stream));
+    });
+}
+
+int fcib_csf_hdiag(fcib_ctx* ctx, int full, double* out) {
+    if (!ctx || !out) { set_error("null argument"); return FCIB_ERR_ARG; }
+    return guarded(ctx, [&] {
+        Context& c = ctx->c;
+        ensure_setup(c);
+        ensure_csf(c);
+        const int keep = c.opt.spin_adapt_full_preconditioner;
+        c.opt.spin_adapt_full_preconditioner = full ? 1 : 0;
+        DBuf<double> d;
+        d.alloc((size_t)c.ncsf);
+        try {
+            csf_hdiag(c, d.p);
+        } catch (...) {
+            c.opt.spin_adapt_full_preconditioner = keep;
+            throw;
+        }
+        c.opt.spin_adapt_full_preconditioner = keep;
+        FCIB_CUDA(cudaMemcpyAsync(out, d.p, sizeof(double) * c.ncsf, cudaMemcpyDeviceToHost, c.stream));
+        FCIB_CUDA(cudaStreamSynchronize(c.stream));
     });
 }
 

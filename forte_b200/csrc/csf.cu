@@ -128,6 +128,61 @@ __global__ void k_csf_map(const double* __restrict__ in, double* __restrict__ ou
     }
 }
 
+// The full CSF diagonal (CI_SPIN_ADAPT_FULL_PRECONDITIONER; form_Hdiag_csf with the full
+// preconditioner, fci_solver_initial_guess.cc:118-138):
+//     E_i = sum_m O_im^2 H_mm + 2 sum_{m < m'} O_im O_im' H_mm'.
+// Within a configuration the only off-diagonal elements join spin patterns m, m' that differ by one
+// alpha <-> beta swap of two open shells at positions a (alpha in m) and b (beta in m), orbitals
+// o_a, o_b: H_mm' = (-1)^(open shells strictly between a and b) * (o_a o_b | o_b o_a) (the doubly
+// occupied orbitals between them contribute to both spins' parities and cancel).  Kx[p][q] =
+// <pq|qp> of the alpha-beta block.  Patterns are in increasing mask order, so the index of m' is
+// its colex rank.  One CTA per configuration; one thread per CSF.
+__global__ void k_csf_full_diag(const double* __restrict__ hd, double* __restrict__ out,
+                                const uint32_t* __restrict__ conf, int nconf, int N, int nd, int f,
+                                const uint32_t* __restrict__ pats, const double* __restrict__ O, int n, int nbs,
+                                SymDev sd, int64_t zoff, const double* __restrict__ Kx) {
+    extern __shared__ __align__(16) unsigned char csf_smem[];
+    double* xs = reinterpret_cast<double*>(csf_smem);  // [nd] determinant diagonal
+    __shared__ int orb[32];                            // orbital of each open-shell position
+    for (int cf = blockIdx.x; cf < nconf; cf += gridDim.x) {
+        const uint32_t D = conf[2 * (size_t)cf], Om = conf[2 * (size_t)cf + 1];
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t rest = Om;
+            for (int k = 0; k < N; k++) {
+                orb[k] = __ffs(rest) - 1;
+                rest &= rest - 1;
+            }
+        }
+        for (int m = threadIdx.x; m < nd; m += blockDim.x) xs[m] = hd[csf_det_id(D, Om, pats[m], N, n, nbs, sd)];
+        __syncthreads();
+        for (int i = threadIdx.x; i < f; i += blockDim.x) {
+            const double* Oi = O + (size_t)i * nd;
+            double e = 0.0, off = 0.0;
+            for (int m = 0; m < nd; m++) {
+                const double om = Oi[m];
+                e = fma(om * om, xs[m], e);
+                if (om == 0.0) continue;
+                const uint32_t pat = pats[m];
+                for (uint32_t ra = pat; ra; ra &= ra - 1) {
+                    const int a = __ffs(ra) - 1;
+                    for (uint32_t rb = ~pat & ((N >= 32) ? 0xFFFFFFFFu : ((1u << N) - 1u)); rb; rb &= rb - 1) {
+                        const int b = __ffs(rb) - 1;
+                        const uint32_t mp = pat ^ (1u << a) ^ (1u << b);
+                        if (mp <= pat) continue;  // each pair once
+                        uint32_t j = 0, t = 1;    // colex rank of mp among the patterns
+                        for (uint32_t x = mp; x; x &= x - 1) j += d_binom[__ffs(x) - 1][t++];
+                        const int between = (a > b ? a - b : b - a) - 1;
+                        const double h = ((between & 1) ? -1.0 : 1.0) * Kx[orb[a] * n + orb[b]];
+                        off = fma(om * Oi[j], h, off);
+                    }
+                }
+            }
+            out[zoff + (int64_t)cf * f + i] = e + 2.0 * off;
+        }
+    }
+}
+
 // Configuration groups of the current state and target spin (rebuilt when either changes)
 void ensure_csf(Context& c) {
     const int twoS = c.multiplicity - 1, twoMs = c.na - c.nb;
@@ -210,7 +265,32 @@ void csf_to_det(Context& c, const double* z, double* x) {
     csf_map<0>(c, z, x);
 }
 void det_to_csf(Context& c, const double* x, double* z) { csf_map<1>(c, x, z); }
-void csf_hdiag(Context& c, double* out) { csf_map<2>(c, c.hdiag.p, out); }
+void csf_hdiag(Context& c, double* out) {
+    if (!c.opt.spin_adapt_full_preconditioner) {
+        csf_map<2>(c, c.hdiag.p, out);
+        return;
+    }
+    ensure_csf(c);
+    const int n = c.n;
+    std::vector<double> kx((size_t)n * n);
+    const size_t n2 = (size_t)n * n, n3 = n2 * n;
+    for (int p = 0; p < n; p++)
+        for (int q = 0; q < n; q++) kx[(size_t)p * n + q] = c.tei_ab[p * n3 + q * n2 + q * n + p];  // <pq|qp>
+    DBuf<double> Kx;
+    Kx.upload(kx, c.stream);
+    for (auto& gp : c.csf) {
+        CsfGroup& g = *gp;
+        if (g.f == 0) continue;
+        const size_t smem = (size_t)g.nd * 8;
+        FCIB_CHECK(smem + 1024 <= (size_t)c.smem_optin, FCIB_ERR_UNSUPPORTED, "spin adaptation: configuration too large");
+        FCIB_CUDA(cudaFuncSetAttribute(k_csf_full_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const int grid = std::min(g.nconf, 8 * c.num_sms);
+        k_csf_full_diag<<<grid, 128, smem, c.stream>>>(c.hdiag.p, out, g.conf.p, g.nconf, g.N, g.nd, g.f, g.pats.p,
+                                                       g.O.p, n, (int)c.nbs, sym_dev(c), g.zoff, Kx.p);
+        FCIB_KCHECK();
+    }
+    FCIB_CUDA(cudaStreamSynchronize(c.stream));  // Kx goes out of scope
+}
 
 }  // namespace fcib
 

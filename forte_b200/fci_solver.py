@@ -46,6 +46,7 @@ DEFAULT_OPTIONS = {
     "FCI_SAME_SPIN": "TC",          # TC | CUDA_CORES (mixed modes)
     "CI_SPIN_ADAPT": False,         # solve in the spin sector of the state's multiplicity
     "FCI_SYM_BLOCKED": True,        # with symmetry: vectors over the target irrep's blocks only
+    "CI_SPIN_ADAPT_FULL_PRECONDITIONER": False,  # CSF diagonal with the spin-exchange elements
 }
 
 
@@ -123,6 +124,7 @@ class FCISolver:
         o.same_spin_kernel = {"TC": capi.SAME_TC, "CUDA_CORES": capi.SAME_CUDA_CORES}[str(d["FCI_SAME_SPIN"]).upper()]
         o.spin_adapt = 1 if d["CI_SPIN_ADAPT"] else 0
         o.sym_blocked = 1 if d["FCI_SYM_BLOCKED"] else 0
+        o.spin_adapt_full_preconditioner = 1 if d["CI_SPIN_ADAPT_FULL_PRECONDITIONER"] else 0
         if o.preconditioner == capi.PRECOND_MLP and getattr(self, "_mlp", None) is None:
             from .learned_precond import load_weights
             self.set_mlp_weights(load_weights())
@@ -174,6 +176,26 @@ class FCISolver:
         n = C.c_int64()
         capi.check(capi.lib().fcib_size(self._h, C.byref(n)))
         return n.value
+
+    def csf_to_det(self, z: np.ndarray) -> np.ndarray:
+        """SpinAdapter::csf_C_to_det_C: CSF coefficients -> determinant vector (flat order)."""
+        z = np.ascontiguousarray(z, dtype=np.float64)
+        out = np.zeros(self.size())
+        capi.check(capi.lib().fcib_csf_to_det(self._h, capi.dptr(z), capi.dptr(out)))
+        return out
+
+    def det_to_csf(self, c: np.ndarray) -> np.ndarray:
+        """SpinAdapter::det_C_to_csf_C: determinant vector (flat order) -> CSF coefficients."""
+        c = np.ascontiguousarray(c, dtype=np.float64)
+        out = np.zeros(self.ncsf())
+        capi.check(capi.lib().fcib_det_to_csf(self._h, capi.dptr(c), capi.dptr(out)))
+        return out
+
+    def csf_hdiag(self, full=False) -> np.ndarray:
+        """FCISolver::form_Hdiag_csf: the CSF diagonal, plain (full=False) or full preconditioner."""
+        out = np.zeros(self.ncsf())
+        capi.check(capi.lib().fcib_csf_hdiag(self._h, 1 if full else 0, capi.dptr(out)))
+        return out
 
     def ncsf(self) -> int:
         """Size of the CSF basis of the state's multiplicity (the Davidson space with CI_SPIN_ADAPT)."""

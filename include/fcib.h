@@ -71,10 +71,12 @@ typedef struct fcib_options {
     int preconditioner;        /* FCIB_PRECOND_* */
     double mixed_switch;       /* mixed modes: residual norm at which sigma switches to FP64 */
     int same_spin_kernel;      /* mixed modes: FCIB_SAME_TC (default) or FCIB_SAME_CUDA_CORES */
-    int spin_adapt;            /* CI_SPIN_ADAPT: keep the Davidson space in the spin sector of the
-                                  state's multiplicity (projection onto its CSFs); default 0 */
+    int spin_adapt;            /* CI_SPIN_ADAPT: solve in the CSF basis of the state's multiplicity;
+                                  default 0 */
     int sym_blocked;           /* nirrep > 1: vectors and sigma cover only the target irrep's blocks
                                   (FCIVector flat order, default 1); 0 = the full C1 space with a mask */
+    int spin_adapt_full_preconditioner;  /* CI_SPIN_ADAPT_FULL_PRECONDITIONER: the CSF diagonal with
+                                  the configuration's spin-exchange elements; default 0 */
 } fcib_options;
 
 typedef struct fcib_ctx fcib_ctx;
@@ -103,6 +105,13 @@ int fcib_size(fcib_ctx* ctx, int64_t* ndet);
 /* size of the CSF basis of the state's multiplicity in the target irrep, the Davidson space of
  * spin-adapted solves (SpinAdapter::ncsf, forte/sparse_ci/ci_spin_adaptation.h:81-183) */
 int fcib_ncsf(fcib_ctx* ctx, int64_t* ncsf);
+/* SpinAdapter::csf_C_to_det_C / det_C_to_csf_C (ci_spin_adaptation.h:81-183): CSF coefficients
+ * z[ncsf] <-> a determinant vector c in FCIVector flat order (fcib_size elements) */
+int fcib_csf_to_det(fcib_ctx* ctx, const double* z, double* c);
+int fcib_det_to_csf(fcib_ctx* ctx, const double* c, double* z);
+/* the CSF diagonal of H (FCISolver::form_Hdiag_csf, fci_solver_initial_guess.cc:111-149):
+ * full = 0: sum_m O_im^2 H_mm; full = 1: <CSF_i|H|CSF_i> (the full preconditioner) */
+int fcib_csf_hdiag(fcib_ctx* ctx, int full, double* out);
 
 /* Runs the Davidson-Liu FCI.  energies[nroot], spin2[nroot] (either may be NULL), iterations
  * (may be NULL).  Returns FCIB_ERR_NOT_CONVERGED when the solver did not converge and

@@ -70,3 +70,56 @@ def test_spin_adaptation_needs_a_multiplicity():
     s = FCISolver(StateInfo(3, 3, 0), 1, ints, OPTS)
     with pytest.raises(RuntimeError, match="multiplicity"):
         s.compute_energy()
+
+
+def _flat_index(s, osym, irrep):
+    """C1 position of every FCIVector flat position (C1 cases: the identity)."""
+    sa, sb = s.strings(0), s.strings(1)
+    if not osym:
+        return np.arange(len(sa) * len(sb))
+
+    def irr(x):
+        h = 0
+        for i, o in enumerate(osym):
+            if (int(x) >> i) & 1:
+                h ^= o
+        return h
+
+    ha, hb = np.array([irr(x) for x in sa]), np.array([irr(x) for x in sb])
+    nirrep = 1 << max(osym).bit_length()
+    return np.concatenate([i * len(sb) + np.nonzero(hb == (h ^ irrep))[0] for h in range(nirrep)
+                           for i in np.nonzero(ha == h)[0]])
+
+
+@pytest.mark.parametrize("n,na,nb,mult,osym,irrep", [(6, 3, 3, 1, None, 0), (6, 3, 3, 3, None, 0),
+                                                    (7, 4, 3, 2, None, 0), (6, 3, 3, 1, [0, 1, 2, 3, 0, 1], 1),
+                                                    (6, 4, 2, 3, [0, 0, 1, 1, 0, 1], 0)])
+def test_csf_transforms_and_diagonals_match_the_dense_hamiltonian(n, na, nb, mult, osym, irrep):
+    """csf_C_to_det_C / det_C_to_csf_C are an isometry and its transpose; the CSF diagonal equals
+    sum_m O_im^2 H_mm, and the full preconditioner's diagonal equals <CSF_i|H|CSF_i> from the dense
+    oracle Hamiltonian (form_Hdiag_csf, fci_solver_initial_guess.cc:111-149)."""
+    ints = synthetic(n, 3 * n, 21, orbsym=osym)
+    s = FCISolver(StateInfo(na, nb, mult, na - nb, irrep), 1, ints, dict(OPTS))
+    nc = s.ncsf()
+    P = np.stack([s.csf_to_det(e) for e in np.eye(nc)], axis=1)
+    assert np.max(np.abs(P.T @ P - np.eye(nc))) < 1e-12
+    z = np.random.default_rng(3).normal(size=nc)
+    assert np.max(np.abs(s.det_to_csf(P @ z) - z)) < 1e-12
+    o = orc.Oracle(n, na, nb, osym, irrep)
+    o.set_integrals(ints)
+    idx = _flat_index(s, osym, irrep)
+    Hf = orc.dense_hamiltonian(o)[np.ix_(idx, idx)]
+    plain = (P ** 2).T @ np.diag(Hf)
+    full = np.einsum("mi,mn,ni->i", P, Hf, P)
+    assert np.max(np.abs(s.csf_hdiag(False) - plain)) < 1e-10
+    assert np.max(np.abs(s.csf_hdiag(True) - full)) < 1e-10
+
+
+def test_full_preconditioner_converges_to_the_same_roots():
+    ints = synthetic(7, 21, 8)
+    st = StateInfo(4, 3, 2, 1)
+    a = FCISolver(st, 2, ints, dict(OPTS))
+    b = FCISolver(st, 2, ints, dict(OPTS, CI_SPIN_ADAPT_FULL_PRECONDITIONER=True))
+    a.compute_energy()
+    b.compute_energy()
+    assert np.max(np.abs(np.array(a.energies()) - np.array(b.energies()))) < 1e-9
