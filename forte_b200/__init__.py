@@ -5,7 +5,7 @@ in include/fcib.h); this package holds its ctypes binding, the FCISolver mirror 
 reference's ActiveSpaceMethod interface and the integral input helpers.
 """
 from .integrals import ActiveSpaceIntegrals, from_chemist, synthetic, read_fcidump, dress_core  # noqa: F401
-from .fci_solver import FCISolver, StateInfo, RDMs, make_active_space_method, DEFAULT_OPTIONS  # noqa: F401
+from .fci_solver import FCISolver, GenCISolver, StateInfo, RDMs, make_active_space_method, DEFAULT_OPTIONS  # noqa: F401
 
-__all__ = ["ActiveSpaceIntegrals", "from_chemist", "synthetic", "read_fcidump", "dress_core", "FCISolver",
+__all__ = ["ActiveSpaceIntegrals", "from_chemist", "synthetic", "read_fcidump", "dress_core", "FCISolver", "GenCISolver",
            "StateInfo", "RDMs", "make_active_space_method", "DEFAULT_OPTIONS"]

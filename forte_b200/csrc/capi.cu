@@ -31,38 +31,6 @@ static int guarded(fcib_ctx* ctx, F&& f) {
     }
 }
 
-static void build_mask_and_maps(Context& c) {
-    c.block_to_c1.clear();
-    if (c.nirrep <= 1 || c.sym.on) {  // C1, or the blocked layout (its vectors are in flat order)
-        c.mask.release();
-        return;
-    }
-    std::vector<uint32_t> sa(c.nas), sb(c.nbs);
-    FCIB_CUDA(cudaMemcpy(sa.data(), c.A.str.p, 4 * c.nas, cudaMemcpyDeviceToHost));
-    FCIB_CUDA(cudaMemcpy(sb.data(), c.B.str.p, 4 * c.nbs, cudaMemcpyDeviceToHost));
-    auto sym = [&](uint32_t s) {
-        int h = 0;
-        for (int i = 0; i < c.n; i++)
-            if (s >> i & 1u) h ^= c.orbsym[i];
-        return h;
-    };
-    std::vector<int> ha(c.nas), hb(c.nbs);
-    for (int64_t i = 0; i < c.nas; i++) ha[i] = sym(sa[i]);
-    for (int64_t i = 0; i < c.nbs; i++) hb[i] = sym(sb[i]);
-    std::vector<uint8_t> m((size_t)c.ndet);
-    for (int64_t i = 0; i < c.nas; i++)
-        for (int64_t j = 0; j < c.nbs; j++) m[i * c.nbs + j] = ((ha[i] ^ hb[j]) == c.irrep);
-    c.mask.upload(m, c.stream);
-    // FCIVector flat order: alpha irrep blocks h, rows = alpha strings of irrep h in string
-    // order, columns = beta strings of irrep h ^ symmetry (forte/fci/fci_string_lists.cc:318-331)
-    for (int h = 0; h < c.nirrep; h++)
-        for (int64_t i = 0; i < c.nas; i++) {
-            if (ha[i] != h) continue;
-            for (int64_t j = 0; j < c.nbs; j++)
-                if (hb[j] == (h ^ c.irrep)) c.block_to_c1.push_back(i * c.nbs + j);
-        }
-}
-
 void ensure_setup(Context& c) {
     FCIB_CHECK(c.has_ints, FCIB_ERR_STATE, "integrals have not been set");
     FCIB_CHECK(c.has_state, FCIB_ERR_STATE, "state has not been set");
@@ -70,6 +38,8 @@ void ensure_setup(Context& c) {
     c.mlp_tables_ready = false;
     c.csf_ready = false;
     FCIB_CHECK(c.na <= c.n && c.nb <= c.n, FCIB_ERR_ARG, "more electrons than orbitals");
+    FCIB_CHECK(c.gas.ngas == 0 || (int)c.gas.space.size() == c.n, FCIB_ERR_STATE,
+               "the GAS spaces were set for a different number of orbitals");
     bool fold = (c.na >= 1 && c.nb >= 1);
     c.tgtR16.release();
     c.vmax = 0.0f;
@@ -81,7 +51,7 @@ void ensure_setup(Context& c) {
     FCIB_CUDA(cudaStreamSynchronize(c.stream));
     prepare_integrals(c);
     build_sym_space(c);
-    build_mask_and_maps(c);
+    build_layout_maps(c);
     c.hdiag.alloc((size_t)c.nvec);
     compute_hdiag(c, c.hdiag.p);
     FCIB_CUDA(cudaStreamSynchronize(c.stream));
@@ -95,27 +65,28 @@ void sigma_dispatch(Context& c, const double* b, double* s, int precision) {
     else throw Error{FCIB_ERR_ARG, "unknown sigma precision"};
 }
 
-// host flat (FCIVector order) <-> device layout (C1, flat order itself when blocked, or C1 with a mask)
+// host flat order (FCIVector, or GenCIVector with GAS) <-> device layout (C1, the blocked layout,
+// or either with a mask; the flat map holds the layout index of every flat position)
 static void upload_flat(Context& c, const double* flat, double* dev) {
-    if (c.nirrep <= 1 || c.sym.on) {
+    if (!c.mask.p) {
         FCIB_CUDA(cudaMemcpyAsync(dev, flat, sizeof(double) * c.nvec, cudaMemcpyHostToDevice, c.stream));
         return;
     }
-    std::vector<double> full((size_t)c.ndet, 0.0);
-    for (size_t i = 0; i < c.block_to_c1.size(); i++) full[c.block_to_c1[i]] = flat[i];
-    FCIB_CUDA(cudaMemcpyAsync(dev, full.data(), sizeof(double) * c.ndet, cudaMemcpyHostToDevice, c.stream));
+    std::vector<double> full((size_t)c.nvec, 0.0);
+    for (size_t i = 0; i < c.flat_map.size(); i++) full[c.flat_map[i]] = flat[i];
+    FCIB_CUDA(cudaMemcpyAsync(dev, full.data(), sizeof(double) * c.nvec, cudaMemcpyHostToDevice, c.stream));
     FCIB_CUDA(cudaStreamSynchronize(c.stream));
 }
 static void download_flat(Context& c, const double* dev, double* flat) {
-    if (c.nirrep <= 1 || c.sym.on) {
+    if (!c.mask.p) {
         FCIB_CUDA(cudaMemcpyAsync(flat, dev, sizeof(double) * c.nvec, cudaMemcpyDeviceToHost, c.stream));
         FCIB_CUDA(cudaStreamSynchronize(c.stream));
         return;
     }
-    std::vector<double> full((size_t)c.ndet);
-    FCIB_CUDA(cudaMemcpyAsync(full.data(), dev, sizeof(double) * c.ndet, cudaMemcpyDeviceToHost, c.stream));
+    std::vector<double> full((size_t)c.nvec);
+    FCIB_CUDA(cudaMemcpyAsync(full.data(), dev, sizeof(double) * c.nvec, cudaMemcpyDeviceToHost, c.stream));
     FCIB_CUDA(cudaStreamSynchronize(c.stream));
-    for (size_t i = 0; i < c.block_to_c1.size(); i++) flat[i] = full[c.block_to_c1[i]];
+    for (size_t i = 0; i < c.flat_map.size(); i++) flat[i] = full[c.flat_map[i]];
 }
 // RDM blocks -> caller buffers; spin-free sums follow FCIVector::compute_rdms
 // (fci_vector_rdm.cc:120-126): G1 = g1a + g1b, G2 = (g2aa + (g2ab(pqrs) + g2ab(qpsr))) + g2bb.
@@ -147,9 +118,8 @@ static void rdms_to_outputs(const RdmBlocks& b, int level, int spin_free, double
     }
     (void)n4;
 }
-static int64_t flat_size(const Context& c) {
-    return (c.nirrep <= 1 || c.sym.on) ? c.nvec : (int64_t)c.block_to_c1.size();
-}
+// masked layouts (a mask is allocated) map every flat position; otherwise the layout is the flat order
+static int64_t flat_size(const Context& c) { return c.mask.p ? (int64_t)c.flat_map.size() : c.nvec; }
 
 }  // namespace fcib
 
@@ -294,6 +264,63 @@ int fcib_set_state(fcib_ctx* ctx, int na, int nb, int irrep, int multiplicity, i
     });
 }
 
+// GenCISolver's determinant space (forte/genci/genci_solver.h; the GAS spaces of MOSpaceInfo and the
+// bounds of StateInfo::gas_min/gas_max)
+int fcib_set_gas(fcib_ctx* ctx, int ngas, const int* space, const int* gas_min, const int* gas_max) {
+    if (!ctx) { set_error("null context"); return FCIB_ERR_ARG; }
+    return guarded(ctx, [&] {
+        Context& c = ctx->c;
+        FCIB_CHECK(c.has_ints, FCIB_ERR_STATE, "set integrals before the GAS spaces");
+        FCIB_CHECK(ngas >= 0 && ngas <= kMaxGas, FCIB_ERR_ARG, "the number of GAS spaces must be 0..6");
+        GasSpace g;
+        if (ngas > 0) {
+            FCIB_CHECK(space && gas_min && gas_max, FCIB_ERR_ARG, "null argument");
+            g.ngas = ngas;
+            g.space.assign(space, space + c.n);
+            for (int p = 0; p < c.n; p++) {
+                FCIB_CHECK(space[p] >= 0 && space[p] < ngas, FCIB_ERR_ARG, "orbital GAS space out of range");
+                g.orbs[space[p]] |= 1u << p;
+            }
+            for (int k = 0; k < ngas; k++) {
+                FCIB_CHECK(g.orbs[k] != 0u, FCIB_ERR_ARG, "every GAS space needs at least one orbital");
+                FCIB_CHECK(gas_min[k] >= 0 && gas_max[k] >= 0, FCIB_ERR_ARG, "GAS electron bounds must be >= 0");
+                g.emin[k] = gas_min[k];
+                g.emax[k] = gas_max[k];
+            }
+        }
+        c.gas = std::move(g);
+        c.tables_ready = false;  // the layout maps, stored vectors and the restart state go
+        c.solved = false;
+        c.dl_prev = false;
+        c.csf_ready = false;
+    });
+}
+
+// FCIStringLists / GenCIStringLists::make_determinants: the strings of every flat position
+int fcib_determinants(fcib_ctx* ctx, uint32_t* alfa, uint32_t* beta) {
+    if (!ctx || !alfa || !beta) { set_error("null argument"); return FCIB_ERR_ARG; }
+    return guarded(ctx, [&] {
+        Context& c = ctx->c;
+        ensure_setup(c);
+        std::vector<uint32_t> sa(c.nas), sb(c.nbs);
+        FCIB_CUDA(cudaMemcpy(sa.data(), c.A.str.p, 4 * c.nas, cudaMemcpyDeviceToHost));
+        FCIB_CUDA(cudaMemcpy(sb.data(), c.B.str.p, 4 * c.nbs, cudaMemcpyDeviceToHost));
+        const int64_t nf = flat_size(c);
+        for (int64_t f = 0; f < nf; f++) {
+            const int64_t I = c.mask.p ? c.flat_map[f] : f;
+            int64_t ia, ib;
+            if (c.sym.on) {
+                sym_host_decode(c, I, ia, ib);
+            } else {
+                ia = I / c.nbs;
+                ib = I % c.nbs;
+            }
+            alfa[f] = sa[ia];
+            beta[f] = sb[ib];
+        }
+    });
+}
+
 int fcib_set_options(fcib_ctx* ctx, const fcib_options* o) {
     if (!ctx || !o) { set_error("null argument"); return FCIB_ERR_ARG; }
     return guarded(ctx, [&] {
@@ -361,7 +388,6 @@ int fcib_det_to_csf(fcib_ctx* ctx, const double* cv, double* z) {
         ensure_csf(c);
         DBuf<double> dz, dx;
         dx.alloc((size_t)c.nvec);
-        if (c.nirrep > 1 && !c.sym.on) FCIB_CUDA(cudaMemsetAsync(dx.p, 0, sizeof(double) * c.nvec, c.stream));
         upload_flat(c, cv, dx.p);
         dz.alloc((size_t)c.ncsf);
         det_to_csf(c, dx.p, dz.p);
@@ -426,7 +452,7 @@ int fcib_solve(fcib_ctx* ctx, double* energies, double* spin2, int* iterations) 
 static void max_abs_elements(Context& c, int root, int num_dets, std::vector<double>& absv, std::vector<double>& val,
                              std::vector<int>& irr, std::vector<int64_t>& ia, std::vector<int64_t>& ib) {
     const int64_t N = c.nvec;
-    const int64_t nflat = (c.nirrep <= 1 || c.sym.on) ? N : (int64_t)c.block_to_c1.size();
+    const int64_t nflat = flat_size(c);
     num_dets = (int)std::min<int64_t>(num_dets, nflat);
     absv.assign(num_dets, 0.0);
     val.assign(num_dets, 0.0);
@@ -462,18 +488,20 @@ static void max_abs_elements(Context& c, int root, int num_dets, std::vector<dou
         for (int h = 0; h < 8; h++) blk[h + 1] = blk[h] + cnta[h] * cntb[h ^ (c.nirrep > 1 ? c.irrep : 0)];
         for (int64_t i = 0; i < c.nas; i++) pa[i] = blk[ha[i]] + ra[i] * cntb[ha[i] ^ (c.nirrep > 1 ? c.irrep : 0)];
     }
-    // vector index -> (FCIVector flat position, alpha irrep, addresses within the irrep blocks)
+    // vector index -> (flat position, alpha irrep, addresses within the irrep blocks); the flat
+    // position (FCIVector order, or GenCIVector order with GAS) orders equal |C|
     auto locate = [&](int64_t idx, int64_t& flat, int& h, int64_t& ai, int64_t& bi) {
-        if (c.sym.on) {  // the blocked layout is the flat order
+        if (c.sym.on) {  // the blocked layout is the FCIVector flat order
             flat = idx;
             sym_host_locate(c, idx, h, ai, bi);
-            return;
+        } else {
+            const int64_t i = idx / c.nbs, j = idx % c.nbs;
+            flat = pa[i] + rb[j];
+            h = ha[i];
+            ai = ra[i];
+            bi = rb[j];
         }
-        const int64_t i = idx / c.nbs, j = idx % c.nbs;
-        flat = pa[i] + rb[j];
-        h = ha[i];
-        ai = ra[i];
-        bi = rb[j];
+        if (c.gas.ngas > 0) flat = gas_flat_position(c, idx);
     };
     std::vector<std::pair<std::pair<double, int64_t>, int64_t>> order;  // ((-|C|, flat), vector index)
     for (auto& e : sel) {

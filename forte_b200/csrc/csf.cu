@@ -214,6 +214,13 @@ void ensure_csf(Context& c) {
                 for (int p = 0; p < n; p++)
                     if (Om >> p & 1u) h ^= c.orbsym[p];
                 if (h != c.irrep) continue;
+                // GAS: the electrons of a space are a function of the configuration
+                bool in_gas = true;
+                for (int k = 0; k < c.gas.ngas && in_gas; k++) {
+                    const int e = 2 * __builtin_popcount(D & c.gas.orbs[k]) + __builtin_popcount(Om & c.gas.orbs[k]);
+                    in_gas = e >= c.gas.emin[k] && e <= c.gas.emax[k];
+                }
+                if (!in_gas) continue;
                 byN[N].push_back(D);
                 byN[N].push_back(Om);
             }
@@ -260,8 +267,8 @@ static void csf_map(Context& c, const double* in, double* out) {
 }
 
 void csf_to_det(Context& c, const double* z, double* x) {
-    // the masked C1 layout also holds determinants of other irreps, which no configuration covers
-    if (c.nirrep > 1 && !c.sym.on) FCIB_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * c.nvec, c.stream));
+    // a masked layout also holds determinants that no configuration covers
+    if (c.mask.p) FCIB_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * c.nvec, c.stream));
     csf_map<0>(c, z, x);
 }
 void det_to_csf(Context& c, const double* x, double* z) { csf_map<1>(c, x, z); }

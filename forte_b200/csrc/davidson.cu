@@ -633,7 +633,7 @@ double spin2_device(Context& c, const double* C) {
 // the `count` smallest keys[] of the determinants in the target irrep with their C1 indices, sorted by
 // (key, index); ties at the boundary are resolved by the index
 std::vector<std::pair<double, int64_t>> lowest_keys(Context& c, const double* keys, int count) {
-    return lowest_keys(c, keys, count, (size_t)c.nvec, (c.nirrep > 1 && !c.sym.on) ? c.mask.p : nullptr);
+    return lowest_keys(c, keys, count, (size_t)c.nvec, c.mask.p);
 }
 std::vector<std::pair<double, int64_t>> lowest_keys(Context& c, const double* keys, int count, size_t N,
                                                     const uint8_t* mask) {
@@ -716,7 +716,7 @@ void dl_solve(Context& c) {
     }
     const int64_t N = csf_basis ? c.ncsf : c.nvec;
     int64_t Neff = N;
-    if (!csf_basis && c.nirrep > 1 && !c.sym.on) {
+    if (!csf_basis && c.mask.p) {
         std::vector<uint8_t> hm(N);
         FCIB_CUDA(cudaMemcpy(hm.data(), c.mask.p, N, cudaMemcpyDeviceToHost));
         Neff = 0;
@@ -785,6 +785,12 @@ void dl_solve(Context& c) {
     std::vector<int64_t> space = {c.n, c.na, c.nb, c.irrep, c.nirrep, (int64_t)N, Neff, nroot, m,
                                   o.spin_adapt ? c.multiplicity : -1};
     for (int x : c.orbsym) space.push_back(x);
+    space.push_back(c.gas.ngas);  // the GAS restriction is part of the space too
+    for (int k = 0; k < c.gas.ngas; k++) {
+        space.push_back(c.gas.orbs[k]);
+        space.push_back(c.gas.emin[k]);
+        space.push_back(c.gas.emax[k]);
+    }
     const bool restart = c.dl_prev && c.dl_prev_space == space &&
                          (int64_t)num_guess_states * o.dets_per_guess < Neff;
     c.dl_prev = false;  // set again when this solve completes

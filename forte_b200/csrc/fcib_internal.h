@@ -229,6 +229,21 @@ struct CsfGroup {
     DBuf<double> O;                       // [f][nd] coupling coefficients
 };
 
+// generalized active spaces (gas.cu): bounds on the electrons in each orbital space
+constexpr int kMaxGas = 6;
+struct GasSpace {
+    int ngas = 0;                          // 0: no restriction
+    std::vector<int> space;                // [n] space of each orbital
+    int emin[kMaxGas] = {}, emax[kMaxGas] = {};  // bounds on alpha + beta electrons per space
+    uint32_t orbs[kMaxGas] = {};           // orbitals of each space
+    // string classes of the current state (GenCIStringLists): per C1 string its class (-1: none)
+    // and address in it; strings per class; flat offset of each (alpha class, beta class) block
+    std::vector<int32_t> acls, bcls;
+    std::vector<int64_t> aadd, badd, acnt, bcnt, blk_off;
+    int ncb = 0;
+    int64_t ndet = 0;                      // determinants of the GAS space
+};
+
 struct Context {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -254,7 +269,8 @@ struct Context {
     DBuf<double> M2a, M2b;  // same-spin <pq||rs> over pairs p>q, r>s
     DBuf<double> Ha, Hb;  // one-body matrices (used when h is not folded)
     bool fold_h = true;
-    DBuf<uint8_t> mask;   // determinant in target irrep (only when nirrep > 1)
+    DBuf<uint8_t> mask;   // kept determinants of a masked layout (gas.cu), else unallocated
+    GasSpace gas;         // GAS restriction (ngas = 0: none)
     // work vectors
     DBuf<double> ct;      // transposed C for the beta same-spin terms
     DBuf<uint16_t> tgtR16; // beta replacement targets [column/8][string][column%8] for the tensor-core kernel
@@ -273,8 +289,9 @@ struct Context {
     std::vector<double> energies, spin2;
     int iterations = 0;
     bool solved = false;
-    // flat-order maps for nirrep > 1 (reference block layout <-> C1 layout)
-    std::vector<int64_t> block_to_c1;
+    // masked layouts: layout index of every position of the caller's flat order (FCIVector or
+    // GenCIVector order); empty when the layout is the flat order itself
+    std::vector<int64_t> flat_map;
     DBuf<int> counter;    // work counters for persistent kernels
     DBuf<double> red;     // reduction scratch
     // timers and status of the last solve
@@ -348,6 +365,9 @@ void sigma_fp64(Context& c, const double* C, double* S);
 float host_vmax(Context& c);  // max |V| (pair matrix) with a small margin, from a host copy
 void sigma_mixed(Context& c, const double* C, double* S, bool three);
 void apply_mask(Context& c, double* v);
+// gas.cu: mask and flat map of the layout (masked C1 with symmetry, GAS); GenCIVector position
+void build_layout_maps(Context& c);
+int64_t gas_flat_position(const Context& c, int64_t I);
 void export_list(int n, int k, int kind, int p, int q, int r, int s, std::vector<int8_t>& sign,
                  std::vector<uint32_t>& I, std::vector<uint32_t>& J, cudaStream_t st);
 void compute_hdiag(Context& c, double* out);

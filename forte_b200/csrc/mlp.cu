@@ -572,7 +572,6 @@ int fcib_precondition(fcib_ctx* ctx, const double* r, double lambda, double* out
         rn = std::sqrt(rn);
         DBuf<double> d;
         d.alloc(c.nvec);
-        if (c.nirrep > 1 && !c.sym.on) FCIB_CUDA(cudaMemsetAsync(d.p, 0, sizeof(double) * c.nvec, c.stream));
         upload_flat(c, r, d.p);
         k_diag_correction<<<4 * c.num_sms, 256, 0, c.stream>>>(d.p, c.hdiag.p, lambda, (size_t)c.nvec);
         FCIB_KCHECK();

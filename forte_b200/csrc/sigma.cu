@@ -645,8 +645,8 @@ static void transpose(Context& c, const double* in, double* out, int rows, int c
     FCIB_KCHECK();
 }
 void apply_mask(Context& c, double* v) {
-    if (c.nirrep <= 1 || c.sym.on || !c.mask.p) return;
-    k_apply_mask<<<4 * c.num_sms, 256, 0, c.stream>>>(v, c.mask.p, (size_t)c.ndet);
+    if (!c.mask.p) return;
+    k_apply_mask<<<4 * c.num_sms, 256, 0, c.stream>>>(v, c.mask.p, (size_t)c.nvec);
     FCIB_KCHECK();
 }
 

@@ -20,12 +20,15 @@ from .integrals import ActiveSpaceIntegrals
 
 @dataclass(frozen=True)
 class StateInfo:
-    """Active-space state: electron counts, 2S+1, 2*Ms and irrep (forte StateInfo)."""
+    """Active-space state: electron counts, 2S+1, 2*Ms, irrep and the GAS electron bounds per space
+    (forte StateInfo, base_classes/state_info.h; gas_min/gas_max are read by GenCISolver only)."""
     na: int
     nb: int
     multiplicity: int = 1
     twice_ms: int = 0
     irrep: int = 0
+    gas_min: tuple = ()
+    gas_max: tuple = ()
 
 
 #: Forte option names understood by FCISolver.set_options with their defaults
@@ -354,6 +357,16 @@ class FCISolver:
             return RDMs(True, g1=g1a, g2=g2[0], **g3)
         return RDMs(False, g1a=g1a, g1b=g1b, g2aa=g2[0], g2ab=g2[1], g2bb=g2[2], **g3)
 
+    def determinants(self):
+        """Alpha and beta strings (bit p = orbital p) of every flat position
+        (FCIStringLists / GenCIStringLists::make_determinants)."""
+        N = self.size()
+        a = np.zeros(max(N, 1), dtype=np.uint32)
+        b = np.zeros(max(N, 1), dtype=np.uint32)
+        capi.check(capi.lib().fcib_determinants(self._h, a.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                                b.ctypes.data_as(C.POINTER(C.c_uint32))))
+        return a[:N], b[:N]
+
     # ---- string tables (parity checks) ----------------------------------------------------
     def strings(self, spin):
         cnt = C.c_int64()
@@ -377,9 +390,57 @@ class FCISolver:
         return sg[:n], I[:n], J[:n]
 
 
+class GenCISolver(FCISolver):
+    """GenCISolver (forte/genci/genci_solver.h): the FCISolver interface over a generalized active
+    space -- the determinants whose number of electrons in each orbital space k lies in
+    [state.gas_min[k], state.gas_max[k]].
+
+    gas_spaces: the active orbitals of GAS1, GAS2, ... (what MOSpaceInfo.pos_in_space("GASn",
+    "ACTIVE") returns); every active orbital belongs to one space, and empty spaces may only trail.
+    Missing bounds default to 0 and 2 * size, as make_state_weights_map sets them
+    (base_classes/active_space_solver.cc:706-740).  Vectors are in GenCIVector flat order.
+    """
+
+    def __init__(self, state: StateInfo, nroot: int, ints: ActiveSpaceIntegrals, gas_spaces, options=None,
+                 device=0):
+        super().__init__(state, nroot, ints, options, device)
+        self.set_gas(gas_spaces, state.gas_min, state.gas_max)
+
+    def set_gas(self, gas_spaces, gas_min=(), gas_max=()):
+        """Set the GAS spaces and bounds; no spaces restores the full determinant space."""
+        spaces = [sorted(int(p) for p in sp) for sp in gas_spaces]
+        while spaces and not spaces[-1]:
+            spaces.pop()
+        n = self.ints.n
+        if len(spaces) > 6:
+            raise ValueError("at most six GAS spaces")
+        if any(not sp for sp in spaces):
+            raise ValueError("an empty GAS space is followed by a non-empty one")
+        owner = [-1] * n
+        for k, sp in enumerate(spaces):
+            for p in sp:
+                if not 0 <= p < n or owner[p] >= 0:
+                    raise ValueError(f"orbital {p} is outside the active space or in two GAS spaces")
+                owner[p] = k
+        if spaces and n and min(owner) < 0:
+            raise ValueError("every active orbital must belong to a GAS space")
+        mn = [int(gas_min[k]) if k < len(gas_min) else 0 for k in range(len(spaces))]
+        mx = [int(gas_max[k]) if k < len(gas_max) else 2 * len(sp) for k, sp in enumerate(spaces)]
+        ng = len(spaces)
+        self.gas_spaces, self.gas_min, self.gas_max = spaces, mn, mx
+        capi.check(capi.lib().fcib_set_gas(self._h, ng, (C.c_int * max(n, 1))(*owner),
+                                           (C.c_int * max(ng, 1))(*mn), (C.c_int * max(ng, 1))(*mx)))
+
+
 def make_active_space_method(method: str, state: StateInfo, nroot: int, ints: ActiveSpaceIntegrals,
-                             options=None, device=0):
-    """make_active_space_method (forte/base_classes/active_space_method.cc:126-184), FCI only."""
-    if method.upper() != "FCI":
-        raise ValueError(f"active space method {method} is not provided by the B200 engine")
-    return FCISolver(state, nroot, ints, options, device)
+                             options=None, device=0, gas_spaces=None):
+    """make_active_space_method (forte/base_classes/active_space_method.cc:126-184): "FCI", or
+    "GENCI" with the GAS orbital spaces."""
+    m = method.upper()
+    if m == "FCI":
+        return FCISolver(state, nroot, ints, options, device)
+    if m == "GENCI":
+        if gas_spaces is None:
+            raise ValueError("GENCI needs the GAS orbital spaces (gas_spaces)")
+        return GenCISolver(state, nroot, ints, gas_spaces, options, device)
+    raise ValueError(f"active space method {method} is not provided by the B200 engine")

@@ -7,7 +7,9 @@
  * pointers in the engine's layout and a CUDA stream handle passed as void*.  The engine's layout
  * is the C1 layout (na_str x nb_str row-major) without point-group symmetry; with symmetry it is
  * FCIVector flat order (fcib_size elements, the target irrep's blocks only) by default, or the C1
- * layout with zeros outside the target irrep when fcib_options.sym_blocked = 0.
+ * layout with zeros outside the target irrep when fcib_options.sym_blocked = 0.  With GAS spaces
+ * (fcib_set_gas) host vectors follow GenCIVector flat order (fcib_size elements) and device
+ * vectors keep the engine's layout with zeros outside the GAS space.
  *
  * Each entry point replaces a piece of Forte's FCISolver path (paths relative to the Forte
  * project root):
@@ -24,6 +26,8 @@
  *   fcib_rdms               -- FCISolver::rdms / FCIVector::compute_rdms (fci_solver_rdms.cc:40-104,
  *                              fci_vector_rdm.cc:43-393)
  *   fcib_spin2              -- FCIVector::compute_spin2 (fci_vector_spin2.cc:38-75)
+ *   fcib_set_gas            -- GenCISolver's GAS space (forte/genci/genci_solver.h, genci_string_lists.cc:58-210)
+ *   fcib_determinants       -- FCIStringLists / GenCIStringLists::make_determinants (genci_string_lists.cc:276-291)
  *   fcib_strings / fcib_string_list -- FCIStringLists strings and VO/OO/VVOO lists
  *                              (fci_string_lists.cc:52-205, fci_string_vo_list.cc:54-140,
  *                              fci_string_oo_list.cc:59-115, fci_string_vvoo_list.cc:56-187)
@@ -99,9 +103,20 @@ int fcib_set_integrals(fcib_ctx* ctx, int n, int nirrep, const int* orbsym, doub
  * guess, number of roots and the root returned by the solver's energy. */
 int fcib_set_state(fcib_ctx* ctx, int na, int nb, int irrep, int multiplicity, int nroot, int root);
 int fcib_set_options(fcib_ctx* ctx, const fcib_options* opt);
+/* Generalized active spaces (GenCISolver, forte/genci/genci_solver.h): keep the determinants whose
+ * number of electrons (alpha + beta) in each space k lies in [gas_min[k], gas_max[k]]
+ * (StateInfo::gas_min/gas_max).  space[p] in 0..ngas-1 is the space of active orbital p (GAS1..GAS6
+ * of MOSpaceInfo, each non-empty, ngas <= 6); ngas = 0 restores the full space.  Call after
+ * fcib_set_integrals.  Host vectors then follow GenCIVector flat order: per occupation pair of
+ * get_ci_occupation_patterns (ci_occupation.cc:131-170) and alpha irrep, the block of the alpha
+ * and beta string classes (genci_string_address.cc:81-133, string_lists_makers.cc:65-127). */
+int fcib_set_gas(fcib_ctx* ctx, int ngas, const int* space, const int* gas_min, const int* gas_max);
 
-/* determinant-space size in FCIVector flat order (sum over irrep blocks) */
+/* determinant-space size in flat order: FCIVector (sum over irrep blocks) or GenCIVector */
 int fcib_size(fcib_ctx* ctx, int64_t* ndet);
+/* alpha and beta strings (bit p = orbital p) of every flat position, fcib_size entries each
+ * (FCIStringLists / GenCIStringLists::make_determinants, genci_string_lists.cc:276-291) */
+int fcib_determinants(fcib_ctx* ctx, uint32_t* alfa, uint32_t* beta);
 /* size of the CSF basis of the state's multiplicity in the target irrep, the Davidson space of
  * spin-adapted solves (SpinAdapter::ncsf, forte/sparse_ci/ci_spin_adaptation.h:81-183) */
 int fcib_ncsf(fcib_ctx* ctx, int64_t* ncsf);
