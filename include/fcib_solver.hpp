@@ -55,6 +55,15 @@ class Solver {
         root_ = root;
         check(fcib_set_state(ctx_, na, nb, irrep, multiplicity, nroot, root));
     }
+    /* GenCISolver's GAS space: space[p] = GAS space of active orbital p, electron bounds per space;
+     * an empty space vector restores the full determinant space */
+    void set_gas(const std::vector<int>& space, const std::vector<int>& gas_min, const std::vector<int>& gas_max) {
+        int ngas = 0;
+        for (int k : space) ngas = k + 1 > ngas ? k + 1 : ngas;
+        if ((int)gas_min.size() < ngas || (int)gas_max.size() < ngas)
+            throw std::runtime_error("GAS bounds are needed for every space");
+        check(fcib_set_gas(ctx_, ngas, space.empty() ? nullptr : space.data(), gas_min.data(), gas_max.data()));
+    }
     fcib_options& options() { return opt_; }
     void set_die_if_not_converged(bool v) { opt_.die_if_not_converged = v ? 1 : 0; }
 
@@ -74,6 +83,13 @@ class Solver {
     const std::vector<double>& spin2() const { return spin2_; }
     int iterations() const { return iterations_; }
     int nroot() const { return nroot_; }
+
+    /* determinant-space size in flat order (FCIVector, or GenCIVector with GAS spaces) */
+    int64_t size() {
+        int64_t nd = 0;
+        check(fcib_size(ctx_, &nd));
+        return nd;
+    }
 
     /* eigenvector of a root in FCIVector flat order */
     std::vector<double> evec(int root) {

@@ -1,6 +1,7 @@
 // C++ driver of the engine through include/fcib_solver.hpp, the way a Forte-side ActiveSpaceMethod
 // adapter calls it: integrals and state in, compute_energy, spin-free and spin-dependent RDMs of the
-// roots, and transition 1-RDMs against a second solver whose state belongs to another irrep.
+// roots, transition 1-RDMs against a second solver whose state belongs to another irrep, and a
+// GenCISolver-style solve on a GAS space (at most two electrons in the upper half of the orbitals).
 //
 //   fcib_solver_main <input.bin> <output.bin>
 //
@@ -8,7 +9,8 @@
 //   int32 orbsym[n]; float64 scalar, oei[n*n], tei_aa[n^4], tei_ab[n^4] (oei_b = oei_a, tei_bb = tei_aa)
 // output.bin: float64 energies[nroot], spin2[nroot], iterations, then for root 0 the spin-dependent
 //   g1a, g1b [n^2], g2aa, g2ab, g2bb [n^4], the spin-free g1 [n^2] and g2 [n^4], then the second
-//   solver's energy and the transition g1a, g1b [n^2] of <root 0, irrep| ... |root 0, irrep2>.
+//   solver's energy and the transition g1a, g1b [n^2] of <root 0, irrep| ... |root 0, irrep2>, the
+//   refusal flag of a level-2 transition RDM, and the GAS solve's energy and determinant count.
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
@@ -73,6 +75,17 @@ int main(int argc, char** argv) {
             level2_refused = true;
         }
 
+        // GenCISolver: at most two electrons in the upper half of the orbitals
+        fcib_cpp::Solver g(device);
+        g.set_integrals(n, nirrep, orbsym, scalar, oei.data(), oei.data(), taa.data(), tab.data(), taa.data());
+        g.set_state(na, nb, /*irrep=*/0, mult, 1);
+        std::vector<int> space(n);
+        for (int p = 0; p < n; p++) space[p] = p < n / 2 ? 0 : 1;
+        g.set_gas(space, {na + nb - 2, 0}, {2 * (n / 2), 2});
+        g.options().e_convergence = 1e-12;
+        g.options().r_convergence = 1e-8;
+        g.compute_energy();
+
         std::ofstream out(argv[2], std::ios::binary);
         wr(out, s.energies());
         wr(out, s.spin2());
@@ -83,6 +96,7 @@ int main(int argc, char** argv) {
         wr(out, tr[0].g1a);
         wr(out, tr[0].g1b);
         wr(out, std::vector<double>{level2_refused ? 1.0 : 0.0});
+        wr(out, std::vector<double>{g.energies()[0], (double)g.size()});
         std::printf("fcib_solver_main: E = %.12f (%d iterations), second state E = %.12f\n", s.energies()[0],
                     s.iterations(), t.energies()[0]);
         return 0;

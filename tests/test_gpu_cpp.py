@@ -78,6 +78,7 @@ def test_cpp_driver_golden_c2v(tmp_path):
     g1a, g1b, g2aa, g2ab, g2bb = take(n2), take(n2), take(n4), take(n4), take(n4)
     sf1, sf2 = take(n2), take(n4)
     e2, t1a, t1b, refused = take(1), take(n2), take(n2), take(1)
+    e_gas, n_gas = take(2)
     assert pos == out.size
     assert abs(energies[0] - ref) < 1e-9
     assert refused[0] == 1.0
@@ -114,6 +115,12 @@ def test_cpp_driver_golden_c2v(tmp_path):
     assert np.max(np.abs(np.concatenate([tp.g1a.ravel(), tp.g1b.ravel()]) - ref_t)) < 1e-9
     sfp = s.transition_rdms([(0, 0)], t, 1, "spin_free")[0]
     assert np.max(np.abs(sfp.g1.ravel() - (rt["g1a"] + rt["g1b"]).ravel())) < 1e-9
+    # the GAS solve of the driver (at most two electrons in the upper half) through the Python mirror
+    from forte_b200 import GenCISolver
+    g = GenCISolver(StateInfo(na, nb, mult, na - nb, irrep, (na + nb - 2, 0), (2 * (n // 2), 2)), 1, ints,
+                    [list(range(n // 2)), list(range(n // 2, n))], {"E_CONVERGENCE": 1e-12, "R_CONVERGENCE": 1e-8})
+    assert g.size() == int(n_gas) and 0 < g.size() < s.size()
+    assert abs(g.compute_energy() - e_gas) < 1e-10 and e_gas > energies[0]
     with pytest.raises(Exception):
         s.transition_rdms([(0, 0)], t, 2)
     with pytest.raises(Exception):
