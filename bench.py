@@ -13,6 +13,7 @@ One FP64 solve of the same problem gives the reference energy (|dE| check) and t
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
   python bench.py --mode sigma --n 15 [--precision MIXED|MIXED_TF32|FP64]   (sigma builds/s)
+  python bench.py --mode gas                       (GAS spaces: kept-string blocks vs the masked C1 layout)
 
 N > 1 runs independent replicas (the solve does not shard across GPUs), one per rank.
 """
@@ -362,6 +363,74 @@ def run_sym(args, world, rank, local):
         }), flush=True)
 
 
+def run_gas(args, world, rank, local):
+    """GAS spaces (GenCISolver): C1 CAS(n,n), GAS1 = the lower half of the orbitals, GAS2 = the upper
+    half holding at most m electrons (m = 2, 4).  Sigma time and time to solution of the kept-string
+    blocked layout (blocks of the strings some GAS determinant uses) against the masked C1 layout."""
+    import ctypes as C
+    import torch
+    from forte_b200 import GenCISolver, StateInfo, build, capi, synthetic
+    build.build()
+    torch.cuda.set_device(local)
+    n, k = args.n, args.n // 2
+    ints = synthetic(n, 3 * n, SEED, gap=GAP)
+    spaces = [list(range(k)), list(range(k, n))]
+    L = capi.lib()
+    res = {}
+    for m in (2, 4):
+        st = StateInfo(k, k, 1, 0, 0, (2 * k - m, 0), (2 * k, m))
+        for blocked in (True, False):
+            lay = "blocked" if blocked else "masked"
+            s = GenCISolver(st, 1, ints, spaces, {"FCI_SYM_BLOCKED": blocked, "E_CONVERGENCE": 1e-9,
+                                                   "R_CONVERGENCE": 1e-5, "DL_SUBSPACE_PER_ROOT": 8}, device=local)
+            ndet = s.size()
+            nv = s.layout_size()
+            r = {"gas_determinants": ndet, "layout_elements": nv, "sigma_ms": {}, "solve": {}}
+            g = torch.Generator(device="cuda").manual_seed(0)
+            x = torch.randn(nv, dtype=torch.float64, device="cuda", generator=g)
+            x /= x.norm()
+            y = torch.empty_like(x)
+            stream = torch.cuda.ExternalStream(s.stream())
+            for prec_name, prec in (("FP64", capi.PREC_FP64), ("MIXED", capi.PREC_MIXED)):
+                def one():
+                    capi.check(L.fcib_sigma_device(s._h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), prec,
+                                                   None))
+                for _ in range(args.warmup):
+                    one()
+                torch.cuda.synchronize()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                for _ in range(args.steps):
+                    one()
+                e1.record(stream)
+                e1.synchronize()
+                r["sigma_ms"][prec_name] = e0.elapsed_time(e1) / args.steps
+            del x, y
+            torch.cuda.empty_cache()
+            for prec_name in ("MIXED", "FP64"):
+                s.set_options({"FCI_PRECISION": prec_name})
+                s.reset_guess()
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                e = s.compute_energy()
+                r["solve"][prec_name] = {"seconds": time.perf_counter() - t0, "energy": e,
+                                         "iterations": s.iterations()}
+            res[f"m{m}_{lay}"] = r
+            del s
+            torch.cuda.empty_cache()
+    if rank == 0:
+        print(json.dumps({
+            "metric": f"GAS CAS({n},{n}) time to solution (mixed), upper half <= 4 electrons, kept-string blocks",
+            "value": res["m4_blocked"]["solve"]["MIXED"]["seconds"], "unit": "s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": False, "dtype": "tf32x3/f64",
+            "data": "synthetic",
+            "config": {"workload": f"C1 CAS({n},{n}) synthetic L={3 * n}, GAS1 = orbitals 0..{k - 1}, GAS2 = "
+                                   f"{k}..{n - 1} with at most m electrons"},
+            "results": res,
+        }), flush=True)
+
+
 def run_configs(args, world, rank, local):
     """Time to solution of the two small workloads: CAS(8,8) (4,900 determinants, 1 root, FP64,
     synthetic L = 24; also solved by the CPU oracle on one core) and CAS(12,12) (853,776
@@ -621,7 +690,7 @@ def main():
     ap.add_argument("--phases", action="store_true",
                     help="batch mode: run the profiling build and report the share of clock cycles per phase")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--mode", default="solve", choices=["solve", "sigma", "precond", "batch", "configs", "sym"],
+    ap.add_argument("--mode", default="solve", choices=["solve", "sigma", "precond", "batch", "configs", "sym", "gas"],
                     help="solve: the Davidson time-to-solution metric; sigma: sigma builds/s at CAS(n,n); "
                          "precond: learned vs diagonal preconditioner at CAS(14,14), 2 roots; "
                          "batch: batched CASCI instances/s; configs: time to solution at CAS(8,8) and "
@@ -644,6 +713,9 @@ def main():
         return
     if args.mode == "configs":
         run_configs(args, world, rank, local)
+        return
+    if args.mode == "gas":
+        run_gas(args, world, rank, local)
         return
     if args.mode == "sym":
         run_sym(args, world, rank, local)

@@ -83,6 +83,7 @@ SIGNATURES = {
     "fcib_set_state": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
     "fcib_set_options": (C.c_int, [_vp, C.POINTER(FcibOptions)]),
     "fcib_size": (C.c_int, [_vp, C.POINTER(C.c_int64)]),
+    "fcib_layout_size": (C.c_int, [_vp, C.POINTER(C.c_int64)]),
     "fcib_set_gas": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "fcib_determinants": (C.c_int, [_vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     "fcib_ncsf": (C.c_int, [_vp, C.POINTER(C.c_int64)]),

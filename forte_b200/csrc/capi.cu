@@ -355,6 +355,14 @@ int fcib_size(fcib_ctx* ctx, int64_t* ndet) {
     });
 }
 
+int fcib_layout_size(fcib_ctx* ctx, int64_t* n) {
+    if (!ctx || !n) { set_error("null argument"); return FCIB_ERR_ARG; }
+    return guarded(ctx, [&] {
+        ensure_setup(ctx->c);
+        *n = ctx->c.nvec;
+    });
+}
+
 // SpinAdapter::ncsf (ci_spin_adaptation.h:81-183): CSFs of the state's multiplicity in the target irrep
 int fcib_ncsf(fcib_ctx* ctx, int64_t* ncsf) {
     if (!ctx || !ncsf) { set_error("null argument"); return FCIB_ERR_ARG; }
@@ -491,9 +499,13 @@ static void max_abs_elements(Context& c, int root, int num_dets, std::vector<dou
     // vector index -> (flat position, alpha irrep, addresses within the irrep blocks); the flat
     // position (FCIVector order, or GenCIVector order with GAS) orders equal |C|
     auto locate = [&](int64_t idx, int64_t& flat, int& h, int64_t& ai, int64_t& bi) {
-        if (c.sym.on) {  // the blocked layout is the FCIVector flat order
+        if (c.sym.on) {  // the blocked layout is the FCIVector flat order (without GAS spaces)
             flat = idx;
-            sym_host_locate(c, idx, h, ai, bi);
+            int64_t i, j;  // string indices (the blocks of a GAS layout hold a subset of the strings)
+            sym_host_decode(c, idx, i, j);
+            h = ha[i];
+            ai = ra[i];
+            bi = rb[j];
         } else {
             const int64_t i = idx / c.nbs, j = idx % c.nbs;
             flat = pa[i] + rb[j];

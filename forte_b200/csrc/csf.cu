@@ -82,7 +82,7 @@ __device__ __forceinline__ int64_t csf_det_id(uint32_t D, uint32_t Om, uint32_t 
         else b |= bit;
     }
     const uint32_t ra = d_rank(a, n), rb = d_rank(b, n);
-    return sd.nirrep > 1 ? sym_encode(sd, a, (int)ra, (int)rb) : (int64_t)ra * nbs + rb;
+    return sd.on ? sym_encode(sd, a, (int)ra, (int)rb) : (int64_t)ra * nbs + rb;
 }
 
 // One CTA per configuration (grid-stride) of a group with N open shells, nd spin patterns and f

@@ -357,12 +357,12 @@ __global__ void k_collect_le(const double* __restrict__ hd, const uint8_t* __res
 // per determinant: doubly occupied orbitals (r = s) and alpha/beta open-shell swaps.
 // ------------------------------------------------------------------------------------------
 
-// C in the engine layout: C1 (sd.nirrep = 1, nas * nbs elements) or the blocked layout of sd (N elements)
+// C in the engine layout: C1 (sd.on = 0, nas * nbs elements) or the blocked layout of sd (N elements)
 __global__ void __launch_bounds__(kRedThreads) k_spin2(const double* __restrict__ C, const uint32_t* __restrict__ sa,
                                                        const uint32_t* __restrict__ sb, int nas, int nbs, int n,
                                                        double* __restrict__ partial, SymDev sd, size_t N) {
     double acc = 0.0;
-    const bool blocked = sd.nirrep > 1;
+    const bool blocked = sd.on;
     if (!blocked) N = (size_t)nas * nbs;
     for (size_t I = blockIdx.x * (size_t)blockDim.x + threadIdx.x; I < N; I += (size_t)gridDim.x * blockDim.x) {
         double ci = C[I];
@@ -388,7 +388,10 @@ __global__ void __launch_bounds__(kRedThreads) k_spin2(const double* __restrict_
                 uint32_t m = (hi - lo < 2) ? 0u : (((1u << hi) - 1u) & ~((2u << lo) - 1u));
                 int par = (__popc(Ia & m) + __popc(Ib & m)) & 1;
                 const int ja = (int)d_rank(Ja, n), jb = (int)d_rank(Jb, n);
-                double cj = C[blocked ? (size_t)sym_encode(sd, Ja, ja, jb) : (size_t)ja * nbs + jb];
+                // blocked: a swap may leave the kept strings of a GAS layout (no such determinant there)
+                const int64_t J = blocked ? sym_encode_kept(sd, Ja, ja, jb) : (int64_t)ja * nbs + jb;
+                if (J < 0) continue;
+                const double cj = C[J];
                 t += par ? -cj : cj;
             }
         }

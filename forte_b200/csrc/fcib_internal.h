@@ -120,8 +120,10 @@ void build_spin_tables(SpinTables& t, int n, int k, bool need_g1, cudaStream_t s
 // terms work on the transposed blocks: beta irrep h x the alpha strings of irrep h ^ irrep.
 constexpr uint32_t kNullRow = 0x7FFFFFFFu;  // padding member of a same-spin group (no string)
 
-// device view of the blocked layout, passed to kernels by value
+// device view of the blocked layout, passed to kernels by value.  With GAS spaces the blocks hold
+// only the strings that some GAS determinant uses (the kept strings); loc of any other string is -1.
 struct SymDev {
+    int on = 0;                         // 1: the blocked layout (0: the C1 layout)
     int nirrep = 1, irrep = 0;
     uint32_t irrbit[3] = {0u, 0u, 0u};  // orbitals whose irrep label has bit b set
     int64_t blk[9] = {};                // alpha-major block offsets
@@ -157,6 +159,13 @@ __device__ __forceinline__ int64_t sym_encode(const SymDev& d, uint32_t sa, int 
     const int h = sym_irrep_of(d, sa);
     return d.blk[h] + (int64_t)d.aloc[ia] * d.bcol[h] + d.bloc[ib];
 }
+// the same, or -1 when either string is not in the blocks (GAS spaces)
+__device__ __forceinline__ int64_t sym_encode_kept(const SymDev& d, uint32_t sa, int ia, int ib) {
+    const int la = d.aloc[ia], lb = d.bloc[ib];
+    if (la < 0 || lb < 0) return -1;
+    const int h = sym_irrep_of(d, sa);
+    return d.blk[h] + (int64_t)la * d.bcol[h] + lb;
+}
 
 // one opposite-spin sub-problem of the blocked sigma: target alpha irrep ha, pair irrep g.  Rows are
 // the alpha strings of irrep ha; their connections through pairs of irrep g reach alpha strings of
@@ -180,7 +189,8 @@ struct SymSpace {
     int64_t blkT[9] = {};
     int acnt[8] = {}, bcnt[8] = {};
     std::vector<int> airr, birr;                      // irrep of each string
-    std::vector<int32_t> asrc_h, bsrc_h, aloc_h, bloc_h;
+    std::vector<int32_t> asrc_h, bsrc_h, aloc_h, bloc_h;  // loc -1: string not in the blocks (GAS)
+    std::vector<uint8_t> bkeep;                       // beta strings in the blocks
     DBuf<int32_t> asrc, bsrc, aloc, bloc;
     DBuf<uint32_t> bstr_sorted;                       // beta strings in irrep-sorted order
     // opposite spin
@@ -368,6 +378,9 @@ void apply_mask(Context& c, double* v);
 // gas.cu: mask and flat map of the layout (masked C1 with symmetry, GAS); GenCIVector position
 void build_layout_maps(Context& c);
 int64_t gas_flat_position(const Context& c, int64_t I);
+// strings used by some GAS determinant (1) or by none (0), per C1 string index of each spin
+void gas_keep_strings(const Context& c, const std::vector<uint32_t>& sa, const std::vector<uint32_t>& sb,
+                      std::vector<uint8_t>& keep_a, std::vector<uint8_t>& keep_b);
 void export_list(int n, int k, int kind, int p, int q, int r, int s, std::vector<int8_t>& sign,
                  std::vector<uint32_t>& I, std::vector<uint32_t>& J, cudaStream_t st);
 void compute_hdiag(Context& c, double* out);

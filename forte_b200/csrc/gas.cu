@@ -9,8 +9,11 @@
 //     (alpha + beta) in each orbital space k lies in [emin[k], emax[k]], host vectors in
 //     GenCIVector flat order.
 // Sigma of a masked layout is P H P, P the projector on the kept determinants: on the kept
-// space that is H itself, so energies, vectors and RDMs are those of the restricted space.  The
-// cost of a sigma is that of the unrestricted layout.
+// space that is H itself, so energies, vectors and RDMs are those of the restricted space.
+// With GAS spaces the blocked layout (symblock.cu, also without point-group symmetry) holds only
+// the strings whose occupation pattern some GAS determinant has: its blocks are the products of
+// those strings, a superset of the GAS space, and a sigma costs what those blocks cost.  The
+// masked C1 layout (sym_blocked = 0) keeps every string and costs the full sigma.
 //
 // The GenCIVector flat order restated here, from the reference:
 //   1. occupation patterns (get_ci_occupation_patterns and recursive_ormas_generation,
@@ -49,7 +52,7 @@ __global__ void k_layout_mask(uint8_t* __restrict__ mask, int64_t nvec, SymDev d
                               const uint32_t* __restrict__ sa, const uint32_t* __restrict__ sb, GasDev g) {
     for (int64_t I = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; I < nvec; I += (int64_t)gridDim.x * blockDim.x) {
         int ia, ib;
-        if (d.nirrep > 1) {
+        if (d.on) {
             sym_decode(d, I, ia, ib);
         } else {
             ia = (int)(I / nbs);
@@ -117,6 +120,24 @@ static void gas_patterns(const Context& c, std::vector<Occ>& alfa, std::vector<O
             }
     };
     walk(walk, 0, c.na, c.nb);
+}
+
+void gas_keep_strings(const Context& c, const std::vector<uint32_t>& sa, const std::vector<uint32_t>& sb,
+                      std::vector<uint8_t>& keep_a, std::vector<uint8_t>& keep_b) {
+    std::vector<Occ> pa, pb;
+    std::vector<std::pair<int, int>> pairs;
+    gas_patterns(c, pa, pb, pairs);
+    // a string is used by some GAS determinant when its occupation pattern is in its spin's list
+    auto mark = [&](const std::vector<uint32_t>& s, const std::vector<Occ>& pats, std::vector<uint8_t>& keep) {
+        keep.assign(s.size(), 0);
+        for (size_t i = 0; i < s.size(); i++) {
+            Occ o{};
+            for (int k = 0; k < c.gas.ngas; k++) o[k] = __builtin_popcount(s[i] & c.gas.orbs[k]);
+            keep[i] = std::find(pats.begin(), pats.end(), o) != pats.end() ? 1 : 0;
+        }
+    };
+    mark(sa, pa, keep_a);
+    mark(sb, pb, keep_b);
 }
 
 // step 2 above: the strings of every class, as C1 string indices, for one spin

@@ -100,9 +100,9 @@ struct EngineSource {  // determinant I of an engine-layout vector: diagonal cor
     double lambda;
     float inv_rnorm;
     float skip;  // tiles whose |t_I| are all below this keep the diagonal rule
-    SymDev sd;   // the blocked layout (sd.nirrep > 1) or C1
+    SymDev sd;   // the blocked layout (sd.on) or C1
     __device__ bool load(size_t I, uint32_t& a, uint32_t& b, float& u, float& rr, double& tv) const {
-        if (sd.nirrep > 1) {
+        if (sd.on) {
             int ia, ib;
             sym_decode(sd, (int64_t)I, ia, ib);
             a = (uint32_t)ia;

@@ -899,12 +899,12 @@ struct DiagInts {
 };
 __constant__ DiagInts d_diag;
 
-// out in the engine layout: C1 (sd.nirrep = 1) or the blocked layout of sd
+// out in the engine layout: C1 (sd.on = 0) or the blocked layout of sd
 __global__ void k_hdiag(const uint32_t* __restrict__ sa, const uint32_t* __restrict__ sb, int nas,
                         int nbs, int n, double e0, double* __restrict__ out, size_t N, SymDev sd) {
     for (size_t I = blockIdx.x * (size_t)blockDim.x + threadIdx.x; I < N; I += (size_t)gridDim.x * blockDim.x) {
         int ia, ib;
-        if (sd.nirrep > 1) {
+        if (sd.on) {
             sym_decode(sd, (int64_t)I, ia, ib);
         } else {
             ia = (int)(I / nbs);

@@ -50,7 +50,9 @@ static void build_group_subs(Context& c, const SpinTables& t, bool alpha, bool o
         for (auto& b : bucket) b.clear();
         for (int m = 0; m < G; m++) {
             const uint32_t e = rows[(size_t)gi * G + m];
+            if (e == kNullRow) continue;
             const uint32_t I = e & kConnIdxMask;
+            if (loc[I] < 0) continue;  // a string no GAS determinant uses: its rows and columns are absent
             bucket[irr[I]].push_back({(uint32_t)loc[I] | (e & kSignBit), labs[(size_t)gi * G + m]});
         }
         for (int h = 0; h < nh; h++)
@@ -163,6 +165,7 @@ static void build_ab_subs(Context& c, const std::vector<uint32_t>& sb) {
                     if (P >= npair || pirr[P] != g) continue;
                     const uint32_t J = e & kConnIdxMask;
                     FCIB_CHECK(y.airr[J] == src, FCIB_ERR_NUMERIC, "blocked sigma: connection irrep mismatch");
+                    if (y.aloc_h[J] < 0) continue;  // a source string no GAS determinant uses
                     lists[i].push_back((uint32_t)y.aloc_h[J] | ((uint32_t)P << 21) | (e & kSignBit));
                 }
                 u.kmax = std::max(u.kmax, (int)lists[i].size());
@@ -186,7 +189,7 @@ static void build_ab_subs(Context& c, const std::vector<uint32_t>& sb) {
                         if (e != kNoTarget) {
                             const uint32_t I = (uint32_t)e & kConnIdxMask;
                             FCIB_CHECK(y.birr[I] == hb, FCIB_ERR_NUMERIC, "blocked sigma: target irrep mismatch");
-                            v = (int32_t)((uint32_t)y.bloc_h[I] | ((uint32_t)e & kSignBit));
+                            if (y.bloc_h[I] >= 0) v = (int32_t)((uint32_t)y.bloc_h[I] | ((uint32_t)e & kSignBit));
                         }
                     }
                     tgt32_all.push_back(v);
@@ -205,7 +208,7 @@ static void build_ab_subs(Context& c, const std::vector<uint32_t>& sb) {
                             if (R >= 0 && j < u.ns) {
                                 const int Jb = y.bsrc_h[y.d.boff[hjb] + j];
                                 const int32_t e = tgt[(size_t)Jb * npp + R];
-                                if (e != kNoTarget)
+                                if (e != kNoTarget && y.bloc_h[(uint32_t)e & kConnIdxMask] >= 0)
                                     v = (uint16_t)(((uint32_t)y.bloc_h[(uint32_t)e & kConnIdxMask] << 2) |
                                                    ((uint32_t)e >> 31));
                             }
@@ -213,13 +216,17 @@ static void build_ab_subs(Context& c, const std::vector<uint32_t>& sb) {
                         }
             }
             // contributions per target element of the tensor-core scatter: one per off-diagonal pair of
-            // irrep g with exactly one orbital occupied, plus the diagonal sum when g = 0
+            // irrep g with exactly one orbital occupied whose source string (the other orbital occupied)
+            // is in the blocks, plus the diagonal sum when g = 0
             u.mag = mag_all.size();
             for (int j = 0; j < u.nt; j++) {
                 const uint32_t s = sb[y.bsrc_h[y.d.boff[hb] + j]];
                 int cnt = g == 0 ? 1 : 0;
-                for (int P : plist[g])
-                    if (pp[P] != pq[P]) cnt += (int)(((s >> pp[P]) ^ (s >> pq[P])) & 1u);
+                for (int P : plist[g]) {
+                    if (pp[P] == pq[P] || !(((s >> pp[P]) ^ (s >> pq[P])) & 1u)) continue;
+                    const uint32_t J = s ^ (1u << pp[P]) ^ (1u << pq[P]);
+                    cnt += y.bkeep[host_rank(J, n)] ? 1 : 0;
+                }
                 mag_all.push_back((uint8_t)cnt);
             }
             y.ab.push_back(u);
@@ -252,38 +259,45 @@ void build_sym_space(Context& c) {
     y.b2.clear();
     y.b1.clear();
     c.nvec = c.ndet;
-    if (c.nirrep <= 1 || !c.opt.sym_blocked) return;
+    // blocks with point-group symmetry, and with GAS spaces (blocks of the kept strings) even in C1
+    if (!c.opt.sym_blocked || (c.nirrep <= 1 && c.gas.ngas == 0)) return;
     const int nh = c.nirrep, S = c.irrep, n = c.n;
     std::vector<uint32_t> sa(c.nas), sb(c.nbs);
     FCIB_CUDA(cudaMemcpy(sa.data(), c.A.str.p, 4 * c.nas, cudaMemcpyDeviceToHost));
     FCIB_CUDA(cudaMemcpy(sb.data(), c.B.str.p, 4 * c.nbs, cudaMemcpyDeviceToHost));
+    std::vector<uint8_t> keep_a(c.nas, 1), keep_b(c.nbs, 1);
+    if (c.gas.ngas > 0) gas_keep_strings(c, sa, sb, keep_a, keep_b);
     SymDev& d = y.d;
     d = SymDev{};
+    d.on = 1;
     d.nirrep = nh;
     d.irrep = S;
     for (int b = 0; b < 3; b++)
         for (int p = 0; p < n; p++)
             if (c.orbsym[p] >> b & 1) d.irrbit[b] |= 1u << p;
-    auto sort_strings = [&](const std::vector<uint32_t>& s, std::vector<int>& irr, int* cnt, int32_t* off,
-                            std::vector<int32_t>& src, std::vector<int32_t>& loc) {
+    // kept strings sorted by irrep (string order within an irrep); loc = -1 for the others
+    auto sort_strings = [&](const std::vector<uint32_t>& s, const std::vector<uint8_t>& keep, std::vector<int>& irr,
+                            int* cnt, int32_t* off, std::vector<int32_t>& src, std::vector<int32_t>& loc) {
         const size_t ns = s.size();
         irr.resize(ns);
-        src.assign(ns, 0);
-        loc.assign(ns, 0);
+        loc.assign(ns, -1);
         for (int h = 0; h < 8; h++) cnt[h] = 0;
         for (size_t i = 0; i < ns; i++) {
             irr[i] = sym_irrep_of(d, s[i]);
-            loc[i] = cnt[irr[i]]++;
+            if (keep[i]) loc[i] = cnt[irr[i]]++;
         }
         int32_t o = 0;
         for (int h = 0; h < 8; h++) {
             off[h] = o;
             o += cnt[h];
         }
-        for (size_t i = 0; i < ns; i++) src[off[irr[i]] + loc[i]] = (int32_t)i;
+        src.assign((size_t)o, 0);
+        for (size_t i = 0; i < ns; i++)
+            if (loc[i] >= 0) src[off[irr[i]] + loc[i]] = (int32_t)i;
     };
-    sort_strings(sa, y.airr, y.acnt, d.aoff, y.asrc_h, y.aloc_h);
-    sort_strings(sb, y.birr, y.bcnt, d.boff, y.bsrc_h, y.bloc_h);
+    sort_strings(sa, keep_a, y.airr, y.acnt, d.aoff, y.asrc_h, y.aloc_h);
+    sort_strings(sb, keep_b, y.birr, y.bcnt, d.boff, y.bsrc_h, y.bloc_h);
+    y.bkeep = keep_b;
     d.blk[0] = 0;
     y.blkT[0] = 0;
     for (int h = 0; h < 8; h++) {
@@ -300,8 +314,8 @@ void build_sym_space(Context& c) {
     d.bsrc = y.bsrc.p;
     d.aloc = y.aloc.p;
     d.bloc = y.bloc.p;
-    std::vector<uint32_t> bsorted(c.nbs);
-    for (int64_t i = 0; i < c.nbs; i++) bsorted[i] = sb[y.bsrc_h[i]];
+    std::vector<uint32_t> bsorted(y.bsrc_h.size());
+    for (size_t i = 0; i < bsorted.size(); i++) bsorted[i] = sb[y.bsrc_h[i]];
     y.bstr_sorted.upload(bsorted, c.stream);
     c.nvec = d.blk[nh];
     y.on = true;

@@ -180,6 +180,12 @@ class FCISolver:
         capi.check(capi.lib().fcib_size(self._h, C.byref(n)))
         return n.value
 
+    def layout_size(self) -> int:
+        """Length of device vectors in the engine's layout (the *_device entry points)."""
+        n = C.c_int64()
+        capi.check(capi.lib().fcib_layout_size(self._h, C.byref(n)))
+        return n.value
+
     def csf_to_det(self, z: np.ndarray) -> np.ndarray:
         """SpinAdapter::csf_C_to_det_C: CSF coefficients -> determinant vector (flat order)."""
         z = np.ascontiguousarray(z, dtype=np.float64)

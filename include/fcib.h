@@ -114,6 +114,10 @@ int fcib_set_gas(fcib_ctx* ctx, int ngas, const int* space, const int* gas_min, 
 
 /* determinant-space size in flat order: FCIVector (sum over irrep blocks) or GenCIVector */
 int fcib_size(fcib_ctx* ctx, int64_t* ndet);
+/* length of device vectors in the engine's layout (the *_device entry points): fcib_size without
+ * symmetry or GAS spaces and in the blocked layout; with GAS spaces the blocks of the strings some
+ * GAS determinant uses (blocked) or the C1 space (sym_blocked = 0) */
+int fcib_layout_size(fcib_ctx* ctx, int64_t* n);
 /* alpha and beta strings (bit p = orbital p) of every flat position, fcib_size entries each
  * (FCIStringLists / GenCIStringLists::make_determinants, genci_string_lists.cc:276-291) */
 int fcib_determinants(fcib_ctx* ctx, uint32_t* alfa, uint32_t* beta);
