@@ -382,7 +382,8 @@ def run_gas(args, world, rank, local):
         for blocked in (True, False):
             lay = "blocked" if blocked else "masked"
             s = GenCISolver(st, 1, ints, spaces, {"FCI_SYM_BLOCKED": blocked, "E_CONVERGENCE": 1e-9,
-                                                   "R_CONVERGENCE": 1e-5, "DL_SUBSPACE_PER_ROOT": 8}, device=local)
+                                                   "R_CONVERGENCE": 1e-5, "DL_SUBSPACE_PER_ROOT": 8,
+                                                   "DL_MAXITER": 400}, device=local)
             ndet = s.size()
             nv = s.layout_size()
             r = {"gas_determinants": ndet, "layout_elements": nv, "sigma_ms": {}, "solve": {}}

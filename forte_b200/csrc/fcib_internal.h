@@ -171,17 +171,28 @@ __device__ __forceinline__ int64_t sym_encode_kept(const SymDev& d, uint32_t sa,
 // the alpha strings of irrep ha; their connections through pairs of irrep g reach alpha strings of
 // irrep ha ^ g, whose rows hold the beta strings of irrep ha ^ irrep ^ g (the source columns); the
 // beta replacements of irrep g take those to the target columns (beta irrep ha ^ irrep).
+// With GAS spaces a sub-problem covers one alpha pattern range of the target rows (row0, rows)
+// and one beta pattern range of the source columns (col0, ns; the source row length is lds); its
+// targets are the whole row of the target block (nt).  Without GAS both ranges are whole blocks.
 struct AbSub {
     int ha = 0, g = 0, src = 0;  // target alpha irrep, pair irrep, source alpha irrep ha ^ g
     int rows = 0, ns = 0, nt = 0;
+    int row0 = 0, col0 = 0, lds = 0;
+    int diag_off = 0;            // target column of the first source string (g = 0 only)
+    int accumulate = 0;          // 0: the first sub-problem of its rows (writes E0 C + its part)
     int kmax = 0;                // connections per row (short rows padded with the zero pair)
     size_t conn = 0, tgt32 = 0, tgt16 = 0, mag = 0;  // offsets into the SymSpace tables
 };
-// same-spin groups whose strings lie in one irrep (padded to G members with kNullRow)
+// same-spin groups whose strings lie in one irrep (padded to G members with kNullRow), over a range
+// of ncols columns of rows of length ld
 struct GroupSub {
-    int ngroups = 0, G = 0, ncols = 0;
-    int64_t blk = 0;   // block offset: alpha-major for alpha groups, transposed for beta groups
+    int ngroups = 0, G = 0, ncols = 0, ld = 0;
+    int64_t blk = 0;   // block offset (+ first column): alpha-major for alpha groups, transposed for beta groups
     size_t off = 0;    // into SymSpace::grow / glab
+};
+// a run of strings of one occupation pattern inside an irrep's kept strings
+struct PatRange {
+    int pat = 0, start = 0, count = 0;
 };
 struct SymSpace {
     bool on = false;
@@ -190,7 +201,14 @@ struct SymSpace {
     int acnt[8] = {}, bcnt[8] = {};
     std::vector<int> airr, birr;                      // irrep of each string
     std::vector<int32_t> asrc_h, bsrc_h, aloc_h, bloc_h;  // loc -1: string not in the blocks (GAS)
-    std::vector<uint8_t> bkeep;                       // beta strings in the blocks
+    // GAS occupation patterns (one pattern 0 covering everything without GAS): per string its
+    // pattern (-1: not kept), per irrep the pattern runs of the kept strings, the pattern pairs
+    // that GAS determinants have, and which patterns one electron replacement connects
+    std::vector<int> apat, bpat;
+    std::vector<PatRange> arun[8], brun[8];
+    int npa = 1, npb = 1;
+    std::vector<uint8_t> allowed;                     // [npa * npb]
+    std::vector<uint8_t> areach, breach;              // [npa * npa], [npb * npb]
     DBuf<int32_t> asrc, bsrc, aloc, bloc;
     DBuf<uint32_t> bstr_sorted;                       // beta strings in irrep-sorted order
     // opposite spin
@@ -378,9 +396,12 @@ void apply_mask(Context& c, double* v);
 // gas.cu: mask and flat map of the layout (masked C1 with symmetry, GAS); GenCIVector position
 void build_layout_maps(Context& c);
 int64_t gas_flat_position(const Context& c, int64_t I);
-// strings used by some GAS determinant (1) or by none (0), per C1 string index of each spin
-void gas_keep_strings(const Context& c, const std::vector<uint32_t>& sa, const std::vector<uint32_t>& sb,
-                      std::vector<uint8_t>& keep_a, std::vector<uint8_t>& keep_b);
+// GAS occupation pattern of every string of each spin (index into its spin's pattern list, -1 when
+// no GAS determinant uses the string), the allowed pattern pairs [npa * npb] and, per spin, which
+// patterns differ by one electron moved between spaces or not at all ([np * np])
+void gas_string_patterns(const Context& c, const std::vector<uint32_t>& sa, const std::vector<uint32_t>& sb,
+                         std::vector<int>& pat_a, std::vector<int>& pat_b, int& npa, int& npb,
+                         std::vector<uint8_t>& allowed, std::vector<uint8_t>& reach_a, std::vector<uint8_t>& reach_b);
 void export_list(int n, int k, int kind, int p, int q, int r, int s, std::vector<int8_t>& sign,
                  std::vector<uint32_t>& I, std::vector<uint32_t>& J, cudaStream_t st);
 void compute_hdiag(Context& c, double* out);

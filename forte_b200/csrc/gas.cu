@@ -122,22 +122,46 @@ static void gas_patterns(const Context& c, std::vector<Occ>& alfa, std::vector<O
     walk(walk, 0, c.na, c.nb);
 }
 
-void gas_keep_strings(const Context& c, const std::vector<uint32_t>& sa, const std::vector<uint32_t>& sb,
-                      std::vector<uint8_t>& keep_a, std::vector<uint8_t>& keep_b) {
+void gas_string_patterns(const Context& c, const std::vector<uint32_t>& sa, const std::vector<uint32_t>& sb,
+                         std::vector<int>& pat_a, std::vector<int>& pat_b, int& npa, int& npb,
+                         std::vector<uint8_t>& allowed, std::vector<uint8_t>& reach_a, std::vector<uint8_t>& reach_b) {
     std::vector<Occ> pa, pb;
     std::vector<std::pair<int, int>> pairs;
     gas_patterns(c, pa, pb, pairs);
+    npa = (int)pa.size();
+    npb = (int)pb.size();
     // a string is used by some GAS determinant when its occupation pattern is in its spin's list
-    auto mark = [&](const std::vector<uint32_t>& s, const std::vector<Occ>& pats, std::vector<uint8_t>& keep) {
-        keep.assign(s.size(), 0);
+    auto mark = [&](const std::vector<uint32_t>& s, const std::vector<Occ>& pats, std::vector<int>& pat) {
+        pat.assign(s.size(), -1);
         for (size_t i = 0; i < s.size(); i++) {
             Occ o{};
             for (int k = 0; k < c.gas.ngas; k++) o[k] = __builtin_popcount(s[i] & c.gas.orbs[k]);
-            keep[i] = std::find(pats.begin(), pats.end(), o) != pats.end() ? 1 : 0;
+            auto it = std::find(pats.begin(), pats.end(), o);
+            if (it != pats.end()) pat[i] = (int)(it - pats.begin());
         }
     };
-    mark(sa, pa, keep_a);
-    mark(sb, pb, keep_b);
+    mark(sa, pa, pat_a);
+    mark(sb, pb, pat_b);
+    allowed.assign((size_t)npa * npb, 0);
+    for (auto& pr : pairs) allowed[(size_t)pr.first * npb + pr.second] = 1;
+    // one replacement moves one electron: the patterns are equal or differ by +1 and -1 in two spaces
+    auto reach = [&](const std::vector<Occ>& pats, std::vector<uint8_t>& r) {
+        const size_t np = pats.size();
+        r.assign(np * np, 0);
+        for (size_t x = 0; x < np; x++)
+            for (size_t y = 0; y < np; y++) {
+                int up = 0, down = 0, other = 0;
+                for (int k = 0; k < c.gas.ngas; k++) {
+                    const int d = pats[y][k] - pats[x][k];
+                    if (d == 1) up++;
+                    else if (d == -1) down++;
+                    else if (d != 0) other++;
+                }
+                r[x * np + y] = (other == 0 && up == down && up <= 1) ? 1 : 0;
+            }
+    };
+    reach(pa, reach_a);
+    reach(pb, reach_b);
 }
 
 // step 2 above: the strings of every class, as C1 string indices, for one spin

@@ -290,7 +290,7 @@ __device__ __forceinline__ unsigned long long fixed64(float v, float scale) {
 
 template <typename T>
 __global__ void __launch_bounds__(1024) k_group(
-    const T* __restrict__ C, typename GroupOut<T>::type* __restrict__ S, int ncols,
+    const T* __restrict__ C, typename GroupOut<T>::type* __restrict__ S, int ncols, int ld,
     const uint32_t* __restrict__ rows, const uint16_t* __restrict__ labs, int G, int Gp,
     const double* __restrict__ M, int ldm, int ngroups, int nchunks, int* __restrict__ counter, int m_in_smem,
     const int* __restrict__ grid_el) {
@@ -333,7 +333,7 @@ __global__ void __launch_bounds__(1024) k_group(
             T v = (T)0;
             if (idx < G * kGrTN) {
                 const int j = idx / kGrTN, col = c0 + (idx - j * kGrTN);
-                if (col < ncols && rs[j] != kNullRow) v = C[(size_t)(rs[j] & kConnIdxMask) * ncols + col];
+                if (col < ncols && rs[j] != kNullRow) v = C[(size_t)(rs[j] & kConnIdxMask) * ld + col];
             }
             xv[r] = v;
         }
@@ -386,7 +386,7 @@ __global__ void __launch_bounds__(1024) k_group(
                 int ii = i0 + i;
                 if (ii < G && rs[ii] != kNullRow) {
                     uint32_t e = rs[ii];
-                    const size_t off = (size_t)(e & kConnIdxMask) * ncols + col;
+                    const size_t off = (size_t)(e & kConnIdxMask) * ld + col;
                     auto* dst = S + off;
                     const T a0 = (e & kSignBit) ? -acc[i][0] : acc[i][0];
                     const T a1 = (e & kSignBit) ? -acc[i][1] : acc[i][1];
@@ -419,9 +419,9 @@ constexpr int kGdMaxG = 48;
 constexpr int kGdLdW = 52;
 
 __global__ void __launch_bounds__(kGdThreads) k_group_dmma(
-    const double* __restrict__ C, unsigned long long* __restrict__ S, int ncols, const uint32_t* __restrict__ rows,
-    const uint16_t* __restrict__ labs, int G, const double* __restrict__ M, int ldm, int ngroups, int nchunks,
-    int* __restrict__ counter, const int* __restrict__ grid_el) {
+    const double* __restrict__ C, unsigned long long* __restrict__ S, int ncols, int ld,
+    const uint32_t* __restrict__ rows, const uint16_t* __restrict__ labs, int G, const double* __restrict__ M, int ldm,
+    int ngroups, int nchunks, int* __restrict__ counter, const int* __restrict__ grid_el) {
     const double scale = ldexp(1.0, *grid_el);  // the sigma's same-spin fixed-point grid
     extern __shared__ __align__(16) unsigned char gd_smem[];
     double* Ws = reinterpret_cast<double*>(gd_smem);      // W[i][j] at i*kGdLdW + j
@@ -457,7 +457,7 @@ __global__ void __launch_bounds__(kGdThreads) k_group_dmma(
             double v = 0.0;
             if (j < G && c0 + col < ncols && rs[j] != kNullRow) {
                 const uint32_t r = rs[j];
-                v = C[(size_t)(r & kConnIdxMask) * ncols + c0 + col];
+                v = C[(size_t)(r & kConnIdxMask) * ld + c0 + col];
                 if (r & kSignBit) v = -v;
             }
             Xs[j * kGdTN + (col ^ ((j & 1) << 3))] = v;
@@ -488,7 +488,7 @@ __global__ void __launch_bounds__(kGdThreads) k_group_dmma(
             const int i = m * 8 + fr;
             if (m < nmt && i < G && rs[i] != kNullRow) {
                 const uint32_t r = rs[i];
-                unsigned long long* srow = S + (size_t)(r & kConnIdxMask) * ncols;
+                unsigned long long* srow = S + (size_t)(r & kConnIdxMask) * ld;
 #pragma unroll
                 for (int t = 0; t < 2; t++) {
                     const int col = c0 + (2 * warp + t) * 8 + 2 * fk;
@@ -503,7 +503,7 @@ __global__ void __launch_bounds__(kGdThreads) k_group_dmma(
 }
 
 template <typename T>
-static void launch_group_t(Context& c, const T* C, typename GroupOut<T>::type* S, int ncols, int ngroups, int G,
+static void launch_group_t(Context& c, const T* C, typename GroupOut<T>::type* S, int ncols, int ld, int ngroups, int G,
                            const uint32_t* rows, const uint16_t* labs, const double* M, int ldm,
                            const int* grid_el) {
     if (ngroups == 0 || G == 0) return;
@@ -523,12 +523,13 @@ static void launch_group_t(Context& c, const T* C, typename GroupOut<T>::type* S
     int grid = std::min(ngroups * nchunks, per_sm * c.num_sms);
     ensure_counter(c);
     FCIB_CUDA(cudaMemsetAsync(c.counter.p + 2, 0, sizeof(int), c.stream));
-    k_group<T><<<grid, threads, smem, c.stream>>>(C, S, ncols, rows, labs, G, Gp, M, ldm, ngroups, nchunks, c.counter.p + 2,
+    k_group<T><<<grid, threads, smem, c.stream>>>(C, S, ncols, ld, rows, labs, G, Gp, M, ldm, ngroups, nchunks, c.counter.p + 2,
                                                   m_in_smem, grid_el);
     FCIB_KCHECK();
 }
 
-static void launch_group(Context& c, const double* C, unsigned long long* S, int ncols, int ngroups, int G,
+// ld: row stride of C and S (ncols, or the row length of the block when the columns are a sub-range)
+static void launch_group(Context& c, const double* C, unsigned long long* S, int ncols, int ld, int ngroups, int G,
                          const uint32_t* rows, const uint16_t* labs, const double* M, int ldm) {
     if (ngroups == 0 || G == 0) return;
     if (G <= kGdMaxG) {
@@ -539,16 +540,16 @@ static void launch_group(Context& c, const double* C, unsigned long long* S, int
         FCIB_CUDA(cudaFuncSetAttribute(k_group_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         ensure_counter(c);
         FCIB_CUDA(cudaMemsetAsync(c.counter.p + 2, 0, sizeof(int), c.stream));
-        k_group_dmma<<<grid, kGdThreads, smem, c.stream>>>(C, S, ncols, rows, labs, G, M, ldm, ngroups, nchunks,
+        k_group_dmma<<<grid, kGdThreads, smem, c.stream>>>(C, S, ncols, ld, rows, labs, G, M, ldm, ngroups, nchunks,
                                                            c.counter.p + 2, c.counter.p + kSlotSameGrid);
         FCIB_KCHECK();
         return;
     }
-    launch_group_t<double>(c, C, S, ncols, ngroups, G, rows, labs, M, ldm, c.counter.p + kSlotSameGrid);
+    launch_group_t<double>(c, C, S, ncols, ld, ngroups, G, rows, labs, M, ldm, c.counter.p + kSlotSameGrid);
 }
-static void launch_group(Context& c, const float* C, unsigned long long* S, int ncols, int ngroups, int G,
+static void launch_group(Context& c, const float* C, unsigned long long* S, int ncols, int ld, int ngroups, int G,
                          const uint32_t* rows, const uint16_t* labs, const double* M, int ldm) {
-    launch_group_t<float>(c, C, S, ncols, ngroups, G, rows, labs, M, ldm, c.counter.p + kSlotSameGrid);
+    launch_group_t<float>(c, C, S, ncols, ld, ngroups, G, rows, labs, M, ldm, c.counter.p + kSlotSameGrid);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -653,15 +654,15 @@ void apply_mask(Context& c, double* v) {
 // ------------------------------------------------------------------------------------------
 // sigma orchestration
 // ------------------------------------------------------------------------------------------
-bool launch_group_tc(Context& c, const float* C, unsigned long long* S, int ncols, int ngroups, int G,
+bool launch_group_tc(Context& c, const float* C, unsigned long long* S, int ncols, int ld, int ngroups, int G,
                      const uint32_t* rows, const uint16_t* labs, const double* M, int ldm);
 
 // mixed same-spin two-body groups: tensor cores unless disabled or the groups are too large
-static void launch_group_same_f32(Context& c, const float* C, unsigned long long* S, int ncols, int ngroups, int G,
-                                  const uint32_t* rows, const uint16_t* labs, const double* M, int ldm) {
-    if (c.opt.same_spin_kernel == FCIB_SAME_TC && launch_group_tc(c, C, S, ncols, ngroups, G, rows, labs, M, ldm))
+static void launch_group_same_f32(Context& c, const float* C, unsigned long long* S, int ncols, int ld, int ngroups,
+                                  int G, const uint32_t* rows, const uint16_t* labs, const double* M, int ldm) {
+    if (c.opt.same_spin_kernel == FCIB_SAME_TC && launch_group_tc(c, C, S, ncols, ld, ngroups, G, rows, labs, M, ldm))
         return;
-    launch_group(c, C, S, ncols, ngroups, G, rows, labs, M, ldm);
+    launch_group(c, C, S, ncols, ld, ngroups, G, rows, labs, M, ldm);
 }
 
 // same-spin (and, when not folded into the opposite-spin block, one-body) terms added to S
@@ -722,13 +723,13 @@ static void sigma_same_spin(Context& c, const double* C, double* S, bool fp32) {
         auto groups = [&](const double* X, unsigned long long* out, const std::vector<GroupSub>& subs, const SpinTables& t,
                           bool one_body, int ncols, const double* M, int ldm) {
             if (!y.on) {
-                if (one_body) launch_group(c, X, out, ncols, t.ng1, t.g1, t.g1row.p, t.g1lab.p, M, ldm);
-                else launch_group(c, X, out, ncols, t.ng2, t.g2, t.g2row.p, t.g2lab.p, M, ldm);
+                if (one_body) launch_group(c, X, out, ncols, ncols, t.ng1, t.g1, t.g1row.p, t.g1lab.p, M, ldm);
+                else launch_group(c, X, out, ncols, ncols, t.ng2, t.g2, t.g2row.p, t.g2lab.p, M, ldm);
                 return;
             }
             for (const GroupSub& g : subs)
-                launch_group(c, X + g.blk, out + g.blk, g.ncols, g.ngroups, g.G, y.grow.p + g.off, y.glab.p + g.off, M,
-                             ldm);
+                launch_group(c, X + g.blk, out + g.blk, g.ncols, g.ld, g.ngroups, g.G, y.grow.p + g.off, y.glab.p + g.off,
+                             M, ldm);
         };
         if (a_g1) groups(C, c.s64a.p, y.a1, c.A, true, nbs, c.Ha.p, c.n);
         if (c.A.ng2) groups(C, c.s64a.p, y.a2, c.A, false, nbs, c.M2a.p, np2);
@@ -755,17 +756,18 @@ static void sigma_same_spin(Context& c, const double* C, double* S, bool fp32) {
     FCIB_CUDA(cudaMemsetAsync(c.counter.p + 5, 0, sizeof(int), c.stream));  // tensor-core group timeout flag
     auto groups32 = [&](const float* X, unsigned long long* out, const std::vector<GroupSub>& subs, const SpinTables& t,
                         bool one_body, int ncols, const double* M, int ldm) {
-        auto one = [&](const float* Xb, unsigned long long* Ob, int nc, int ng, int G, const uint32_t* rows,
+        auto one = [&](const float* Xb, unsigned long long* Ob, int nc, int ld, int ng, int G, const uint32_t* rows,
                        const uint16_t* labs) {
-            if (one_body) launch_group(c, Xb, Ob, nc, ng, G, rows, labs, M, ldm);
-            else launch_group_same_f32(c, Xb, Ob, nc, ng, G, rows, labs, M, ldm);
+            if (one_body) launch_group(c, Xb, Ob, nc, ld, ng, G, rows, labs, M, ldm);
+            else launch_group_same_f32(c, Xb, Ob, nc, ld, ng, G, rows, labs, M, ldm);
         };
         if (!y.on) {
-            if (one_body) one(X, out, ncols, t.ng1, t.g1, t.g1row.p, t.g1lab.p);
-            else one(X, out, ncols, t.ng2, t.g2, t.g2row.p, t.g2lab.p);
+            if (one_body) one(X, out, ncols, ncols, t.ng1, t.g1, t.g1row.p, t.g1lab.p);
+            else one(X, out, ncols, ncols, t.ng2, t.g2, t.g2row.p, t.g2lab.p);
             return;
         }
-        for (const GroupSub& g : subs) one(X + g.blk, out + g.blk, g.ncols, g.ngroups, g.G, y.grow.p + g.off, y.glab.p + g.off);
+        for (const GroupSub& g : subs)
+            one(X + g.blk, out + g.blk, g.ncols, g.ld, g.ngroups, g.G, y.grow.p + g.off, y.glab.p + g.off);
     };
     if (a_g1) groups32(c.c32.p, c.s64a.p, y.a1, c.A, true, nbs, c.Ha.p, c.n);
     if (c.A.ng2) groups32(c.c32.p, c.s64a.p, y.a2, c.A, false, nbs, c.M2a.p, np2);
@@ -846,11 +848,12 @@ void sigma_fp64(Context& c, const double* C, double* S) {
             FCIB_KCHECK();
         };
         if (c.sym.on) {
-            // per target alpha irrep: the g = 0 sub-problem writes the block, the others add to it
+            // per target rows: the first sub-problem writes them, the others add to them
             const SymSpace& y = c.sym;
             for (const AbSub& u : y.ab) {
-                const int64_t sb = y.d.blk[u.src], tb = y.d.blk[u.ha];
-                launch(C + sb, u.ns, u.ns, C + tb, S + tb, u.nt, u.g != 0 ? 1 : 0, y.conn.p + u.conn, u.kmax,
+                // source columns: a run of the source block's rows; target rows: a run of the target block
+                const int64_t sb = y.d.blk[u.src] + u.col0, tb = y.d.blk[u.ha] + (int64_t)u.row0 * u.nt;
+                launch(C + sb, u.lds, u.ns, C + tb, S + tb, u.nt, u.accumulate, y.conn.p + u.conn, u.kmax,
                        y.tgt32.p + u.tgt32, y.npg[u.g], y.np_g[u.g], y.Vg.p + y.vg_off[u.g], y.npg[u.g], u.rows);
             }
         } else {

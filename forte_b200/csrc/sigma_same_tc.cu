@@ -76,7 +76,7 @@ __device__ __forceinline__ void reg_after4(uint32_t (&r)[4]) {
 
 template <int Q>
 __global__ void __launch_bounds__(kGtThreads, 2)
-    k_group_tc(const float* __restrict__ C, unsigned long long* __restrict__ S, int ncols,
+    k_group_tc(const float* __restrict__ C, unsigned long long* __restrict__ S, int ncols, int ld,
                const uint32_t* __restrict__ rows, const uint16_t* __restrict__ labs, int G,
                const double* __restrict__ M, int ldm, int ngroups, int* __restrict__ counter,
                int* __restrict__ err, const int* __restrict__ grid_el) {
@@ -149,14 +149,14 @@ __global__ void __launch_bounds__(kGtThreads, 2)
             *reinterpret_cast<float*>(Blo + off) = lo;
         }
         fence_proxy_async();  // W (generic-proxy stores) becomes visible to the tensor core's reads
-        // row offsets (string index * ncols) of this thread's quads, shared by gather and epilogue
+        // row offsets (string index * ld) of this thread's quads, shared by gather and epilogue
         uint32_t off[Q][4];
 #pragma unroll
         for (int i = 0; i < Q; i++)
 #pragma unroll
             for (int u = 0; u < 4; u++) {
                 const int j = 4 * (cg + 4 * i) + u;
-                off[i][u] = (j < G && rs[j] != kNullRow) ? (rs[j] & kConnIdxMask) * (uint32_t)ncols : kGtNoRow;
+                off[i][u] = (j < G && rs[j] != kNullRow) ? (rs[j] & kConnIdxMask) * (uint32_t)ld : kGtNoRow;
             }
         // X-tile gather, one tile ahead in registers (coalesced across lanes)
         float xv[Q][4];
@@ -263,7 +263,7 @@ __global__ void __launch_bounds__(kGtThreads, 2)
 // 32-bit element offsets; the caller then uses k_group<float>.  The group counter and the timeout
 // flag live in counter slots 4 and 5; the flag is cleared by the caller once per sigma and read
 // back by tc_check_error.
-bool launch_group_tc(Context& c, const float* C, unsigned long long* S, int ncols, int ngroups, int G,
+bool launch_group_tc(Context& c, const float* C, unsigned long long* S, int ncols, int ld, int ngroups, int G,
                      const uint32_t* rows, const uint16_t* labs, const double* M, int ldm) {
     if (G < 1 || G > kGtMaxG || (uint64_t)c.nas * (uint64_t)c.nbs >= (1ull << 32) - kGtM) return false;
     if (ngroups == 0) return true;
@@ -276,7 +276,7 @@ bool launch_group_tc(Context& c, const float* C, unsigned long long* S, int ncol
     ensure_counter(c);
     FCIB_CUDA(cudaMemsetAsync(c.counter.p + 4, 0, sizeof(int), c.stream));
     const int grid = std::min(ngroups, 2 * c.num_sms);
-    kern<<<grid, kGtThreads, smem, c.stream>>>(C, S, ncols, rows, labs, G, M, ldm, ngroups, c.counter.p + 4,
+    kern<<<grid, kGtThreads, smem, c.stream>>>(C, S, ncols, ld, rows, labs, G, M, ldm, ngroups, c.counter.p + 4,
                                                c.counter.p + 5, c.counter.p + kSlotSameGrid);
     FCIB_KCHECK();
     return true;

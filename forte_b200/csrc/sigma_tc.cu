@@ -214,7 +214,9 @@ constexpr int kMagicBits = 0x4B400000;      // bit pattern of kMagic
 // barrier.
 // Source rows (plane, ns beta strings) and target rows (C, S: nt beta strings) have their own
 // lengths, so one launch also serves a sub-problem of the irrep-blocked layout; ndiag = 0 drops the
-// diagonal pairs and accumulate = 1 adds the row to S instead of writing E0 C + the product.
+// diagonal pairs and accumulate = 1 adds the row to S instead of writing E0 C + the product.  The
+// source strings may be a sub-range of the target row's strings (GAS sub-problems): their own
+// elements, which the diagonal pairs add to, start at target column diag_off.
 // NW warps: NW / 4 column groups per TMEM lane quarter.  Gather chunks of column group cg: cg + NCG j
 // (at 16 warps the third round goes to group 3 - cg, which holds one epilogue chunk fewer);
 // off-diagonal epilogue chunks: (NCG - 1 - cg) + NCG i; the diagonal chunks go to group 0.
@@ -228,7 +230,8 @@ template <bool THREE, int NW>
 __global__ void __launch_bounds__(NW * 32, 1)
     k_ab_tc(const float2* __restrict__ Phl, int ldp, int ns, const double* __restrict__ C, double* __restrict__ S,
             int nt, int accumulate, const uint32_t* __restrict__ connA, int s1a, const uint16_t* __restrict__ tgtR,
-            int npair, const int* __restrict__ perm, int noff8, int ndiag, const uint32_t* __restrict__ bstr, int kb,
+            int npair, const int* __restrict__ perm, int noff8, int ndiag, int diag_off,
+            const uint32_t* __restrict__ bstr, int kb,
             const double* __restrict__ V, int ldv, float vmax, const unsigned int* __restrict__ cmax_bits,
             int nas, int ncontrib, const uint8_t* __restrict__ mag, double e0, int* __restrict__ row_counter,
             int* __restrict__ err) {
@@ -475,7 +478,7 @@ __global__ void __launch_bounds__(NW * 32, 1)
 #pragma unroll
                     for (int r = 0; r < 16; r++)
                         if (r < ndiag && ((occ >> r) & 1u)) d += __uint_as_float(rd[r >> 3][r & 7]);
-                    add_fixed(d, acc_s + (uint32_t)jb_epi * 4u, jb_epi < ns ? 0u : 0xFFFFu);
+                    add_fixed(d, acc_s + (uint32_t)(jb_epi + diag_off) * 4u, jb_epi < ns ? 0u : 0xFFFFu);
                 }
             }
             tc_fence_before();
@@ -583,8 +586,14 @@ void ab_tc(Context& c, const double* C, double* S, bool three) {
     };
     c.tc_ev.ensure();
     if (y.on) {
-        // blocked layout: TF32 planes per alpha block, one launch per (target irrep, pair irrep)
-        c.tf_hi.alloc(2 * std::max<size_t>(y.plane_total, 1));
+        // blocked layout: TF32 planes per alpha block, one launch per sub-problem
+        // a sub-problem whose source columns start inside a row gathers up to 127 pairs past the
+        // row's end; the planes carry that much (zeroed) slack at their end
+        const size_t slack = kTcM;
+        if (c.tf_hi.n != 2 * (y.plane_total + slack)) {
+            c.tf_hi.alloc(2 * (y.plane_total + slack));
+            FCIB_CUDA(cudaMemsetAsync(c.tf_hi.p, 0, sizeof(float) * c.tf_hi.n, c.stream));
+        }
         c.c32.alloc((size_t)c.nvec);
         float2* hl = reinterpret_cast<float2*>(c.tf_hi.p);
         for (int h = 0; h < c.nirrep; h++) {
@@ -601,11 +610,12 @@ void ab_tc(Context& c, const double* C, double* S, bool three) {
             const int ncol = noff8 + ndiag;
             const size_t smem = smem_of(u.kmax, ncol, u.nt, noff8, ndiag);
             FCIB_CUDA(cudaMemsetAsync(c.counter.p, 0, sizeof(int), c.stream));  // row counter (errors stay)
-            const int64_t tb = y.d.blk[u.ha];
+            const int64_t tb = y.d.blk[u.ha] + (int64_t)u.row0 * u.nt;
             kern<<<std::min(u.rows, c.num_sms), kTcWarps * 32, smem, c.stream>>>(
-                hl + y.plane_off[u.src], y.ldp[u.src], u.ns, C + tb, S + tb, u.nt, g != 0 ? 1 : 0, y.conn.p + u.conn,
-                u.kmax, y.tgt16.p + u.tgt16, ncol, y.perm.p + y.perm_off[g], noff8, ndiag,
-                y.bstr_sorted.p + y.d.boff[u.ha ^ c.irrep ^ g], kb, y.Vz.p, y.npp, c.vmax, cmax_bits, u.rows, 0,
+                hl + y.plane_off[u.src] + u.col0, y.ldp[u.src], u.ns, C + tb, S + tb, u.nt, u.accumulate,
+                y.conn.p + u.conn, u.kmax, y.tgt16.p + u.tgt16, ncol, y.perm.p + y.perm_off[g], noff8, ndiag,
+                u.diag_off, y.bstr_sorted.p + y.d.boff[u.ha ^ c.irrep ^ g] + u.col0, kb, y.Vz.p, y.npp, c.vmax,
+                cmax_bits, u.rows, 0,
                 y.mag.p + u.mag, c.scalar, c.counter.p, c.counter.p + 1);
             FCIB_KCHECK();
         }
@@ -643,7 +653,7 @@ void ab_tc(Context& c, const double* C, double* S, bool three) {
     const int grid = std::min(nas, c.num_sms);
     FCIB_CUDA(cudaEventRecord(c.tc_ev.e[0], c.stream));
     kern<<<grid, kTcWarps * 32, smem, c.stream>>>(hl, ldp, nbs, C, S, nbs, 0, c.A.conn.p, s1a, c.tgtR16.p, ncol,
-                                                  c.tc_perm.p, noff8, n, c.B.str.p, kb, c.V.p, c.A.npair_pad, c.vmax,
+                                                  c.tc_perm.p, noff8, n, 0, c.B.str.p, kb, c.V.p, c.A.npair_pad, c.vmax,
                                                   cmax_bits, nas, kb * (n - kb) + 1, nullptr, c.scalar, c.counter.p,
                                                   c.counter.p + 1);
     FCIB_KCHECK();

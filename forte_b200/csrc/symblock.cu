@@ -20,6 +20,16 @@
 // Each sub-problem is smaller than the C1 problem by about the irrep count in rows or columns and
 // in connections or pairs, so a sigma costs ~1/nirrep of the masked C1 sigma and a vector
 // 1/nirrep of its memory.
+//
+// With GAS spaces (gas.cu) the blocks hold the strings of the GAS determinants only, sorted within
+// an irrep by occupation pattern, so each pattern is a run of rows (alpha) or columns (beta).  The
+// sub-problems then also split by the pattern run of the target rows and of the source columns,
+// and keep only those through which a GAS determinant receives a contribution: source columns one
+// replacement away from a column pattern that the rows pair with, and connections to source rows
+// whose pattern pairs with the source columns.  Same-spin groups split by the column run and keep
+// the members whose pattern pairs with it.  The first sub-problem of a row run writes it; elements
+// outside the GAS space are left to the mask.  The work then follows the GAS determinants rather
+// than the products of their strings.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -30,7 +40,9 @@ namespace fcib {
 
 static int sb_pad8(int x) { return (x + 7) / 8 * 8; }
 
-// same-spin groups of one spin and kind, split by the irrep of their strings
+// same-spin groups of one spin and kind, split by the irrep of their strings and, per column
+// pattern run of the block (one run without GAS), restricted to the members whose pattern some GAS
+// determinant pairs with that run's pattern (the others meet zeros there and are masked there)
 static void build_group_subs(Context& c, const SpinTables& t, bool alpha, bool one_body, std::vector<GroupSub>& out,
                              std::vector<uint32_t>& rows_all, std::vector<uint16_t>& labs_all) {
     SymSpace& y = c.sym;
@@ -43,9 +55,17 @@ static void build_group_subs(Context& c, const SpinTables& t, bool alpha, bool o
     FCIB_CUDA(cudaMemcpy(labs.data(), (one_body ? t.g1lab.p : t.g2lab.p), 2 * labs.size(), cudaMemcpyDeviceToHost));
     const std::vector<int>& irr = alpha ? y.airr : y.birr;
     const std::vector<int32_t>& loc = alpha ? y.aloc_h : y.bloc_h;
+    const std::vector<int>& pat = alpha ? y.apat : y.bpat;
     const int nh = c.nirrep, S = c.irrep;
-    std::vector<std::vector<std::vector<std::pair<uint32_t, uint16_t>>>> parts(nh);
-    std::vector<std::vector<std::pair<uint32_t, uint16_t>>> bucket(nh);
+    // parts[h][r]: the groups of rows of irrep h for column run r of the block
+    std::vector<std::vector<std::vector<std::vector<std::pair<uint32_t, uint16_t>>>>> parts(nh);
+    for (int h = 0; h < nh; h++) parts[h].resize((alpha ? y.brun[h ^ S] : y.arun[h ^ S]).size());
+    struct Member {
+        uint32_t e;
+        uint16_t lab;
+        int pat;
+    };
+    std::vector<std::vector<Member>> bucket(nh);
     for (int gi = 0; gi < ng; gi++) {
         for (auto& b : bucket) b.clear();
         for (int m = 0; m < G; m++) {
@@ -53,26 +73,40 @@ static void build_group_subs(Context& c, const SpinTables& t, bool alpha, bool o
             if (e == kNullRow) continue;
             const uint32_t I = e & kConnIdxMask;
             if (loc[I] < 0) continue;  // a string no GAS determinant uses: its rows and columns are absent
-            bucket[irr[I]].push_back({(uint32_t)loc[I] | (e & kSignBit), labs[(size_t)gi * G + m]});
+            bucket[irr[I]].push_back({(uint32_t)loc[I] | (e & kSignBit), labs[(size_t)gi * G + m], pat[I]});
         }
-        for (int h = 0; h < nh; h++)
-            if (!bucket[h].empty()) parts[h].push_back(bucket[h]);
+        for (int h = 0; h < nh; h++) {
+            if (bucket[h].empty()) continue;
+            const std::vector<PatRange>& cr = alpha ? y.brun[h ^ S] : y.arun[h ^ S];
+            for (size_t r = 0; r < cr.size(); r++) {
+                std::vector<std::pair<uint32_t, uint16_t>> part;
+                for (const Member& x : bucket[h]) {
+                    const int pa = alpha ? x.pat : cr[r].pat, pb = alpha ? cr[r].pat : x.pat;
+                    if (y.allowed[(size_t)pa * y.npb + pb]) part.push_back({x.e, x.lab});
+                }
+                if (!part.empty()) parts[h][r].push_back(std::move(part));
+            }
+        }
     }
     for (int h = 0; h < nh; h++) {
-        const int ncols = alpha ? y.bcnt[h ^ S] : y.acnt[h ^ S];
-        if (parts[h].empty() || ncols == 0) continue;
-        GroupSub s;
-        s.ngroups = (int)parts[h].size();
-        for (auto& p : parts[h]) s.G = std::max(s.G, (int)p.size());
-        s.ncols = ncols;
-        s.blk = alpha ? y.d.blk[h] : y.blkT[h];
-        s.off = rows_all.size();
-        for (auto& p : parts[h])
-            for (int m = 0; m < s.G; m++) {
-                rows_all.push_back(m < (int)p.size() ? p[m].first : kNullRow);
-                labs_all.push_back(m < (int)p.size() ? p[m].second : (uint16_t)0);
-            }
-        out.push_back(s);
+        const std::vector<PatRange>& cr = alpha ? y.brun[h ^ S] : y.arun[h ^ S];
+        const int ld = alpha ? y.bcnt[h ^ S] : y.acnt[h ^ S];
+        for (size_t r = 0; r < cr.size(); r++) {
+            if (parts[h][r].empty()) continue;
+            GroupSub s;
+            s.ngroups = (int)parts[h][r].size();
+            for (auto& p : parts[h][r]) s.G = std::max(s.G, (int)p.size());
+            s.ncols = cr[r].count;
+            s.ld = ld;
+            s.blk = (alpha ? y.d.blk[h] : y.blkT[h]) + cr[r].start;
+            s.off = rows_all.size();
+            for (auto& p : parts[h][r])
+                for (int m = 0; m < s.G; m++) {
+                    rows_all.push_back(m < (int)p.size() ? p[m].first : kNullRow);
+                    labs_all.push_back(m < (int)p.size() ? p[m].second : (uint16_t)0);
+                }
+            out.push_back(s);
+        }
     }
 }
 
@@ -143,93 +177,122 @@ static void build_ab_subs(Context& c, const std::vector<uint32_t>& sb) {
     std::vector<uint16_t> tgt16_all;
     std::vector<uint8_t> mag_all;
     y.ab.clear();
+    auto allowed = [&](int pa, int pb) { return y.allowed[(size_t)pa * y.npb + pb] != 0; };
     for (int ha = 0; ha < nh; ha++) {
         const int hb = ha ^ S;
         if (y.acnt[ha] == 0 || y.bcnt[hb] == 0) continue;
-        for (int g = 0; g < nh; g++) {
-            const int src = ha ^ g, hjb = hb ^ g;
-            if (y.np_g[g] == 0 || y.acnt[src] == 0 || y.bcnt[hjb] == 0) continue;
-            AbSub u;
-            u.ha = ha;
-            u.g = g;
-            u.src = src;
-            u.rows = y.acnt[ha];
-            u.ns = y.bcnt[hjb];
-            u.nt = y.bcnt[hb];
-            std::vector<std::vector<uint32_t>> lists(u.rows);
-            for (int i = 0; i < u.rows; i++) {
-                const int Ia = y.asrc_h[y.d.aoff[ha] + i];
-                for (int k = 0; k < s1; k++) {
-                    const uint32_t e = conn[(size_t)Ia * s1 + k];
-                    const int P = (int)((e >> 21) & 1023u);
-                    if (P >= npair || pirr[P] != g) continue;
-                    const uint32_t J = e & kConnIdxMask;
-                    FCIB_CHECK(y.airr[J] == src, FCIB_ERR_NUMERIC, "blocked sigma: connection irrep mismatch");
-                    if (y.aloc_h[J] < 0) continue;  // a source string no GAS determinant uses
-                    lists[i].push_back((uint32_t)y.aloc_h[J] | ((uint32_t)P << 21) | (e & kSignBit));
-                }
-                u.kmax = std::max(u.kmax, (int)lists[i].size());
-            }
-            if (u.kmax == 0) {
-                if (g != 0) continue;
-                u.kmax = 1;  // the g = 0 launch writes the block (E0 C) even without connections
-            }
-            u.conn = conn_all.size();
-            for (int i = 0; i < u.rows; i++)
-                for (int k = 0; k < u.kmax; k++)
-                    conn_all.push_back(k < (int)lists[i].size() ? lists[i][k] : (Pz << 21));
-            // FP64 targets [ns][npg]: local target | sign, or kNoTarget
-            u.tgt32 = tgt32_all.size();
-            for (int j = 0; j < u.ns; j++) {
-                const int Jb = y.bsrc_h[y.d.boff[hjb] + j];
-                for (int col = 0; col < y.npg[g]; col++) {
-                    int32_t v = kNoTarget;
-                    if (col < y.np_g[g]) {
-                        const int32_t e = tgt[(size_t)Jb * npp + plist[g][col]];
-                        if (e != kNoTarget) {
-                            const uint32_t I = (uint32_t)e & kConnIdxMask;
-                            FCIB_CHECK(y.birr[I] == hb, FCIB_ERR_NUMERIC, "blocked sigma: target irrep mismatch");
-                            if (y.bloc_h[I] >= 0) v = (int32_t)((uint32_t)y.bloc_h[I] | ((uint32_t)e & kSignBit));
+        // target rows: one alpha pattern run at a time (the whole block without GAS)
+        for (const PatRange& ar : y.arun[ha]) {
+            bool written = false;  // the first sub-problem of these rows writes them
+            // patterns of target columns that GAS determinants pair with these rows
+            std::vector<int> tcols;
+            for (const PatRange& br : y.brun[hb])
+                if (allowed(ar.pat, br.pat)) tcols.push_back(br.pat);
+            for (int g = 0; g < nh; g++) {
+                const int src = ha ^ g, hjb = hb ^ g;
+                if (y.np_g[g] == 0 || y.acnt[src] == 0 || y.bcnt[hjb] == 0) continue;
+                for (const PatRange& sr : y.brun[hjb]) {
+                    // useful when the source columns reach a column pattern of these rows and some
+                    // alpha pattern one replacement away from the rows' pairs with the source columns
+                    bool reach_t = false, reach_s = false;
+                    for (int pb : tcols) reach_t = reach_t || y.breach[(size_t)sr.pat * y.npb + pb];
+                    for (int pa = 0; pa < y.npa; pa++)
+                        reach_s = reach_s || (y.areach[(size_t)ar.pat * y.npa + pa] && allowed(pa, sr.pat));
+                    const bool writer = !written && g == 0;
+                    if (!(reach_t && reach_s) && !writer) continue;
+                    AbSub u;
+                    u.ha = ha;
+                    u.g = g;
+                    u.src = src;
+                    u.row0 = ar.start;
+                    u.rows = ar.count;
+                    u.col0 = sr.start;
+                    u.ns = sr.count;
+                    u.lds = y.bcnt[hjb];
+                    u.nt = y.bcnt[hb];
+                    u.diag_off = g == 0 ? sr.start : 0;
+                    // connections of the rows through pairs of irrep g to sources whose pattern the
+                    // source columns pair with (other sources hold zeros there)
+                    std::vector<std::vector<uint32_t>> lists(u.rows);
+                    for (int i = 0; i < u.rows; i++) {
+                        const int Ia = y.asrc_h[y.d.aoff[ha] + ar.start + i];
+                        for (int k = 0; k < s1; k++) {
+                            const uint32_t e = conn[(size_t)Ia * s1 + k];
+                            const int P = (int)((e >> 21) & 1023u);
+                            if (P >= npair || pirr[P] != g) continue;
+                            const uint32_t J = e & kConnIdxMask;
+                            FCIB_CHECK(y.airr[J] == src, FCIB_ERR_NUMERIC, "blocked sigma: connection irrep mismatch");
+                            if (y.aloc_h[J] < 0 || !allowed(y.apat[J], sr.pat)) continue;
+                            lists[i].push_back((uint32_t)y.aloc_h[J] | ((uint32_t)P << 21) | (e & kSignBit));
+                        }
+                        u.kmax = std::max(u.kmax, (int)lists[i].size());
+                    }
+                    if (u.kmax == 0) {
+                        if (!writer) continue;
+                        u.kmax = 1;  // the writer writes its rows (E0 C) even without connections
+                    }
+                    u.accumulate = written ? 1 : 0;
+                    written = true;
+                    u.conn = conn_all.size();
+                    for (int i = 0; i < u.rows; i++)
+                        for (int k = 0; k < u.kmax; k++)
+                            conn_all.push_back(k < (int)lists[i].size() ? lists[i][k] : (Pz << 21));
+                    // FP64 targets [ns][npg]: target column in the whole row | sign, or kNoTarget
+                    u.tgt32 = tgt32_all.size();
+                    for (int j = 0; j < u.ns; j++) {
+                        const int Jb = y.bsrc_h[y.d.boff[hjb] + sr.start + j];
+                        for (int col = 0; col < y.npg[g]; col++) {
+                            int32_t v = kNoTarget;
+                            if (col < y.np_g[g]) {
+                                const int32_t e = tgt[(size_t)Jb * npp + plist[g][col]];
+                                if (e != kNoTarget) {
+                                    const uint32_t I = (uint32_t)e & kConnIdxMask;
+                                    FCIB_CHECK(y.birr[I] == hb, FCIB_ERR_NUMERIC, "blocked sigma: target irrep mismatch");
+                                    if (y.bloc_h[I] >= 0) v = (int32_t)((uint32_t)y.bloc_h[I] | ((uint32_t)e & kSignBit));
+                                }
+                            }
+                            tgt32_all.push_back(v);
                         }
                     }
-                    tgt32_all.push_back(v);
-                }
-            }
-            // tensor-core targets [noff8/8][ns padded to 128][8]: local target * 4 | sign, 0xFFFF none
-            u.tgt16 = tgt16_all.size();
-            if (u.nt <= kMaxBetaStrings) {
-                const int ldp = (u.ns + kTcM - 1) / kTcM * kTcM;
-                const int* pm = perm_all.data() + y.perm_off[g];
-                for (int c8 = 0; c8 < y.noff8_g[g] / 8; c8++)
-                    for (int j = 0; j < ldp; j++)
-                        for (int uu = 0; uu < 8; uu++) {
-                            uint16_t v = 0xFFFFu;
-                            const int R = pm[8 * c8 + uu];
-                            if (R >= 0 && j < u.ns) {
-                                const int Jb = y.bsrc_h[y.d.boff[hjb] + j];
-                                const int32_t e = tgt[(size_t)Jb * npp + R];
-                                if (e != kNoTarget && y.bloc_h[(uint32_t)e & kConnIdxMask] >= 0)
-                                    v = (uint16_t)(((uint32_t)y.bloc_h[(uint32_t)e & kConnIdxMask] << 2) |
-                                                   ((uint32_t)e >> 31));
-                            }
-                            tgt16_all.push_back(v);
+                    // tensor-core targets [noff8/8][ns padded to 128][8]: target column * 4 | sign, 0xFFFF none
+                    u.tgt16 = tgt16_all.size();
+                    if (u.nt <= kMaxBetaStrings) {
+                        const int ldp = (u.ns + kTcM - 1) / kTcM * kTcM;
+                        const int* pm = perm_all.data() + y.perm_off[g];
+                        for (int c8 = 0; c8 < y.noff8_g[g] / 8; c8++)
+                            for (int j = 0; j < ldp; j++)
+                                for (int uu = 0; uu < 8; uu++) {
+                                    uint16_t v = 0xFFFFu;
+                                    const int R = pm[8 * c8 + uu];
+                                    if (R >= 0 && j < u.ns) {
+                                        const int Jb = y.bsrc_h[y.d.boff[hjb] + sr.start + j];
+                                        const int32_t e = tgt[(size_t)Jb * npp + R];
+                                        if (e != kNoTarget && y.bloc_h[(uint32_t)e & kConnIdxMask] >= 0)
+                                            v = (uint16_t)(((uint32_t)y.bloc_h[(uint32_t)e & kConnIdxMask] << 2) |
+                                                           ((uint32_t)e >> 31));
+                                    }
+                                    tgt16_all.push_back(v);
+                                }
+                    }
+                    // contributions per target element of the tensor-core scatter: one per off-diagonal
+                    // pair of irrep g with exactly one orbital occupied whose source string (the other
+                    // orbital occupied) is in the source columns, plus the diagonal sum when g = 0 and
+                    // the element's own string is a source column
+                    u.mag = mag_all.size();
+                    for (int j = 0; j < u.nt; j++) {
+                        const int Ib = y.bsrc_h[y.d.boff[hb] + j];
+                        const uint32_t s = sb[Ib];
+                        int cnt = (g == 0 && y.bpat[Ib] == sr.pat) ? 1 : 0;
+                        for (int P : plist[g]) {
+                            if (pp[P] == pq[P] || !(((s >> pp[P]) ^ (s >> pq[P])) & 1u)) continue;
+                            const uint32_t J = s ^ (1u << pp[P]) ^ (1u << pq[P]);
+                            cnt += y.bpat[host_rank(J, n)] == sr.pat ? 1 : 0;
                         }
-            }
-            // contributions per target element of the tensor-core scatter: one per off-diagonal pair of
-            // irrep g with exactly one orbital occupied whose source string (the other orbital occupied)
-            // is in the blocks, plus the diagonal sum when g = 0
-            u.mag = mag_all.size();
-            for (int j = 0; j < u.nt; j++) {
-                const uint32_t s = sb[y.bsrc_h[y.d.boff[hb] + j]];
-                int cnt = g == 0 ? 1 : 0;
-                for (int P : plist[g]) {
-                    if (pp[P] == pq[P] || !(((s >> pp[P]) ^ (s >> pq[P])) & 1u)) continue;
-                    const uint32_t J = s ^ (1u << pp[P]) ^ (1u << pq[P]);
-                    cnt += y.bkeep[host_rank(J, n)] ? 1 : 0;
+                        mag_all.push_back((uint8_t)cnt);
+                    }
+                    y.ab.push_back(u);
                 }
-                mag_all.push_back((uint8_t)cnt);
             }
-            y.ab.push_back(u);
         }
     }
     y.conn.upload(conn_all, c.stream);
@@ -265,8 +328,16 @@ void build_sym_space(Context& c) {
     std::vector<uint32_t> sa(c.nas), sb(c.nbs);
     FCIB_CUDA(cudaMemcpy(sa.data(), c.A.str.p, 4 * c.nas, cudaMemcpyDeviceToHost));
     FCIB_CUDA(cudaMemcpy(sb.data(), c.B.str.p, 4 * c.nbs, cudaMemcpyDeviceToHost));
-    std::vector<uint8_t> keep_a(c.nas, 1), keep_b(c.nbs, 1);
-    if (c.gas.ngas > 0) gas_keep_strings(c, sa, sb, keep_a, keep_b);
+    // occupation patterns: with GAS spaces those of the GAS determinants (strings of no GAS
+    // determinant are dropped), otherwise one pattern 0 for every string
+    y.apat.assign(c.nas, 0);
+    y.bpat.assign(c.nbs, 0);
+    y.npa = y.npb = 1;
+    y.allowed.assign(1, 1);
+    y.areach.assign(1, 1);
+    y.breach.assign(1, 1);
+    if (c.gas.ngas > 0)
+        gas_string_patterns(c, sa, sb, y.apat, y.bpat, y.npa, y.npb, y.allowed, y.areach, y.breach);
     SymDev& d = y.d;
     d = SymDev{};
     d.on = 1;
@@ -275,29 +346,37 @@ void build_sym_space(Context& c) {
     for (int b = 0; b < 3; b++)
         for (int p = 0; p < n; p++)
             if (c.orbsym[p] >> b & 1) d.irrbit[b] |= 1u << p;
-    // kept strings sorted by irrep (string order within an irrep); loc = -1 for the others
-    auto sort_strings = [&](const std::vector<uint32_t>& s, const std::vector<uint8_t>& keep, std::vector<int>& irr,
-                            int* cnt, int32_t* off, std::vector<int32_t>& src, std::vector<int32_t>& loc) {
+    // kept strings sorted by irrep, then by pattern, then in string order; loc = -1 for the others
+    auto sort_strings = [&](const std::vector<uint32_t>& s, const std::vector<int>& pat, int npat, std::vector<int>& irr,
+                            int* cnt, int32_t* off, std::vector<int32_t>& src, std::vector<int32_t>& loc,
+                            std::vector<PatRange>* run) {
         const size_t ns = s.size();
         irr.resize(ns);
         loc.assign(ns, -1);
-        for (int h = 0; h < 8; h++) cnt[h] = 0;
+        std::vector<std::vector<std::vector<int32_t>>> by(8, std::vector<std::vector<int32_t>>(npat));
         for (size_t i = 0; i < ns; i++) {
             irr[i] = sym_irrep_of(d, s[i]);
-            if (keep[i]) loc[i] = cnt[irr[i]]++;
+            if (pat[i] >= 0) by[irr[i]][pat[i]].push_back((int32_t)i);
         }
         int32_t o = 0;
+        src.clear();
         for (int h = 0; h < 8; h++) {
             off[h] = o;
+            cnt[h] = 0;
+            run[h].clear();
+            for (int q = 0; q < npat; q++) {
+                if (by[h][q].empty()) continue;
+                run[h].push_back(PatRange{q, cnt[h], (int)by[h][q].size()});
+                for (int32_t i : by[h][q]) {
+                    loc[i] = cnt[h]++;
+                    src.push_back(i);
+                }
+            }
             o += cnt[h];
         }
-        src.assign((size_t)o, 0);
-        for (size_t i = 0; i < ns; i++)
-            if (loc[i] >= 0) src[off[irr[i]] + loc[i]] = (int32_t)i;
     };
-    sort_strings(sa, keep_a, y.airr, y.acnt, d.aoff, y.asrc_h, y.aloc_h);
-    sort_strings(sb, keep_b, y.birr, y.bcnt, d.boff, y.bsrc_h, y.bloc_h);
-    y.bkeep = keep_b;
+    sort_strings(sa, y.apat, y.npa, y.airr, y.acnt, d.aoff, y.asrc_h, y.aloc_h, y.arun);
+    sort_strings(sb, y.bpat, y.npb, y.birr, y.bcnt, d.boff, y.bsrc_h, y.bloc_h, y.brun);
     d.blk[0] = 0;
     y.blkT[0] = 0;
     for (int h = 0; h < 8; h++) {
