@@ -222,3 +222,41 @@ def test_gas_rejects_bad_spaces():
     assert s.size() == 0
     with pytest.raises(RuntimeError, match="dimension zero"):
         s.compute_energy()
+
+
+def test_gas_rdms3_and_transition_rdm_match_oracle():
+    # 3-RDMs of a GAS root and the transition 1-RDM between GAS states of two irreps
+    case = CASES[2]
+    opts = {"E_CONVERGENCE": 1e-12, "R_CONVERGENCE": 1e-8}
+    ints, s, o, dets, idx = _setup(case, opts)
+    s.compute_energy()
+    c0 = np.zeros(o.ndet)
+    c0[idx] = s.evecs()[0]
+    got = s.rdms([(0, 0)], 3)[0]
+    ref = o.rdms3(c0)
+    for name in ("g3aaa", "g3aab", "g3abb", "g3bbb"):
+        assert np.max(np.abs(getattr(got, name) - ref[name])) <= 1e-9, name
+    osym, na, nb, irrep, spaces, mn, mx = case
+    irrep2 = 1
+    t = GenCISolver(StateInfo(na, nb, abs(na - nb) + 1, na - nb, irrep2, tuple(mn), tuple(mx)), 1, ints, spaces, opts)
+    t.compute_energy()
+    dets2 = G.determinants(len(osym), osym, _nirrep(osym), irrep2, na, nb, spaces, mn, mx)
+    sa = {int(x): i for i, x in enumerate(o.strings(0))}
+    sb = {int(x): i for i, x in enumerate(o.strings(1))}
+    cr = np.zeros(o.ndet)
+    cr[[sa[a] * o.nbs + sb[b] for a, b in dets2]] = t.evecs()[0]
+    tr = s.transition_rdms([(0, 0)], t, 1)[0]
+    rt = o.rdms(c0, cr, 1)
+    assert max(np.max(np.abs(rt["g1a"])), np.max(np.abs(rt["g1b"]))) > 1e-6
+    assert np.max(np.abs(tr.g1a - rt["g1a"])) <= 1e-9
+    assert np.max(np.abs(tr.g1b - rt["g1b"])) <= 1e-9
+
+
+def test_gas_learned_preconditioner_converges_to_the_same_energy():
+    case = CASES[0]
+    opts = {"E_CONVERGENCE": 1e-11, "R_CONVERGENCE": 1e-7, "DL_MAXITER": 200}
+    ints, s, o, dets, idx = _setup(case, opts)
+    e = s.compute_energy()
+    m = GenCISolver(StateInfo(4, 4, 1, 0, 0, tuple(case[5]), tuple(case[6])), 1, ints, case[4],
+                    dict(opts, FCI_PRECONDITIONER="MLP"))
+    assert abs(m.compute_energy() - e) <= 1e-9
