@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstring>
 #include <random>
+#include <stdexcept>
 
 #include "fcib_internal.h"
 #include "guess.h"
@@ -617,7 +618,7 @@ static void project_out(Context& c, std::vector<SparseDev>& bad, std::vector<dou
 }
 
 const double* root_vector(Context& c, int root) {
-    return c.csf_basis_solve ? c.evdet.p + (size_t)root * c.nvec : c.b.p + (size_t)root * c.nvec;
+    return c.roots_in_evdet ? c.evdet.p + (size_t)root * c.nvec : c.b.p + (size_t)root * c.nvec;
 }
 
 double spin2_device(Context& c, const double* C) {
@@ -691,6 +692,30 @@ static std::vector<std::pair<double, int64_t>> lowest_diagonal(Context& c, int c
     return lowest_keys(c, c.hdiag.p, count);
 }
 
+// out[i] = in[idx[i]] and out[idx[i]] = in[i] (flat order <-> engine layout)
+__global__ void k_gather_idx(double* __restrict__ out, const double* __restrict__ in, const int64_t* __restrict__ idx,
+                             size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = in[idx[i]];
+}
+__global__ void k_scatter_idx(double* __restrict__ out, const double* __restrict__ in, const int64_t* __restrict__ idx,
+                              size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[idx[i]] = in[i];
+}
+static void gather_flat(Context& c, const double* layout, double* flat) {
+    const size_t nf = c.flat_map.size();
+    k_gather_idx<<<(int)std::min<size_t>((nf + 255) / 256, 8 * (size_t)c.num_sms), 256, 0, c.stream>>>(
+        flat, layout, c.flat_map_d.p, nf);
+    FCIB_KCHECK();
+}
+static void scatter_flat(Context& c, const double* flat, double* layout) {
+    const size_t nf = c.flat_map.size();
+    k_scatter_idx<<<(int)std::min<size_t>((nf + 255) / 256, 8 * (size_t)c.num_sms), 256, 0, c.stream>>>(
+        layout, flat, c.flat_map_d.p, nf);
+    FCIB_KCHECK();
+}
+
 __global__ void k_neg_abs(const double* __restrict__ x, double* __restrict__ out, size_t n) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
         out[i] = -fabs(x[i]);
@@ -717,9 +742,24 @@ void dl_solve(Context& c) {
         c.csf_x.alloc((size_t)c.nvec);
         c.csf_s.alloc((size_t)c.nvec);
     }
-    const int64_t N = csf_basis ? c.ncsf : c.nvec;
+    // GAS spaces: the Davidson space is the GAS determinants themselves (GenCIVector flat order),
+    // so the vector work follows them and not the layout's string products; sigma scatters its
+    // input into the layout and gathers its output back.  The learned preconditioner and the
+    // residual capture work on layout vectors, so they keep the layout.
+    const bool gas_basis = !csf_basis && c.gas.ngas > 0 && c.opt.preconditioner != FCIB_PRECOND_MLP &&
+                           c.capture_max == 0 && !c.flat_map.empty();
+    if (gas_basis) {
+        const size_t nf = c.flat_map.size();
+        c.flat_map_d.upload(c.flat_map, c.stream);
+        c.gas_x.alloc((size_t)c.nvec);
+        FCIB_CUDA(cudaMemsetAsync(c.gas_x.p, 0, sizeof(double) * c.nvec, c.stream));  // scatters write GAS positions only
+        c.gas_s.alloc((size_t)c.nvec);
+        c.hd_gas.alloc(nf);
+        gather_flat(c, c.hdiag.p, c.hd_gas.p);
+    }
+    const int64_t N = csf_basis ? c.ncsf : gas_basis ? (int64_t)c.flat_map.size() : c.nvec;
     int64_t Neff = N;
-    if (!csf_basis && c.mask.p) {
+    if (!csf_basis && !gas_basis && c.mask.p) {
         std::vector<uint8_t> hm(N);
         FCIB_CUDA(cudaMemcpy(hm.data(), c.mask.p, N, cudaMemcpyDeviceToHost));
         Neff = 0;
@@ -749,10 +789,16 @@ void dl_solve(Context& c) {
         tmp[i] = c.tmp.p + (size_t)i * N;
     }
     for (int k = 0; k < nroot; k++) r[k] = c.r.p + (size_t)k * N;
-    Ops ops(c, (size_t)N, csf_basis ? c.hd_csf.p : c.hdiag.p);
+    Ops ops(c, (size_t)N, csf_basis ? c.hd_csf.p : gas_basis ? c.hd_gas.p : c.hdiag.p);
     // sigma of a vector of the Davidson space: in the CSF basis z -> P z -> H P z -> P^T H P z
     // (fci_solver.cc:247-254)
     auto space_sigma = [&](const double* bj, double* sj, int prec) {
+        if (gas_basis) {
+            scatter_flat(c, bj, c.gas_x.p);
+            sigma_dispatch(c, c.gas_x.p, c.gas_s.p, prec);
+            gather_flat(c, c.gas_s.p, sj);
+            return;
+        }
         if (!csf_basis) {
             sigma_dispatch(c, bj, sj, prec);
             return;
@@ -850,7 +896,8 @@ void dl_solve(Context& c) {
         return added;
     };
     auto fresh_guess = [&]() -> int {
-        auto lowest = lowest_diagonal(c, ng);
+        // lowest diagonal elements (GAS basis: over the flat order, ties by flat position)
+        auto lowest = gas_basis ? lowest_keys(c, c.hd_gas.p, ng, (size_t)N, nullptr) : lowest_diagonal(c, ng);
         std::vector<uint32_t> sa(c.nas), sbv(c.nbs);
         FCIB_CUDA(cudaMemcpy(sa.data(), c.A.str.p, 4 * c.nas, cudaMemcpyDeviceToHost));
         FCIB_CUDA(cudaMemcpy(sbv.data(), c.B.str.p, 4 * c.nbs, cudaMemcpyDeviceToHost));
@@ -861,10 +908,12 @@ void dl_solve(Context& c) {
         const int n = c.n;
         GuessResult gr;
         try {
-            // vector index <-> determinant in the engine layout (C1 or the target irrep's blocks)
+            // vector index <-> determinant in the engine layout (C1 or the target irrep's blocks), or
+            // in the GAS flat order
             gr = make_guess(
                 hi, lowest,
                 [&](int64_t I) {
+                    if (gas_basis) I = c.flat_map[I];
                     if (!c.sym.on) return Det{sa[I / nbs], sbv[I % nbs]};
                     int64_t ia, ib;
                     sym_host_decode(c, I, ia, ib);
@@ -872,7 +921,12 @@ void dl_solve(Context& c) {
                 },
                 [&](const Det& d) {
                     const int64_t ia = host_rank((uint32_t)d.a, n), ib = host_rank((uint32_t)d.b, n);
-                    return c.sym.on ? sym_host_encode(c, ia, ib) : ia * nbs + ib;
+                    const int64_t I = c.sym.on ? sym_host_encode(c, ia, ib) : ia * nbs + ib;
+                    if (!gas_basis) return I;
+                    // spin partners of GAS determinants are GAS determinants (same electrons per space)
+                    const int64_t f = gas_flat_position(c, I);
+                    if (f < 0) throw std::runtime_error("initial guess: a determinant outside the GAS space");
+                    return f;
                 },
                 num_guess_states, c.multiplicity);
         } catch (std::exception& e) {
@@ -905,7 +959,7 @@ void dl_solve(Context& c) {
                 k_add_random<<<ops.nblk, kRedThreads, 0, c.stream>>>(tmp[k], N, 0x9E3779B97F4A7C15ull * (k + 1),
                                                                      1.0e-3 * std::sqrt(3.0 / (double)N));
                 FCIB_KCHECK();
-                apply_mask(c, tmp[k]);
+                if (!gas_basis) apply_mask(c, tmp[k]);
             }
         }
         project_out(c, bad, tmp, std::min(nroot, nguess));
@@ -1109,7 +1163,7 @@ void dl_solve(Context& c) {
                 FCIB_CUDA(cudaMemsetAsync(tmp[m - 1], 0, sizeof(double) * N, c.stream));
                 k_add_random<<<ops.nblk, kRedThreads, 0, c.stream>>>(tmp[m - 1], N, 0xD1B54A32D192ED03ull + rng(), 1.0);
                 FCIB_KCHECK();
-                if (!csf_basis) apply_mask(c, tmp[m - 1]);
+                if (!csf_basis && !gas_basis) apply_mask(c, tmp[m - 1]);
                 std::vector<double*> one{tmp[m - 1]};
                 project_out(c, bad, one, 1);
                 int ra = add_rows_orth(ops, b, basis, one, 1);
@@ -1145,12 +1199,16 @@ void dl_solve(Context& c) {
     c.dl_prev = true;
     c.dl_prev_space = space;
     c.dl_lambda_old = lambda;
-    if (csf_basis) {
+    if (csf_basis || gas_basis) {
         // the roots in the determinant layout, for <S^2>, RDMs and the flat-order vectors
         c.evdet.alloc((size_t)nroot * c.nvec);
-        for (int k = 0; k < nroot; k++) csf_to_det(c, c.b.p + (size_t)k * N, c.evdet.p + (size_t)k * c.nvec);
+        if (gas_basis) FCIB_CUDA(cudaMemsetAsync(c.evdet.p, 0, sizeof(double) * nroot * c.nvec, c.stream));
+        for (int k = 0; k < nroot; k++) {
+            if (gas_basis) scatter_flat(c, c.b.p + (size_t)k * N, c.evdet.p + (size_t)k * c.nvec);
+            else csf_to_det(c, c.b.p + (size_t)k * N, c.evdet.p + (size_t)k * c.nvec);
+        }
     }
-    c.csf_basis_solve = csf_basis;
+    c.roots_in_evdet = csf_basis || gas_basis;
     c.spin2.resize(nroot);
     for (int k = 0; k < nroot; k++) c.spin2[k] = spin2_device(c, root_vector(c, k));
     FCIB_CUDA(cudaStreamSynchronize(c.stream));

@@ -350,7 +350,11 @@ struct Context {
     DBuf<double> csf_x, csf_s;  // determinant-space scratch of the CSF-basis sigma
     DBuf<double> hd_csf;        // CSF diagonal of the last spin-adapted solve
     DBuf<double> evdet;         // spin-adapted solves: the roots in the engine's determinant layout
-    bool csf_basis_solve = false;  // the last solve ran in the CSF basis (its roots are in evdet)
+    bool roots_in_evdet = false;   // the last solve ran in the CSF basis or the GAS flat basis (roots in evdet)
+    // GAS solves: the Davidson space is the GAS determinants in GenCIVector flat order
+    DBuf<int64_t> flat_map_d;   // device copy of flat_map
+    DBuf<double> gas_x, gas_s;  // layout-sized sigma input (zero outside the GAS space) and output
+    DBuf<double> hd_gas;        // diagonal in flat order
     std::vector<int64_t> dl_prev_space;
     std::vector<std::vector<std::pair<int64_t, double>>> dl_bad;
     std::vector<double> dl_lambda_old;  // eigenvalues of the previous solve's last iteration

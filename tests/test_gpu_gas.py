@@ -260,3 +260,23 @@ def test_gas_learned_preconditioner_converges_to_the_same_energy():
     m = GenCISolver(StateInfo(4, 4, 1, 0, 0, tuple(case[5]), tuple(case[6])), 1, ints, case[4],
                     dict(opts, FCI_PRECONDITIONER="MLP"))
     assert abs(m.compute_energy() - e) <= 1e-9
+
+
+def test_gas_restart_with_new_integrals_matches_a_fresh_solver():
+    # repeated solves restart from the previous roots (here in the GAS flat basis) with the new
+    # integrals of a nearby Hamiltonian, as FCISolver keeps its Davidson-Liu solver between calls
+    from forte_b200.integrals import ActiveSpaceIntegrals
+    case = CASES[0]
+    opts = {"E_CONVERGENCE": 1e-12, "R_CONVERGENCE": 1e-8, "DL_MAXITER": 200}
+    ints, s, o, dets, idx = _setup(case, opts, nroot=2)
+    s.compute_energy()
+    h = ints.oei_a + 0.02 * np.eye(ints.n) * np.linspace(-1.0, 1.0, ints.n)
+    ints2 = ActiveSpaceIntegrals(ints.n, ints.scalar, h, h, 1.03 * ints.tei_aa, 1.03 * ints.tei_ab,
+                                 1.03 * ints.tei_bb, ints.orbsym)
+    s.set_integrals(ints2)
+    s.compute_energy()
+    f = GenCISolver(StateInfo(case[1], case[2], 1, 0, case[3], tuple(case[5]), tuple(case[6])), 2, ints2, case[4],
+                    opts)
+    f.compute_energy()
+    assert np.max(np.abs(np.array(s.energies()) - np.array(f.energies()))) <= 1e-10
+    assert s.iterations() < f.iterations()
