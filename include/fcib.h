@@ -100,7 +100,8 @@ int fcib_set_integrals(fcib_ctx* ctx, int n, int nirrep, const int* orbsym, doub
                        const double* oei_a, const double* oei_b, const double* tei_aa,
                        const double* tei_ab, const double* tei_bb);
 /* na/nb active alpha/beta electrons, target irrep, multiplicity (2S+1) used to select the
- * guess, number of roots and the root returned by the solver's energy. */
+ * guess, number of roots and the root returned by the solver's energy.  StateInfo's twice_ms is
+ * not a separate argument: the determinant space fixes 2 Ms = na - nb. */
 int fcib_set_state(fcib_ctx* ctx, int na, int nb, int irrep, int multiplicity, int nroot, int root);
 int fcib_set_options(fcib_ctx* ctx, const fcib_options* opt);
 /* Generalized active spaces (GenCISolver, forte/genci/genci_solver.h): keep the determinants whose
