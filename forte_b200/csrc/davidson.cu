@@ -295,23 +295,29 @@ __global__ void k_fill_sparse(double* __restrict__ v, const int64_t* __restrict_
     if (i < cnt) v[idx[i]] = val[i];
 }
 
-// v -= (v . u) u for a sparse vector u (one block)
-__global__ void k_project_sparse(double* __restrict__ v, const int64_t* __restrict__ idx, const double* __restrict__ val, int cnt) {
+// v -= (v . u_b) u_b for the sparse vectors u_0, u_1, ... in order (one block; entries of u_b at
+// off[b] .. off[b + 1] of idx/val)
+__global__ void k_project_sparse(double* __restrict__ v, const int64_t* __restrict__ idx, const double* __restrict__ val,
+                                 const int* __restrict__ off, int nb) {
     __shared__ double red[32];
-    double s = 0.0;
-    for (int i = threadIdx.x; i < cnt; i += blockDim.x) s = fma(v[idx[i]], val[i], s);
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double t = 0.0;
-        for (int w = 0; w < (int)(blockDim.x + 31) / 32; w++) t += red[w];
-        red[0] = t;
+    for (int b = 0; b < nb; b++) {
+        const int o0 = off[b], cnt = off[b + 1] - o0;
+        double s = 0.0;
+        for (int i = threadIdx.x; i < cnt; i += blockDim.x) s = fma(v[idx[o0 + i]], val[o0 + i], s);
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+            for (int w = 0; w < (int)(blockDim.x + 31) / 32; w++) t += red[w];
+            red[0] = t;
+        }
+        __syncthreads();
+        double ov = red[0];
+        __syncthreads();
+        for (int i = threadIdx.x; i < cnt; i += blockDim.x) v[idx[o0 + i]] -= ov * val[o0 + i];
+        __syncthreads();  // the next vector's dot reads these updates
     }
-    __syncthreads();
-    double ov = red[0];
-    __syncthreads();
-    for (int i = threadIdx.x; i < cnt; i += blockDim.x) v[idx[i]] -= ov * val[i];
 }
 
 // ------------------------------------------------------------------------------------------
@@ -556,6 +562,14 @@ struct SparseDev {
     DBuf<double> val;
     int cnt = 0;
 };
+// the unwanted roots of the guess, packed: root b holds entries off[b] .. off[b + 1]
+struct BadRoots {
+    DBuf<int64_t> idx;
+    DBuf<double> val;
+    DBuf<int> off;
+    int nb = 0;
+    bool empty() const { return nb == 0; }
+};
 
 // add_row_and_orthonormalize (davidson_liu_solver.cc:634-687): A[rowsA] <- s*src Gram-Schmidt
 // orthonormalised against A[0..rowsA); false if discarded (norm < 1e-7 after projection).
@@ -609,12 +623,12 @@ static int add_rows_orth(Ops& ops, std::vector<double*>& A, int rowsA, const std
     return added;
 }
 
-static void project_out(Context& c, std::vector<SparseDev>& bad, std::vector<double*>& V, int nvec) {
-    for (int k = 0; k < nvec; k++)
-        for (auto& b : bad) {
-            k_project_sparse<<<1, 256, 0, c.stream>>>(V[k], b.idx.p, b.val.p, b.cnt);
-            FCIB_KCHECK();
-        }
+static void project_out(Context& c, BadRoots& bad, std::vector<double*>& V, int nvec) {
+    if (bad.empty()) return;
+    for (int k = 0; k < nvec; k++) {
+        k_project_sparse<<<1, 256, 0, c.stream>>>(V[k], bad.idx.p, bad.val.p, bad.off.p, bad.nb);
+        FCIB_KCHECK();
+    }
 }
 
 const double* root_vector(Context& c, int root) {
@@ -795,6 +809,12 @@ void dl_solve(Context& c) {
     auto space_sigma = [&](const double* bj, double* sj, int prec) {
         if (gas_basis) {
             scatter_flat(c, bj, c.gas_x.p);
+            // only the GAS positions of the output are gathered, so the mask pass is skipped
+            struct Unmasked {
+                Context& c;
+                explicit Unmasked(Context& cc) : c(cc) { c.sigma_unmasked = true; }
+                ~Unmasked() { c.sigma_unmasked = false; }
+            } guard(c);
             sigma_dispatch(c, c.gas_x.p, c.gas_s.p, prec);
             gather_flat(c, c.gas_s.p, sj);
             return;
@@ -852,18 +872,19 @@ void dl_solve(Context& c) {
     int ng = (int)std::min<int64_t>((int64_t)num_guess_states * o.dets_per_guess, Neff);
     double t_guess0 = now_ms();
     int basis = 0;
-    std::vector<SparseDev> bad;
+    BadRoots bad;
     auto upload_bad = [&](const std::vector<std::vector<std::pair<int64_t, double>>>& src) {
-        std::vector<SparseDev> v(src.size());  // device buffers are neither copied nor moved
-        for (size_t i = 0; i < src.size(); i++) {
-            std::vector<int64_t> ix;
-            std::vector<double> vv;
-            for (auto& e : src[i]) { ix.push_back(e.first); vv.push_back(e.second); }
-            v[i].idx.upload(ix, c.stream);
-            v[i].val.upload(vv, c.stream);
-            v[i].cnt = (int)ix.size();
+        std::vector<int64_t> ix;
+        std::vector<double> vv;
+        std::vector<int> off(1, 0);
+        for (auto& r : src) {
+            for (auto& e : r) { ix.push_back(e.first); vv.push_back(e.second); }
+            off.push_back((int)ix.size());
         }
-        bad.swap(v);
+        bad.nb = (int)src.size();
+        bad.idx.upload(ix, c.stream);
+        bad.val.upload(vv, c.stream);
+        bad.off.upload(off, c.stream);
         FCIB_CUDA(cudaStreamSynchronize(c.stream));  // the host index vectors go out of scope
     };
     // a fresh guess (FCISolver::initial_guess_det): lowest diagonal determinants, spin-adapted

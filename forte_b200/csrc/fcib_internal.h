@@ -355,6 +355,7 @@ struct Context {
     DBuf<int64_t> flat_map_d;   // device copy of flat_map
     DBuf<double> gas_x, gas_s;  // layout-sized sigma input (zero outside the GAS space) and output
     DBuf<double> hd_gas;        // diagonal in flat order
+    bool sigma_unmasked = false;  // the sigma being built is only gathered at GAS positions (no mask pass)
     std::vector<int64_t> dl_prev_space;
     std::vector<std::vector<std::pair<int64_t, double>>> dl_bad;
     std::vector<double> dl_lambda_old;  // eigenvalues of the previous solve's last iteration

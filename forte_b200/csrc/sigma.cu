@@ -646,7 +646,7 @@ static void transpose(Context& c, const double* in, double* out, int rows, int c
     FCIB_KCHECK();
 }
 void apply_mask(Context& c, double* v) {
-    if (!c.mask.p) return;
+    if (!c.mask.p || c.sigma_unmasked) return;
     k_apply_mask<<<4 * c.num_sms, 256, 0, c.stream>>>(v, c.mask.p, (size_t)c.nvec);
     FCIB_KCHECK();
 }
