@@ -373,7 +373,8 @@ def run_gas(args, world, rank, local):
     build.build()
     torch.cuda.set_device(local)
     n, k = args.n, args.n // 2
-    ints = synthetic(n, 3 * n, SEED, gap=GAP)
+    osym = [(i // 2) % 8 for i in range(n)] if args.gas_sym == "d2h" else None
+    ints = synthetic(n, 3 * n, SEED, gap=GAP, orbsym=osym)
     spaces = [list(range(k)), list(range(k, n))]
     L = capi.lib()
     res = {}
@@ -399,6 +400,7 @@ def run_gas(args, world, rank, local):
                 for _ in range(args.warmup):
                     one()
                 torch.cuda.synchronize()
+                l0 = s.profile()["launches"]
                 e0 = torch.cuda.Event(enable_timing=True)
                 e1 = torch.cuda.Event(enable_timing=True)
                 e0.record(stream)
@@ -407,6 +409,7 @@ def run_gas(args, world, rank, local):
                 e1.record(stream)
                 e1.synchronize()
                 r["sigma_ms"][prec_name] = e0.elapsed_time(e1) / args.steps
+                r.setdefault("launches_per_sigma", {})[prec_name] = (s.profile()["launches"] - l0) / args.steps
             del x, y
             torch.cuda.empty_cache()
             for prec_name in ("MIXED", "FP64"):
@@ -427,8 +430,9 @@ def run_gas(args, world, rank, local):
             "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": False, "dtype": "tf32x3/f64",
             "data": "synthetic",
-            "config": {"workload": f"C1 CAS({n},{n}) synthetic L={3 * n}, GAS1 = orbitals 0..{k - 1}, GAS2 = "
-                                   f"{k}..{n - 1} with at most m electrons"},
+            "config": {"workload": f"{'D2h' if osym else 'C1'} CAS({n},{n}) synthetic L={3 * n}, GAS1 = orbitals "
+                                   f"0..{k - 1}, GAS2 = {k}..{n - 1} with at most m electrons, Ag singlet",
+                       "orbital_irreps": osym},
             "results": res,
         }), flush=True)
 
@@ -701,6 +705,8 @@ def main():
     ap.add_argument("--seeds", type=int, default=5, help="precond mode: integral seeds of the A/B comparison")
     ap.add_argument("--gas-m", default="2,4", help="gas mode: upper-half electron limits to run")
     ap.add_argument("--gas-layouts", default="blocked,masked", help="gas mode: layouts to run")
+    ap.add_argument("--gas-sym", default="c1", choices=["c1", "d2h"],
+                    help="gas mode: no symmetry, or D2h with two orbitals per irrep")
     args = ap.parse_args()
     world, rank, local = dist_init(args)
     if args.impl == "reference":

@@ -321,6 +321,7 @@ struct Context {
     // GenCIVector order); empty when the layout is the flat order itself
     std::vector<int64_t> flat_map;
     DBuf<int> counter;    // work counters for persistent kernels
+    DBuf<int> subctr;     // row counters of the blocked sigma's sub-problems (zeroed once per sigma)
     DBuf<double> red;     // reduction scratch
     // timers and status of the last solve
     double t_sigma_ms = 0.0;

@@ -831,33 +831,42 @@ void sigma_fp64(Context& c, const double* C, double* S) {
         if (c.vmax <= 0.0f) c.vmax = host_vmax(c);
         // one grid for every launch of this sigma (the blocked sub-problems have fewer connections)
         const double bound = std::fabs(c.scalar) + (double)c.B.s1 * kpad * (double)c.vmax;
+        int attr_smem = -1;  // the kernel's dynamic shared memory limit, raised only when a launch needs more
         auto launch = [&](const double* Csrc, int lds, int ns, const double* Ct, double* St, int nt, int acc,
                           const uint32_t* conn, int s1, const int32_t* tgt, int ldt, int npair, const double* V,
-                          int ldv, int rows) {
+                          int ldv, int rows, int* ctr) {
             const size_t smem = ab_fp64_smem(nt, s1, 0);
             FCIB_CHECK(smem + 1024 <= (size_t)c.smem_optin, FCIB_ERR_UNSUPPORTED,
                        "opposite-spin row block exceeds shared memory (beta string count too large)");
-            FCIB_CUDA(cudaFuncSetAttribute(k_ab_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            if ((int)smem > attr_smem) {
+                FCIB_CUDA(cudaFuncSetAttribute(k_ab_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                attr_smem = (int)smem;
+            }
             int per_sm = std::max(1, (int)(c.smem_per_sm / (smem + 1024)));
             per_sm = std::min(per_sm, 2048 / kDmThreads);
             const int grid = std::min(rows, per_sm * c.num_sms);
-            FCIB_CUDA(cudaMemsetAsync(c.counter.p, 0, sizeof(int), c.stream));
             k_ab_fp64<<<grid, kDmThreads, smem, c.stream>>>(Csrc, lds, ns, Ct, St, nt, acc, conn, s1, (s1 + 7) / 8 * 8,
-                                                            tgt, ldt, npair, V, ldv, rows, c.scalar, c.counter.p, cmax64,
+                                                            tgt, ldt, npair, V, ldv, rows, c.scalar, ctr, cmax64,
                                                             bound);
             FCIB_KCHECK();
         };
         if (c.sym.on) {
-            // per target rows: the first sub-problem writes them, the others add to them
+            // per target rows: the first sub-problem writes them, the others add to them; each
+            // sub-problem has its own row counter, all zeroed at once
             const SymSpace& y = c.sym;
-            for (const AbSub& u : y.ab) {
+            c.subctr.alloc(std::max<size_t>(y.ab.size(), 1));
+            FCIB_CUDA(cudaMemsetAsync(c.subctr.p, 0, sizeof(int) * c.subctr.n, c.stream));
+            for (size_t i = 0; i < y.ab.size(); i++) {
+                const AbSub& u = y.ab[i];
                 // source columns: a run of the source block's rows; target rows: a run of the target block
                 const int64_t sb = y.d.blk[u.src] + u.col0, tb = y.d.blk[u.ha] + (int64_t)u.row0 * u.nt;
                 launch(C + sb, u.lds, u.ns, C + tb, S + tb, u.nt, u.accumulate, y.conn.p + u.conn, u.kmax,
-                       y.tgt32.p + u.tgt32, y.npg[u.g], y.np_g[u.g], y.Vg.p + y.vg_off[u.g], y.npg[u.g], u.rows);
+                       y.tgt32.p + u.tgt32, y.npg[u.g], y.np_g[u.g], y.Vg.p + y.vg_off[u.g], y.npg[u.g], u.rows,
+                       c.subctr.p + i);
             }
         } else {
-            launch(C, nbs, nbs, C, S, nbs, 0, c.A.conn.p, s1a, c.B.tgt.p, npp, c.A.npair, c.V.p, npp, nas);
+            FCIB_CUDA(cudaMemsetAsync(c.counter.p, 0, sizeof(int), c.stream));
+            launch(C, nbs, nbs, C, S, nbs, 0, c.A.conn.p, s1a, c.B.tgt.p, npp, c.A.npair, c.V.p, npp, nas, c.counter.p);
         }
     } else {
         k_scale_copy<<<4 * c.num_sms, 256, 0, c.stream>>>(C, S, c.scalar, N);

@@ -573,6 +573,7 @@ void ab_tc(Context& c, const double* C, double* S, bool three) {
     FCIB_CUDA(cudaMemsetAsync(cmax_bits, 0, sizeof(unsigned int), c.stream));
     auto kern = three ? k_ab_tc<true, kTcWarps> : k_ab_tc<false, kTcWarps>;
     // shared memory of one launch: one CTA per SM (it owns all tensor memory)
+    int attr_smem = -1;  // the kernel's dynamic shared memory limit, raised only when a launch needs more
     auto smem_of = [&](int s1, int ncol, int nt, int noff8, int ndiag) {
         const TcLayout L = tc_layout(s1, ncol, nt, three);
         FCIB_CHECK(nt <= kMaxBetaStrings, FCIB_ERR_UNSUPPORTED, "tensor-core opposite-spin kernel: too many beta strings");
@@ -581,7 +582,10 @@ void ab_tc(Context& c, const double* C, double* S, bool three) {
         const size_t smem = std::max<size_t>(L.total, 120 * 1024);
         FCIB_CHECK(smem + 2048 <= (size_t)c.smem_optin, FCIB_ERR_UNSUPPORTED,
                    "tensor-core kernel: sigma row and integral block exceed shared memory");
-        FCIB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        if ((int)smem > attr_smem) {
+            FCIB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            attr_smem = (int)smem;
+        }
         return smem;
     };
     c.tc_ev.ensure();
@@ -605,18 +609,21 @@ void ab_tc(Context& c, const double* C, double* S, bool three) {
         }
         c.c32_ready = true;
         FCIB_CUDA(cudaEventRecord(c.tc_ev.e[0], c.stream));
-        for (const AbSub& u : y.ab) {
+        // one row counter per sub-problem, all zeroed at once (the error flag in counter slot 1 stays)
+        c.subctr.alloc(std::max<size_t>(y.ab.size(), 1));
+        FCIB_CUDA(cudaMemsetAsync(c.subctr.p, 0, sizeof(int) * c.subctr.n, c.stream));
+        for (size_t i = 0; i < y.ab.size(); i++) {
+            const AbSub& u = y.ab[i];
             const int g = u.g, noff8 = y.noff8_g[g], ndiag = y.ndiag_g[g];
             const int ncol = noff8 + ndiag;
             const size_t smem = smem_of(u.kmax, ncol, u.nt, noff8, ndiag);
-            FCIB_CUDA(cudaMemsetAsync(c.counter.p, 0, sizeof(int), c.stream));  // row counter (errors stay)
             const int64_t tb = y.d.blk[u.ha] + (int64_t)u.row0 * u.nt;
             kern<<<std::min(u.rows, c.num_sms), kTcWarps * 32, smem, c.stream>>>(
                 hl + y.plane_off[u.src] + u.col0, y.ldp[u.src], u.ns, C + tb, S + tb, u.nt, u.accumulate,
                 y.conn.p + u.conn, u.kmax, y.tgt16.p + u.tgt16, ncol, y.perm.p + y.perm_off[g], noff8, ndiag,
                 u.diag_off, y.bstr_sorted.p + y.d.boff[u.ha ^ c.irrep ^ g] + u.col0, kb, y.Vz.p, y.npp, c.vmax,
                 cmax_bits, u.rows, 0,
-                y.mag.p + u.mag, c.scalar, c.counter.p, c.counter.p + 1);
+                y.mag.p + u.mag, c.scalar, c.subctr.p + i, c.counter.p + 1);
             FCIB_KCHECK();
         }
         FCIB_CUDA(cudaEventRecord(c.tc_ev.e[1], c.stream));
