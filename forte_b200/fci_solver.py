@@ -414,28 +414,38 @@ class GenCISolver(FCISolver):
 
     def set_gas(self, gas_spaces, gas_min=(), gas_max=()):
         """Set the GAS spaces and bounds; no spaces restores the full determinant space."""
-        spaces = [sorted(int(p) for p in sp) for sp in gas_spaces]
-        while spaces and not spaces[-1]:
-            spaces.pop()
         n = self.ints.n
-        if len(spaces) > 6:
-            raise ValueError("at most six GAS spaces")
-        if any(not sp for sp in spaces):
-            raise ValueError("an empty GAS space is followed by a non-empty one")
-        owner = [-1] * n
-        for k, sp in enumerate(spaces):
-            for p in sp:
-                if not 0 <= p < n or owner[p] >= 0:
-                    raise ValueError(f"orbital {p} is outside the active space or in two GAS spaces")
-                owner[p] = k
-        if spaces and n and min(owner) < 0:
-            raise ValueError("every active orbital must belong to a GAS space")
-        mn = [int(gas_min[k]) if k < len(gas_min) else 0 for k in range(len(spaces))]
-        mx = [int(gas_max[k]) if k < len(gas_max) else 2 * len(sp) for k, sp in enumerate(spaces)]
+        spaces, owner, mn, mx = gas_layout(gas_spaces, n, gas_min, gas_max)
         ng = len(spaces)
         self.gas_spaces, self.gas_min, self.gas_max = spaces, mn, mx
         capi.check(capi.lib().fcib_set_gas(self._h, ng, (C.c_int * max(n, 1))(*owner),
                                            (C.c_int * max(ng, 1))(*mn), (C.c_int * max(ng, 1))(*mx)))
+
+
+def gas_layout(gas_spaces, n, gas_min=(), gas_max=()):
+    """The GAS spaces as the engine takes them: (spaces without trailing empty ones, the space of
+    each of the n orbitals, lower and upper electron bounds per space).  Missing bounds default to
+    0 and 2 * size (make_state_weights_map, base_classes/active_space_solver.cc:706-740).  Raises
+    ValueError for more than six spaces, an empty space before a non-empty one, an orbital outside
+    0..n-1 or in two spaces, or (with any space given) an orbital in none."""
+    spaces = [sorted(int(p) for p in sp) for sp in gas_spaces]
+    while spaces and not spaces[-1]:
+        spaces.pop()
+    if len(spaces) > 6:
+        raise ValueError("at most six GAS spaces")
+    if any(not sp for sp in spaces):
+        raise ValueError("an empty GAS space is followed by a non-empty one")
+    owner = [-1] * n
+    for k, sp in enumerate(spaces):
+        for p in sp:
+            if not 0 <= p < n or owner[p] >= 0:
+                raise ValueError(f"orbital {p} is outside the active space or in two GAS spaces")
+            owner[p] = k
+    if spaces and n and min(owner) < 0:
+        raise ValueError("every active orbital must belong to a GAS space")
+    mn = [int(gas_min[k]) if k < len(gas_min) else 0 for k in range(len(spaces))]
+    mx = [int(gas_max[k]) if k < len(gas_max) else 2 * len(sp) for k, sp in enumerate(spaces)]
+    return spaces, owner, mn, mx
 
 
 def make_active_space_method(method: str, state: StateInfo, nroot: int, ints: ActiveSpaceIntegrals,

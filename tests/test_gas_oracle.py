@@ -1,6 +1,7 @@
 """The GAS oracle (GenCISolver's determinant space restated) pinned on the CPU: the reference's
 golden determinant lists (tests/pytest/gas/test_lists.py, compared as sets there too) and the
-equivalence of the occupation-pattern construction with the per-space electron bounds."""
+equivalence of the occupation-pattern construction with the per-space electron bounds; also the
+host-side validation of GAS spaces in the Python mirror."""
 import itertools
 
 import numpy as np
@@ -77,3 +78,36 @@ def test_pattern_order_follows_the_walk():
     assert walk == sorted(walk)
     assert all(a + b >= 2 for a, b in walk)
     assert np.all(np.array([alfa[i][0] + alfa[i][1] for i, _ in pairs]) == 2)
+
+
+def test_gas_layout_host_validation():
+    # the Python mirror's checks of the GAS spaces, before anything reaches the engine
+    from forte_b200.fci_solver import gas_layout
+    spaces, owner, mn, mx = gas_layout([[3, 0, 1], [2, 4, 5], []], 6, (2,))
+    assert spaces == [[0, 1, 3], [2, 4, 5]] and owner == [0, 0, 1, 0, 1, 1]
+    assert mn == [2, 0] and mx == [6, 6]
+    assert gas_layout([], 4) == ([], [-1] * 4, [], [])
+    # orbital 5 in no space, an empty space inside, orbital 2 twice, orbital 6 outside 0..5
+    for bad in ([[0, 1, 2], [3, 4]], [[0, 1, 2], [], [3, 4, 5]], [[0, 1, 2], [2, 3, 4, 5]], [[0, 1, 2, 3, 4, 5, 6]]):
+        with pytest.raises(ValueError):
+            gas_layout(bad, 6)
+    with pytest.raises(ValueError):
+        gas_layout([[0], [1], [2], [3], [4], [5], [6]], 7)  # seven spaces
+
+
+@pytest.mark.parametrize("nirrep,ngas", [(8, 3), (2, 6)])
+def test_patterns_equal_bounds_many_spaces(nirrep, ngas):
+    # up to six spaces and eight irreps: the pattern construction still equals the bounds filter
+    n = 10
+    rng = np.random.default_rng(nirrep * 10 + ngas)
+    orbsym = [int(x) for x in rng.integers(0, nirrep, n)]
+    cuts = sorted(rng.choice(np.arange(1, n), ngas - 1, replace=False))
+    spaces = [list(range(a, b)) for a, b in zip([0] + list(cuts), list(cuts) + [n])]
+    mn = [max(0, len(sp) - 1) if k == 0 else 0 for k, sp in enumerate(spaces)]
+    mx = [2 * len(sp) if k == 0 else min(2 * len(sp), 3) for k, sp in enumerate(spaces)]
+    irrep = int(rng.integers(0, nirrep))
+    dets = G.determinants(n, orbsym, nirrep, irrep, 4, 3, spaces, mn, mx)
+    assert len(set(dets)) == len(dets)
+    ref = {(a, b) for a in _all_strings(n, 4) for b in _all_strings(n, 3)
+           if G._irrep(a ^ b, orbsym) == irrep and G.in_gas(a, b, spaces, mn, mx)}
+    assert set(dets) == ref and len(ref) > 0
